@@ -1,0 +1,213 @@
+/*
+ * mapgraph_b200.h -- C ABI of the B200 (sm_100a) Gather-Apply-Scatter engine.
+ *
+ * This is the drop-in boundary for MapGraph's GAS hot path. The reference exposes
+ * it as C++ templates (CsrProblem, EnactorVertexCentric and the four bundled
+ * vertex programs); here the same operations are plain extern "C" functions with
+ * pointers and sizes, no CUDA or C++ types in the signatures. Each entry cites the
+ * reference interface it replaces (paths inside the MapGraph tree).
+ *
+ * Conventions
+ *   - Vertex ids and offsets are int32 (the reference's VertexId/SizeT = int).
+ *   - Every call returns an mg_status; nothing throws or exits. mg_last_error()
+ *     gives a human-readable detail for the calling thread's last failure.
+ *   - A graph lives on the CUDA device that was current when it was created and
+ *     owns one CUDA stream; calls on one graph are serialised by the caller
+ *     (a graph is not thread-safe, distinct graphs are). Calls are synchronous:
+ *     results are complete when the call returns, like EnactIterativeSearch.
+ *   - Output pointers are host pointers unless opts->device_output is set, in
+ *     which case they are device pointers on the graph's device.
+ *   - The engine never falls back to CPU code: without a usable GPU every compute
+ *     call returns MG_ERR_NO_DEVICE.
+ */
+#ifndef MAPGRAPH_B200_H
+#define MAPGRAPH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mg_status {
+  MG_OK = 0,
+  MG_ERR_ARG = 1,            /* bad argument: null pointer, size, out-of-range source */
+  MG_ERR_OOM = 2,            /* device or host allocation failed */
+  MG_ERR_QUEUE_OVERFLOW = 3, /* a frontier exceeded the capacity set by queue_sizing */
+  MG_ERR_TIMEOUT = 4,        /* a bounded device-side wait ran out */
+  MG_ERR_CUDA = 5,           /* CUDA runtime error; see mg_last_error() */
+  MG_ERR_NO_DEVICE = 6,      /* no CUDA device / driver available */
+  MG_ERR_UNSUPPORTED = 7     /* option combination not supported */
+} mg_status;
+
+typedef enum mg_dtype {
+  MG_DTYPE_NONE = 0, /* no edge values (unit weights) */
+  MG_DTYPE_I32 = 1,  /* int32 edge values (BFS/SSSP/CC programs: Value = int) */
+  MG_DTYPE_F32 = 2   /* float edge values (PageRank program: Value = float) */
+} mg_dtype;
+
+/* mg_graph_create flags */
+#define MG_GRAPH_SYMMETRIC 0x1u    /* caller asserts the CSR equals its transpose; the CSC aliases it */
+#define MG_GRAPH_NO_CSC 0x2u       /* skip the transpose (then directed == 0, pull BFS and PageRank are refused) */
+#define MG_GRAPH_DEVICE_INPUT 0x4u /* input arrays are device pointers on the current device */
+
+/* BFS direction policy (mg_opts.direction) */
+#define MG_DIR_AUTO 0 /* push/pull switch chosen on the device each level */
+#define MG_DIR_PUSH 1 /* top-down only (the reference engine's only mode) */
+#define MG_DIR_PULL 2 /* bottom-up wherever possible (after the first level) */
+
+/* PageRank modes (mg_pr_opts.mode) */
+#define MG_PR_REFCOMPAT 0  /* x = 0.15 + 0.85 * sum x_u/deg_u, delta frontier (reference semantics) */
+#define MG_PR_NORMALIZED 1 /* x = alpha (P^T x + d t) + (1 - alpha) t, L1-residual stop */
+
+typedef struct mg_graph mg_graph;
+
+/* Options shared by the traversal programs. Zero-initialised means defaults. */
+typedef struct mg_opts {
+  int32_t directed;      /* 1: follow out-edges; 0: out- and in-edges (reference "directed", default 1) */
+  int32_t iter_num;      /* iteration cap (reference "iter_num"); <= 0 means unbounded */
+  int32_t direction;     /* BFS only: MG_DIR_AUTO / MG_DIR_PUSH / MG_DIR_PULL */
+  int32_t device_output; /* 1: output arrays are device pointers */
+  double queue_sizing;   /* frontier capacity = queue_sizing * n (reference "max_queue_sizing");
+                            <= 0 means n, which cannot overflow */
+  int32_t threshold;     /* reference "threshold": accepted for compatibility; strategy is chosen on the device */
+  int32_t use_graph;     /* 1 (default when 0): run the iteration loop as a CUDA graph with a device-side while node;
+                            -1: host-driven loop (one frontier-size read per iteration) */
+  int32_t reserved[4];
+} mg_opts;
+
+/* Counters returned by every compute call (may be NULL). */
+typedef struct mg_stats {
+  int64_t iterations;       /* GAS iterations (BFS levels, relaxation rounds, PR sweeps) */
+  int64_t edges_traversed;  /* TEPS numerator: BFS/SSSP sum of outdeg over reached vertices; CC m; PR m * iterations */
+  int64_t edges_inspected;  /* edges actually read by the kernels */
+  int64_t bytes_compulsory; /* algorithmic DRAM bytes (see the engine's documentation) */
+  double kernel_ms;         /* device time of the iteration loop (CUDA events) */
+  double residual;          /* PageRank: last L1 residual (normalised mode) */
+  int32_t status_detail;    /* engine-specific detail of a non-OK status */
+  int32_t reserved;
+} mg_stats;
+
+/* PageRank options. Zero-initialised fields take the defaults in brackets. */
+typedef struct mg_pr_opts {
+  int32_t mode;          /* MG_PR_REFCOMPAT [default] or MG_PR_NORMALIZED */
+  int32_t directed;      /* REFCOMPAT: 1 in-edges only, 0 both directions with deg = out+in [1] */
+  int32_t max_iter;      /* iteration cap [REFCOMPAT: unbounded; NORMALIZED: 50] */
+  int32_t weighted;      /* NORMALIZED: 1 uses F32 edge values a_uv, P_uv = a_uv / sum_k a_uk [0] */
+  double alpha;          /* NORMALIZED damping [0.85] */
+  double tol;            /* NORMALIZED: stop when the L1 change < tol [1e-6]; REFCOMPAT: active
+                            while |dx| >= tol [0.01] */
+  int32_t compensated;   /* 1: two-sum compensated FP32 accumulation [1]; -1 plain FP32 sums */
+  int32_t device_output; /* 1: ranks/teleport/gradient arrays are device pointers */
+  int32_t use_graph;     /* as mg_opts.use_graph */
+  int32_t reserved[3];
+} mg_pr_opts;
+
+/* ---- status ------------------------------------------------------------- */
+const char *mg_status_string(mg_status s);
+const char *mg_last_error(void);
+const char *mg_version(void);
+/* Number of usable CUDA devices (0 when there is no driver or GPU). */
+int32_t mg_device_count(void);
+
+/* ---- graph storage -------------------------------------------------------
+ * Replaces CsrProblem::FromHostProblem (GASengine/csr_problem.cuh:401-621) and
+ * the GPU CSC build it runs (util.cuh:55-126: offsets_to_indices, sort_by_column).
+ * Copies n+1 row offsets, m column indices and m edge values (vals_t != NONE)
+ * to the current device, validates them, and builds the transpose (CSC, its
+ * edge permutation and the permuted values) unless MG_GRAPH_NO_CSC or
+ * MG_GRAPH_SYMMETRIC. The caller keeps ownership of its arrays. */
+mg_status mg_graph_create(const int32_t *row_offsets, const int32_t *col_idx, const void *edge_vals,
+                          mg_dtype vals_t, int64_t n, int64_t m, uint32_t flags, mg_graph **out);
+
+/* Replaces ~CsrProblem / ~GraphSlice (GASengine/csr_problem.cuh:217-309). NULL is a no-op. */
+mg_status mg_graph_destroy(mg_graph *g);
+
+/* Sizes and flags of a graph (CsrProblem::nodes/edges, csr_problem.cuh:312-314). */
+mg_status mg_graph_info(const mg_graph *g, int64_t *n, int64_t *m, uint32_t *flags, int32_t *device);
+
+/* Device arrays of a graph, as GraphSlice exposes them (csr_problem.cuh:154-163):
+ * row_offsets, column_indices, edge_values (NULL without values), column_offsets,
+ * row_indices and the CSC->CSR edge permutation (the last three NULL without CSC;
+ * equal to the CSR arrays / identity-free NULL perm for symmetric graphs).
+ * Any output pointer may be NULL. */
+mg_status mg_graph_device_arrays(const mg_graph *g, const int32_t **row_offsets,
+                                 const int32_t **col_idx, const void **edge_vals,
+                                 const int32_t **col_offsets, const int32_t **row_idx,
+                                 const int32_t **csc_perm);
+
+/* ---- the four bundled vertex programs ------------------------------------
+ * Each replaces EnactorVertexCentric<CsrProblem, Program>::EnactIterativeSearch
+ * (GASengine/enactor_vertex_centric.cuh:2398-2966) for its Program, followed by
+ * CsrProblem::ExtractResults (csr_problem.cuh:371-396). */
+
+/* struct bfs (Algorithms/BFS/bfs.h:28-262): depth[v] = hops from the nearest of
+ * the nsrc sources (all seeded at 0), -1 when unreached. n outputs. */
+mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth,
+                 const mg_opts *opts, mg_stats *stats);
+
+/* struct sssp (Algorithms/SSSP/sssp.h:33-409): dist[v] = shortest path length from
+ * the nearest source over int32 edge values (unit weights without values),
+ * INT_MAX (2147483647) when unreached. Weights must be >= 0; the graph must carry
+ * I32 values or none. n outputs. */
+mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist,
+                  const mg_opts *opts, mg_stats *stats);
+
+/* struct cc (Algorithms/CC/cc.h:32-349) as driven by Algorithms/CC/cc.cu:289-330
+ * (directed forced to 0, every vertex a source): label[v] = smallest vertex id in
+ * v's weakly connected component. n outputs. */
+mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_stats *stats);
+
+/* struct pagerank (Algorithms/PageRank/PageRank.h:33-409).
+ * REFCOMPAT: the reference's x = 0.15 + 0.85 * sum_{u->v} x_u / deg_u with its
+ *   delta frontier (a vertex stays active while |dx| >= tol, default 0.01);
+ *   nvec must be 1 and teleport NULL.
+ * NORMALIZED: x = alpha * (P^T x + d * t) + (1 - alpha) * t with t the teleport
+ *   vector (uniform when NULL), d the rank mass on dangling vertices, x_0 = t,
+ *   stopping after the first iteration whose L1 change is < tol, or max_iter.
+ *   nvec > 1 runs nvec personalised vectors at once: teleport is nvec x n
+ *   (row-major, each row summing to 1) and ranks is nvec x n.
+ * FP32 values with compensated per-destination accumulation; the residual and
+ * the dangling mass are reduced in FP64. */
+mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nvec, float *ranks,
+                      const mg_pr_opts *opts, mg_stats *stats);
+
+/* ---- batching (no reference counterpart: the reference loops the engine once
+ * per source, Algorithms/BFS/bfs.cu:442-456) ---------------------------------
+ * nsrc independent single-source instances in one device run; depth / dist are
+ * nsrc x n, row i for srcs[i]. */
+mg_status mg_bfs_batch(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth,
+                       const mg_opts *opts, mg_stats *stats);
+mg_status mg_sssp_batch(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist,
+                        const mg_opts *opts, mg_stats *stats);
+
+/* A ragged batch of independent graphs stored as one disjoint union on the device.
+ * Graph i has n[i] vertices and m[i] edges; its vertex v becomes vertex
+ * vertex_base[i] + v of the union (vertex_base = exclusive prefix sum of n,
+ * retrievable with mg_graph_ragged_bases). */
+mg_status mg_graph_create_ragged(int32_t ngraphs, const int32_t *const *row_offsets,
+                                 const int32_t *const *col_idx, const int64_t *n, const int64_t *m,
+                                 uint32_t flags, mg_graph **out);
+mg_status mg_graph_ragged_bases(const mg_graph *g, int64_t *vertex_base /* ngraphs + 1 */);
+/* One BFS per member graph, from local source srcs[i], all in one device run.
+ * depth is laid out like the union's vertices (sum of n[i] entries). */
+mg_status mg_bfs_ragged(mg_graph *g, const int32_t *srcs, int32_t *depth, const mg_opts *opts,
+                        mg_stats *stats);
+
+/* ---- differentiation (no reference counterpart) ----------------------------
+ * Adjoint of the NORMALIZED PageRank fixed point for L = sum_i dL_dranks[i]*x_i:
+ * lambda solves lambda = w + alpha * (P lambda + 1_D (t . lambda)) (the gather
+ * kernel run on the reversed graph), then
+ *   dL/da_uv = alpha * x_u / s_u * (lambda_v - sum_k P_uk lambda_k)   (m, CSR order)
+ *   dL/dt_i  = lambda_i * (1 - alpha + alpha * d)                      (n)
+ * with a the F32 edge values (unit weights when opts->weighted == 0), s_u their
+ * row sums, x = ranks from mg_pagerank with the same options, d its dangling mass.
+ * Either gradient pointer may be NULL. nvec must be 1. */
+mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *ranks,
+                               const float *dL_dranks, float *dL_dweights, float *dL_dteleport,
+                               const mg_pr_opts *opts, mg_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAPGRAPH_B200_H */

@@ -1,0 +1,443 @@
+// bfs.cu -- breadth-first search (struct bfs, Algorithms/BFS/bfs.h:28-262).
+//
+// Per level one of two kernels does the work and the last CTA to finish closes
+// the level (swap queues, pick the next direction, stop or continue):
+//
+//  push (top-down)  input: vertex queue. Each CTA takes a tile of 256 frontier
+//                   vertices and bins them by out-degree: >= CTA_TH edges are
+//                   expanded by the whole CTA, >= 32 by one warp, the rest by a
+//                   block-wide scan over the remaining degrees (thread-level
+//                   bin), so every edge load is coalesced. A neighbour is claimed
+//                   with atomicOr on a visited bitmap (1 bit per vertex); the
+//                   winner writes depth = level + 1 and appends itself to the
+//                   output queue with a warp-aggregated atomic.
+//                   This replaces expand_atomic + contract_atomic
+//                   (GASengine/vertex_centric/expand_atomic/cta.cuh:268-759,
+//                   contract_atomic/cta.cuh:203-612): no edge-sized frontier is
+//                   ever materialised, the dedup is exact, and BFS's contract
+//                   (label := iteration + 1, bfs.h:229-255) is fused in.
+//  pull (bottom-up) every unvisited vertex scans its in-edges for a parent whose
+//                   depth equals the current level and stops at the first hit.
+//                   A warp owns 32 consecutive vertices, i.e. one bitmap word,
+//                   so visited words are updated without atomics.
+//
+// The direction switch (Beamer's heuristic: go bottom-up when the frontier's
+// out-edges exceed 1/14 of the unexplored edges, back when the frontier drops
+// below n/24) is evaluated on the device.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.cuh"
+
+namespace mg {
+
+constexpr int BFS_NT = 256;
+constexpr int BFS_CTA_TH = 512;   // out-degree at or above which a CTA expands the vertex
+constexpr int BFS_WARP_TH = 32;   // out-degree at or above which a warp expands the vertex
+constexpr int PULL_SERIAL = 8;    // in-edges a lane scans alone before the warp helps
+constexpr int64_t BEAMER_ALPHA = 14, BEAMER_BETA = 24;
+
+struct BfsArgs {
+  const int32_t *ro, *ci;  // out-edges (CSR)
+  const int32_t *co, *ri;  // in-edges (CSC; the CSR itself for symmetric graphs)
+  int32_t *label;
+  uint32_t *vis;
+  int32_t *q0, *q1;
+  int32_t qcap;
+  int32_t mode;      // MG_DIR_*
+  int32_t can_pull;  // in-edges available and traversal direction allows it
+  int32_t both;      // directed == 0 on a non-symmetric graph: expand CSR and CSC
+  int64_t n;
+  int64_t m_total;
+  DevCtl *ctl;
+  cudaGraphConditionalHandle h;
+  int32_t use_cond;
+};
+
+template <typename T>
+__device__ __forceinline__ T vload(const T *p) {
+  return *(const volatile T *)p;
+}
+
+__device__ void bfs_level_end(const BfsArgs &a) {
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const int32_t nf = vload(&c->qlen[cur ^ 1]);
+  const int64_t mf = vload(&c->mf_next);
+  const int64_t vdeg = vload(&c->visited_deg) + mf;
+  const int lvl = vload(&c->level) + 1;
+  c->visited_deg = vdeg;
+  c->level = lvl;
+  c->qlen[cur] = 0;
+  c->cur = cur ^ 1;
+  c->mf_next = 0;
+  c->blocks_done = 0;
+  const bool over = vload(&c->overflow) != 0;
+  const bool done = nf == 0 || lvl >= c->iter_cap || over;
+  int dir = vload(&c->dir);
+  if (!done) {
+    if (a.mode == MG_DIR_PULL) {
+      dir = a.can_pull ? 1 : 0;
+    } else if (a.mode == MG_DIR_PUSH || !a.can_pull) {
+      dir = 0;
+    } else if (dir == 0) {
+      if (mf > (a.m_total - vdeg) / BEAMER_ALPHA) dir = 1;
+    } else {
+      if ((int64_t)nf * BEAMER_BETA < a.n) dir = 0;
+    }
+  }
+  if (dir == 1 && !done) c->levels_pull += 1;
+  c->dir = dir;
+  c->nf_next = nf;
+  if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+  __threadfence();
+  c->done = done ? 1 : 0;
+  if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+}
+
+// Early exit shared by both kernels: when the run is already over, make sure
+// the WHILE node stops.
+__device__ __forceinline__ bool bfs_skip(const BfsArgs &a, int want_dir) {
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return true;
+  }
+  return vload(&c->dir) != want_dir;
+}
+
+// Per-thread state of a push level (plain copies, so nothing is read through
+// the kernel-parameter block).
+struct PushCtx {
+  int32_t *label;
+  uint32_t *vis;
+  const int32_t *ro;
+  int32_t *qout;
+  int32_t *qlen_out;
+  int32_t *overflow;
+  int32_t qcap;
+  int32_t level;
+  int64_t mf;
+};
+
+__device__ __forceinline__ void bfs_visit(PushCtx &x, int32_t u) {
+  const uint32_t bit = 1u << (u & 31);
+  uint32_t *wp = x.vis + (u >> 5);
+  bool disc = false;
+  if (!(*wp & bit)) {
+    uint32_t old = atomicOr(wp, bit);
+    disc = !(old & bit);
+  }
+  if (disc) {
+    x.label[u] = x.level + 1;
+    x.mf += x.ro[u + 1] - x.ro[u];
+  }
+  warp_append(disc, u, x.qout, x.qlen_out, x.qcap, x.overflow);
+}
+
+// Expands the edge lists (offsets `off`, targets `tgt`) of a tile of frontier
+// vertices with thread/warp/CTA degree bins.
+__device__ __forceinline__ void expand_tile(PushCtx &x, const int32_t *__restrict__ off,
+                                            const int32_t *__restrict__ tgt, int32_t v, int64_t &insp,
+                                            int32_t *s_scan, int32_t *s_beg, int32_t *s_red, int32_t *s_cta) {
+  const int tid = threadIdx.x, lane = lane_id();
+  int32_t beg = 0, deg = 0;
+  if (v >= 0) {
+    beg = off[v];
+    deg = off[v + 1] - beg;
+    insp += deg;
+  }
+  // CTA bin.
+  while (__syncthreads_or(deg >= BFS_CTA_TH)) {
+    if (deg >= BFS_CTA_TH) s_cta[0] = tid;
+    __syncthreads();
+    if (s_cta[0] == tid) {
+      s_cta[1] = beg;
+      s_cta[2] = beg + deg;
+      deg = 0;
+    }
+    __syncthreads();
+    const int32_t b = s_cta[1], e = s_cta[2];
+    for (int32_t k = b + tid; k < e; k += BFS_NT) bfs_visit(x, tgt[k]);
+  }
+  // Warp bin.
+  for (;;) {
+    unsigned wm = __ballot_sync(FULL, deg >= BFS_WARP_TH);
+    if (!wm) break;
+    const int l = __ffs(wm) - 1;
+    const int32_t b = __shfl_sync(FULL, beg, l), e = __shfl_sync(FULL, beg + deg, l);
+    if (lane == l) deg = 0;
+    for (int32_t k = b + lane; k < e; k += 32) bfs_visit(x, tgt[k]);
+  }
+  // Thread bin: block-wide scan of the remaining degrees, then the CTA walks
+  // the concatenated edge slots; each slot finds its owner by binary search.
+  int32_t total;
+  const int32_t ex = block_exclusive_scan<BFS_NT>(deg, s_red, &total);
+  s_scan[tid] = ex;
+  s_beg[tid] = beg;
+  __syncthreads();
+  for (int32_t k = tid; k < total; k += BFS_NT) {
+    int lo = 0, hi = BFS_NT;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (s_scan[mid] <= k) lo = mid;
+      else hi = mid;
+    }
+    bfs_visit(x, tgt[s_beg[lo] + (k - s_scan[lo])]);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
+  __shared__ int32_t s_scan[BFS_NT], s_beg[BFS_NT], s_red[BFS_NT / 32 + 1], s_cta[4];
+  __shared__ int64_t s_sum[BFS_NT / 32 + 1];
+  if (bfs_skip(a, 0)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
+  int64_t insp = 0, nexp = 0;
+  for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
+    const int64_t i = tile + threadIdx.x;
+    const int32_t v = i < nin ? qin[i] : -1;
+    nexp += v >= 0;
+    expand_tile(x, a.ro, a.ci, v, insp, s_scan, s_beg, s_red, s_cta);
+    if (a.both) expand_tile(x, a.co, a.ri, v, insp, s_scan, s_beg, s_red, s_cta);
+  }
+  const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
+  const int64_t bins = block_sum<BFS_NT>(insp, s_sum);
+  const int64_t bexp = block_sum<BFS_NT>(nexp, s_sum);
+  if (threadIdx.x == 0) {
+    if (bmf) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)bmf);
+    if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
+    if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
+  }
+  if (last_block(&c->blocks_done) && threadIdx.x == 0) bfs_level_end(a);
+}
+
+__global__ void __launch_bounds__(BFS_NT) bfs_pull_kernel(BfsArgs a) {
+  __shared__ int64_t s_sum[BFS_NT / 32 + 1];
+  if (bfs_skip(a, 1)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const int32_t level = vload(&c->level);
+  int32_t *qout = cur ? a.q0 : a.q1;
+  int32_t *qlen_out = &c->qlen[cur ^ 1];
+  const int lane = lane_id();
+  const int64_t nwords = (a.n + 31) >> 5;
+  const int64_t wstride = ((int64_t)gridDim.x * BFS_NT) >> 5;
+  int64_t mf = 0, insp = 0, nexp = 0;
+  for (int64_t w = ((int64_t)blockIdx.x * BFS_NT + threadIdx.x) >> 5; w < nwords; w += wstride) {
+    const uint32_t vw = a.vis[w];
+    if (vw == FULL) continue;
+    const int64_t v = (w << 5) + lane;
+    const bool need = v < a.n && !((vw >> lane) & 1u);
+    bool found = false;
+    int32_t beg = 0, end = 0;
+    if (need) {
+      beg = a.co[v];
+      end = a.co[v + 1];
+      nexp++;
+    }
+    const int32_t lim = min(end, beg + PULL_SERIAL);
+    for (int32_t e = beg; e < lim; e++) {
+      insp++;
+      if (a.label[a.ri[e]] == level) {
+        found = true;
+        break;
+      }
+    }
+    unsigned pend = __ballot_sync(FULL, need && !found && lim < end);
+    while (pend) {
+      const int l = __ffs(pend) - 1;
+      pend &= pend - 1;
+      const int32_t b = __shfl_sync(FULL, lim, l), en = __shfl_sync(FULL, end, l);
+      bool f = false;
+      for (int32_t e0 = b; e0 < en; e0 += 32) {
+        const int32_t e = e0 + lane;
+        const bool hit = e < en && a.label[a.ri[e]] == level;
+        insp += e < en;
+        if (__any_sync(FULL, hit)) {
+          f = true;
+          break;
+        }
+      }
+      if (lane == l) found = f;
+    }
+    const unsigned fm = __ballot_sync(FULL, found);
+    if (fm) {
+      if (lane == 0) a.vis[w] = vw | fm;
+      if (found) {
+        a.label[v] = level + 1;
+        mf += a.ro[v + 1] - a.ro[v];
+      }
+      warp_append(found, (int32_t)v, qout, qlen_out, a.qcap, &c->overflow);
+    }
+  }
+  const int64_t bmf = block_sum<BFS_NT>(mf, s_sum);
+  const int64_t bins = block_sum<BFS_NT>(insp, s_sum);
+  const int64_t bexp = block_sum<BFS_NT>(nexp, s_sum);
+  if (threadIdx.x == 0) {
+    if (bmf) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)bmf);
+    if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
+    if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
+  }
+  if (last_block(&c->blocks_done) && threadIdx.x == 0) bfs_level_end(a);
+}
+
+// labels := -1, visited := 0.
+__global__ void bfs_clear_kernel(int32_t *label, uint32_t *vis, int64_t n) {
+  const int64_t nw = (n + 31) >> 5;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    label[i] = -1;
+    if (i < nw) vis[i] = 0;
+  }
+}
+
+// Seeds the sources (duplicates collapse) and initialises the control block.
+__global__ void bfs_seed_kernel(BfsArgs a, const int32_t *srcs, int32_t nsrc, int32_t iter_cap, int32_t dir0) {
+  __shared__ int64_t s_sum[1024 / 32 + 1];
+  DevCtl *c = a.ctl;
+  int64_t mf = 0;
+  for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
+    const int32_t s = srcs[i];
+    const uint32_t bit = 1u << (s & 31);
+    const uint32_t old = atomicOr(&a.vis[s >> 5], bit);
+    if (!(old & bit)) {
+      a.label[s] = 0;
+      mf += a.ro[s + 1] - a.ro[s];
+      int pos = atomicAdd(&c->qlen[0], 1);
+      if (pos < a.qcap) a.q0[pos] = s;
+      else c->overflow = 1;
+    }
+  }
+  const int64_t t = block_sum<1024>(mf, s_sum);
+  if (threadIdx.x == 0) {
+    c->visited_deg = t;
+    c->level = 0;
+    c->cur = 0;
+    c->dir = dir0;
+    c->iter_cap = iter_cap;
+    c->done = (iter_cap <= 0 || c->overflow) ? 1 : 0;
+    if (c->overflow) c->status = MG_ERR_QUEUE_OVERFLOW;
+  }
+}
+
+}  // namespace mg
+
+extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth, const mg_opts *opts,
+                            mg_stats *stats) {
+  using namespace mg;
+  if (!g || !srcs || nsrc <= 0 || !depth) {
+    mg_set_error("mg_bfs: null argument or nsrc <= 0");
+    return MG_ERR_ARG;
+  }
+  mg_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.directed = 1;
+  if (opts) o = *opts;
+  if (o.direction < MG_DIR_AUTO || o.direction > MG_DIR_PULL) {
+    mg_set_error("mg_bfs: invalid direction %d", o.direction);
+    return MG_ERR_ARG;
+  }
+  for (int32_t i = 0; i < nsrc; i++) {
+    if (srcs[i] < 0 || srcs[i] >= g->n) {
+      mg_set_error("mg_bfs: source %d out of range [0, %lld)", srcs[i], (long long)g->n);
+      return MG_ERR_ARG;
+    }
+  }
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  const bool undirected = o.directed == 0 && !symmetric;
+  if (undirected && !g->has_csc) {
+    mg_set_error("mg_bfs: directed=0 needs the CSC (graph created with MG_GRAPH_NO_CSC)");
+    return MG_ERR_UNSUPPORTED;
+  }
+  MG_TRY(graph_enter(g));
+  const int64_t n = g->n;
+  int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)n) : n;
+  qcap64 = std::max<int64_t>(1, std::min<int64_t>(qcap64, n));
+  const int32_t qcap = (int32_t)qcap64;
+  const int64_t nwords = (n + 31) / 32;
+  const size_t need = Carve::need({sizeof(int32_t) * (size_t)n, sizeof(uint32_t) * (size_t)nwords,
+                                   sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
+                                   sizeof(int32_t) * (size_t)nsrc});
+  MG_TRY(ws_reserve(g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  int32_t *label_ws = cv.take<int32_t>(n);
+  uint32_t *vis = cv.take<uint32_t>(nwords);
+  int32_t *q0 = cv.take<int32_t>(qcap);
+  int32_t *q1 = cv.take<int32_t>(qcap);
+  int32_t *dsrc = cv.take<int32_t>(nsrc);
+  int32_t *label = o.device_output ? depth : label_ws;
+  cudaStream_t s = g->stream;
+
+  BfsArgs a;
+  a.ro = g->ro;
+  a.ci = g->ci;
+  a.co = g->has_csc ? g->co : g->ro;
+  a.ri = g->has_csc ? g->ri : g->ci;
+  a.label = label;
+  a.vis = vis;
+  a.q0 = q0;
+  a.q1 = q1;
+  a.qcap = qcap;
+  a.mode = o.direction;
+  a.can_pull = g->has_csc && !undirected;
+  a.both = undirected ? 1 : 0;
+  a.n = n;
+  a.m_total = g->m;
+  a.ctl = g->ctl;
+  a.h = 0;
+  a.use_cond = 0;
+
+  const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
+  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  bfs_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(label, vis, n);
+  bfs_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap, 0);
+  MG_CUDA_TRY(cudaGetLastError());
+
+  const int grid = g->num_sms * 4;
+  const bool use_graph = o.use_graph >= 0;
+  struct Sig {
+    BfsArgs a;
+    int grid;
+  } sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.a = a;
+  sig.grid = grid;
+  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+    BfsArgs b = a;
+    b.h = h;
+    b.use_cond = use_cond;
+    bfs_push_kernel<<<grid, BFS_NT, 0, st>>>(b);
+    bfs_pull_kernel<<<grid, BFS_NT, 0, st>>>(b);
+  };
+  MG_TRY(run_loop(g, SLOT_BFS, &sig, sizeof(sig), use_graph, body, n + 2));
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  if (!o.device_output) MG_TRY(copy_out(g, depth, label, sizeof(int32_t) * n, 0));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = hc.visited_deg;
+    stats->edges_inspected = hc.edges_inspected;
+    stats->bytes_compulsory = 4 * hc.edges_inspected + 16 * hc.vertices_expanded + 4 * n +
+                              (int64_t)hc.levels_pull * ((n + 7) / 8);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+    stats->status_detail = hc.levels_pull;
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_bfs: frontier exceeded queue capacity %d", qcap);
+    return (mg_status)hc.status;
+  }
+  return MG_OK;
+}

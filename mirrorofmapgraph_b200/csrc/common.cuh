@@ -1,0 +1,111 @@
+// common.cuh -- device helpers shared by the engine's kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "mg_internal.h"
+
+namespace mg {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+  const int l = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(FULL, v, o);
+    if (l >= o) v += t;
+  }
+  return v;
+}
+
+// Block-wide exclusive scan for blockDim.x == NT (multiple of 32, <= 1024).
+// `smem` must hold NT/32 + 1 elements. Returns the exclusive prefix; *total gets the sum.
+template <int NT, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T *smem, T *total) {
+  const int l = lane_id(), w = warp_id();
+  T inc = warp_inclusive_scan(v);
+  if (l == 31) smem[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T s = l < NT / 32 ? smem[l] : T(0);
+    T si = warp_inclusive_scan(s);
+    if (l < NT / 32) smem[l] = si - s;
+    if (l == NT / 32 - 1) smem[NT / 32] = si;
+  }
+  __syncthreads();
+  T r = smem[w] + inc - v;
+  *total = smem[NT / 32];
+  __syncthreads();
+  return r;
+}
+
+template <int NT, typename T>
+__device__ __forceinline__ T block_sum(T v, T *smem) {
+  const int l = lane_id(), w = warp_id();
+  v = warp_sum(v);
+  if (l == 0) smem[w] = v;
+  __syncthreads();
+  T r = T(0);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NT / 32; i++) r += smem[i];
+  }
+  __syncthreads();
+  return r;  // valid in thread 0 only
+}
+
+// Last-block-done election: every CTA calls this once after finishing its work
+// (all threads). Returns true in every thread of the last CTA to arrive. Writes
+// made by any CTA before its call are visible to the last CTA afterwards.
+__device__ __forceinline__ bool last_block(unsigned *counter) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+// Warp-aggregated append of `item` to `queue` (capacity `cap`) for every active
+// lane with `pred` set; the queue length lives at *len. Lanes whose slot lands
+// past the capacity set *overflow instead of writing.
+__device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t *queue, int32_t *len,
+                                            int32_t cap, int32_t *overflow) {
+  const unsigned active = __activemask();
+  const unsigned pm = __ballot_sync(active, pred);
+  if (pm == 0) return;
+  const int leader = __ffs(active) - 1;
+  int base = 0;
+  if (lane_id() == leader) base = atomicAdd(len, __popc(pm));
+  base = __shfl_sync(active, base, leader);
+  if (pred) {
+    int pos = base + __popc(pm & lanemask_lt());
+    if (pos < cap) queue[pos] = item;
+    else *overflow = 1;
+  }
+}
+
+__device__ __forceinline__ int32_t ld_nc(const int32_t *p) { return __ldg(p); }
+
+}  // namespace mg

@@ -1,0 +1,458 @@
+// host_io.cpp -- host-side ingest (Matrix Market) and seeded synthetic graph
+// generators. Plain C++17 + OpenMP; no CUDA.
+//
+// Generators are counter-based: every random draw is splitmix64 of a key derived
+// from (seed, stream) mixed with the draw's index, so the graph is a pure
+// function of the seed, independent of thread count and scheduling.
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <omp.h>
+
+#include "mapgraph_b200_io.h"
+#include "mg_internal.h"
+
+namespace {
+
+inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Stream keys: one independent random sequence per purpose.
+enum : uint64_t { S_SRC = 1, S_DST = 2, S_WEIGHT = 3, S_RMAT = 4, S_LONG = 5, S_REDRAW = 6 };
+
+inline uint64_t stream_key(uint64_t seed, uint64_t stream) {
+  return splitmix64(seed * 0xD1B54A32D192ED03ull + stream * 0x632BE59BD9B4E019ull);
+}
+inline uint64_t draw(uint64_t key, uint64_t idx) { return splitmix64(key ^ (idx * 0x9E3779B97F4A7C15ull)); }
+inline double unit(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }  // [0,1)
+
+struct WeightGen {
+  int32_t kind;
+  double p0, p1;
+  uint64_t key;
+  bool is_float() const { return kind == MG_W_LOGNORMAL; }
+  int32_t ival(uint64_t idx) const {
+    int64_t lo = (int64_t)p0, hi = (int64_t)p1;
+    return (int32_t)(lo + (int64_t)(draw(key, idx) % (uint64_t)(hi - lo + 1)));
+  }
+  float fval(uint64_t idx) const {
+    // Box-Muller from two independent draws.
+    double u1 = unit(draw(key, 2 * idx)), u2 = unit(draw(key, 2 * idx + 1));
+    if (u1 < 1e-300) u1 = 1e-300;
+    double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    return (float)std::exp(p0 + p1 * z);
+  }
+};
+
+bool valid_weights(int32_t wkind, double p0, double p1) {
+  if (wkind == MG_W_NONE) return true;
+  if (wkind == MG_W_UNIFORM_INT) return p0 <= p1 && p0 >= -2147483648.0 && p1 <= 2147483647.0;
+  if (wkind == MG_W_LOGNORMAL) return p1 >= 0.0;
+  return false;
+}
+
+// COO edge list with one weight slot.
+struct Coo {
+  std::vector<int32_t> src, dst, wi;
+  std::vector<float> wf;
+};
+
+// Builds a CSR from COO. Rows come out sorted by (column, weight) when
+// canonical != 0 (generated graphs), or in COO order (stable by row) otherwise
+// (file ingest, matching the reference's std::stable_sort by row).
+mg_status coo_to_csr(int64_t n, Coo &coo, int32_t wkind, bool canonical, mg_host_csr *out) {
+  const int64_t m = (int64_t)coo.src.size();
+  if (n < 0 || n > INT32_MAX - 1 || m > INT32_MAX) return MG_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->n = n;
+  out->m = m;
+  out->row_offsets = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(n + 1));
+  out->col_idx = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1));
+  bool has_i = wkind == MG_W_UNIFORM_INT, has_f = wkind == MG_W_LOGNORMAL;
+  if (has_i) out->weights_i32 = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1));
+  if (has_f) out->weights_f32 = (float *)std::malloc(sizeof(float) * (size_t)std::max<int64_t>(m, 1));
+  if (!out->row_offsets || !out->col_idx || (has_i && !out->weights_i32) || (has_f && !out->weights_f32)) {
+    mg_host_csr_free(out);
+    return MG_ERR_OOM;
+  }
+  std::vector<int64_t> cnt((size_t)n + 1, 0);
+  if (canonical) {
+    std::atomic<int64_t> *acnt = reinterpret_cast<std::atomic<int64_t> *>(cnt.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < m; e++) acnt[coo.src[e]].fetch_add(1, std::memory_order_relaxed);
+  } else {
+    for (int64_t e = 0; e < m; e++) cnt[coo.src[e]]++;
+  }
+  int64_t run = 0;
+  for (int64_t v = 0; v < n; v++) {
+    int64_t c = cnt[v];
+    out->row_offsets[v] = (int32_t)run;
+    cnt[v] = run;
+    run += c;
+  }
+  out->row_offsets[n] = (int32_t)run;
+  if (canonical) {
+    std::vector<int64_t> slot((size_t)m);
+    std::atomic<int64_t> *cur = reinterpret_cast<std::atomic<int64_t> *>(cnt.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < m; e++) slot[e] = cur[coo.src[e]].fetch_add(1, std::memory_order_relaxed);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < m; e++) {
+      out->col_idx[slot[e]] = coo.dst[e];
+      if (has_i) out->weights_i32[slot[e]] = coo.wi[e];
+      if (has_f) out->weights_f32[slot[e]] = coo.wf[e];
+    }
+    // Canonical row order: sort each row by (column, weight).
+#pragma omp parallel
+    {
+      std::vector<std::pair<int32_t, int32_t>> bi;
+      std::vector<std::pair<int32_t, float>> bf;
+#pragma omp for schedule(dynamic, 4096)
+      for (int64_t v = 0; v < n; v++) {
+        int64_t b = out->row_offsets[v], e = out->row_offsets[v + 1];
+        if (e - b < 2) continue;
+        if (has_f) {
+          bf.clear();
+          for (int64_t k = b; k < e; k++) bf.emplace_back(out->col_idx[k], out->weights_f32[k]);
+          std::sort(bf.begin(), bf.end());
+          for (int64_t k = b; k < e; k++) { out->col_idx[k] = bf[k - b].first; out->weights_f32[k] = bf[k - b].second; }
+        } else if (has_i) {
+          bi.clear();
+          for (int64_t k = b; k < e; k++) bi.emplace_back(out->col_idx[k], out->weights_i32[k]);
+          std::sort(bi.begin(), bi.end());
+          for (int64_t k = b; k < e; k++) { out->col_idx[k] = bi[k - b].first; out->weights_i32[k] = bi[k - b].second; }
+        } else {
+          std::sort(out->col_idx + b, out->col_idx + e);
+        }
+      }
+    }
+  } else {
+    for (int64_t e = 0; e < m; e++) {
+      int64_t s = cnt[coo.src[e]]++;
+      out->col_idx[s] = coo.dst[e];
+      if (has_i) out->weights_i32[s] = coo.wi[e];
+      if (has_f) out->weights_f32[s] = coo.wf[e];
+    }
+  }
+  return MG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mg_host_csr_free(mg_host_csr *g) {
+  if (!g) return;
+  std::free(g->row_offsets);
+  std::free(g->col_idx);
+  std::free(g->weights_i32);
+  std::free(g->weights_f32);
+  std::memset(g, 0, sizeof(*g));
+}
+
+mg_status mg_gen_er(int64_t n, int64_t m, uint64_t seed, int32_t wkind, double p0, double p1,
+                    mg_host_csr *out) {
+  if (!out || n < 2 || m < 0 || m > INT32_MAX || n > INT32_MAX - 1 || !valid_weights(wkind, p0, p1)) {
+    mg_set_error("mg_gen_er: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  Coo coo;
+  coo.src.resize(m);
+  coo.dst.resize(m);
+  WeightGen wg{wkind, p0, p1, stream_key(seed, S_WEIGHT)};
+  if (wkind == MG_W_UNIFORM_INT) coo.wi.resize(m);
+  if (wkind == MG_W_LOGNORMAL) coo.wf.resize(m);
+  const uint64_t ks = stream_key(seed, S_SRC), kd = stream_key(seed, S_DST), kr = stream_key(seed, S_REDRAW);
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < m; e++) {
+    int64_t u = (int64_t)(draw(ks, e) % (uint64_t)n);
+    int64_t v = (int64_t)(draw(kd, e) % (uint64_t)n);
+    for (uint64_t t = 1; v == u; t++) v = (int64_t)(draw(kr, (uint64_t)e * 64 + t) % (uint64_t)n);
+    coo.src[e] = (int32_t)u;
+    coo.dst[e] = (int32_t)v;
+    if (wkind == MG_W_UNIFORM_INT) coo.wi[e] = wg.ival(e);
+    if (wkind == MG_W_LOGNORMAL) coo.wf[e] = wg.fval(e);
+  }
+  return coo_to_csr(n, coo, wkind, true, out);
+}
+
+mg_status mg_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                      uint64_t seed, int32_t symmetrize, int32_t wkind, double p0, double p1,
+                      mg_host_csr *out) {
+  if (!out || scale < 1 || scale > 30 || edge_factor < 1 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0 ||
+      !valid_weights(wkind, p0, p1)) {
+    mg_set_error("mg_gen_rmat: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  const int64_t n = (int64_t)1 << scale;
+  const int64_t mg = n * (int64_t)edge_factor;
+  if (mg * (symmetrize ? 2 : 1) > INT32_MAX) {
+    mg_set_error("mg_gen_rmat: edge count exceeds int32");
+    return MG_ERR_ARG;
+  }
+  const uint64_t kq = stream_key(seed, S_RMAT);
+  WeightGen wg{wkind, p0, p1, stream_key(seed, S_WEIGHT)};
+  // Pass 1: endpoints of every generated edge (self-loops flagged by u == v).
+  std::vector<int32_t> gu(mg), gv(mg);
+  const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < mg; e++) {
+    uint32_t u = 0, v = 0;
+    for (int l = 0; l < scale; l++) {
+      double r = unit(draw(kq, (uint64_t)e * (uint64_t)scale + (uint64_t)l));
+      uint32_t bu, bv;
+      if (r < a) { bu = 0; bv = 0; }
+      else if (r < ab) { bu = 0; bv = 1; }
+      else if (r < abc) { bu = 1; bv = 0; }
+      else { bu = 1; bv = 1; }
+      u = (u << 1) | bu;
+      v = (v << 1) | bv;
+    }
+    gu[e] = (int32_t)u;
+    gv[e] = (int32_t)v;
+  }
+  // Pass 2: compact away self-loops (prefix count per block keeps it deterministic).
+  const int nt = omp_get_max_threads();
+  std::vector<int64_t> keep(nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    int t = omp_get_thread_num();
+    int64_t lo = mg * t / nt, hi = mg * (t + 1) / nt, k = 0;
+    for (int64_t e = lo; e < hi; e++) k += gu[e] != gv[e];
+    keep[t + 1] = k;
+  }
+  for (int t = 0; t < nt; t++) keep[t + 1] += keep[t];
+  const int64_t mk = keep[nt];
+  const int64_t mult = symmetrize ? 2 : 1;
+  Coo coo;
+  coo.src.resize(mk * mult);
+  coo.dst.resize(mk * mult);
+  if (wkind == MG_W_UNIFORM_INT) coo.wi.resize(mk * mult);
+  if (wkind == MG_W_LOGNORMAL) coo.wf.resize(mk * mult);
+#pragma omp parallel num_threads(nt)
+  {
+    int t = omp_get_thread_num();
+    int64_t lo = mg * t / nt, hi = mg * (t + 1) / nt, k = keep[t];
+    for (int64_t e = lo; e < hi; e++) {
+      if (gu[e] == gv[e]) continue;
+      int64_t s = k * mult;
+      coo.src[s] = gu[e];
+      coo.dst[s] = gv[e];
+      if (symmetrize) { coo.src[s + 1] = gv[e]; coo.dst[s + 1] = gu[e]; }
+      if (wkind == MG_W_UNIFORM_INT) { int32_t w = wg.ival(e); coo.wi[s] = w; if (symmetrize) coo.wi[s + 1] = w; }
+      if (wkind == MG_W_LOGNORMAL) { float w = wg.fval(e); coo.wf[s] = w; if (symmetrize) coo.wf[s + 1] = w; }
+      k++;
+    }
+  }
+  std::vector<int32_t>().swap(gu);
+  std::vector<int32_t>().swap(gv);
+  return coo_to_csr(n, coo, wkind, true, out);
+}
+
+mg_status mg_gen_lattice(int32_t rows, int32_t cols, double longrange_frac, uint64_t seed,
+                         int32_t wkind, double p0, double p1, mg_host_csr *out) {
+  if (!out || rows < 1 || cols < 1 || longrange_frac < 0 || !valid_weights(wkind, p0, p1)) {
+    mg_set_error("mg_gen_lattice: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  const int64_t n = (int64_t)rows * cols;
+  const int64_t und = (int64_t)rows * (cols - 1) + (int64_t)(rows - 1) * cols;  // undirected lattice edges
+  const int64_t nlong = (int64_t)std::llround(longrange_frac * 2.0 * (double)und);
+  if (n > INT32_MAX - 1 || 2 * (und + nlong) > INT32_MAX || (nlong > 0 && n < 2)) {
+    mg_set_error("mg_gen_lattice: size exceeds int32");
+    return MG_ERR_ARG;
+  }
+  const int64_t mu = und + nlong;  // undirected edges, each emitted in both directions
+  Coo coo;
+  coo.src.resize(2 * mu);
+  coo.dst.resize(2 * mu);
+  if (wkind == MG_W_UNIFORM_INT) coo.wi.resize(2 * mu);
+  if (wkind == MG_W_LOGNORMAL) coo.wf.resize(2 * mu);
+  WeightGen wg{wkind, p0, p1, stream_key(seed, S_WEIGHT)};
+  const int64_t horiz = (int64_t)rows * (cols - 1);
+  const uint64_t kl = stream_key(seed, S_LONG), kr = stream_key(seed, S_REDRAW);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < mu; k++) {
+    int64_t u, v;
+    if (k < horiz) {
+      int64_t r = k / (cols - 1), c = k % (cols - 1);
+      u = r * cols + c;
+      v = u + 1;
+    } else if (k < und) {
+      int64_t q = k - horiz;
+      int64_t r = q / cols, c = q % cols;
+      u = r * cols + c;
+      v = u + cols;
+    } else {
+      int64_t j = k - und;
+      u = (int64_t)(draw(kl, 2 * (uint64_t)j) % (uint64_t)n);
+      v = (int64_t)(draw(kl, 2 * (uint64_t)j + 1) % (uint64_t)n);
+      for (uint64_t t = 1; v == u; t++) v = (int64_t)(draw(kr, (uint64_t)j * 64 + t) % (uint64_t)n);
+    }
+    coo.src[2 * k] = (int32_t)u;
+    coo.dst[2 * k] = (int32_t)v;
+    coo.src[2 * k + 1] = (int32_t)v;
+    coo.dst[2 * k + 1] = (int32_t)u;
+    if (wkind == MG_W_UNIFORM_INT) { int32_t w = wg.ival(k); coo.wi[2 * k] = w; coo.wi[2 * k + 1] = w; }
+    if (wkind == MG_W_LOGNORMAL) { float w = wg.fval(k); coo.wf[2 * k] = w; coo.wf[2 * k + 1] = w; }
+  }
+  return coo_to_csr(n, coo, wkind, true, out);
+}
+
+mg_status mg_read_market(const char *path, int32_t undirected, mg_host_csr *out) {
+  if (!path || !out) {
+    mg_set_error("mg_read_market: null argument");
+    return MG_ERR_ARG;
+  }
+  int fd = open(path, O_RDONLY);
+  if (fd < 0) {
+    mg_set_error("mg_read_market: cannot open %s: %s", path, std::strerror(errno));
+    return MG_ERR_ARG;
+  }
+  struct stat st;
+  if (fstat(fd, &st) != 0) {
+    close(fd);
+    mg_set_error("mg_read_market: cannot stat %s", path);
+    return MG_ERR_ARG;
+  }
+  size_t len = (size_t)st.st_size;
+  std::vector<char> buf(len + 1);
+  size_t got = 0;
+  while (got < len) {
+    ssize_t r = read(fd, buf.data() + got, len - got);
+    if (r <= 0) break;
+    got += (size_t)r;
+  }
+  close(fd);
+  buf[got] = '\0';
+  const char *p = buf.data(), *end = buf.data() + got;
+  int64_t n = -1, declared = 0, read_edges = 0;
+  Coo coo;
+  std::vector<double> vals;
+  while (p < end) {
+    // Blank lines are skipped like the reference's fscanf("%[^\n]\n").
+    const char *eol = (const char *)std::memchr(p, '\n', (size_t)(end - p));
+    if (!eol) eol = end;
+    const char *q = p;
+    while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) q++;
+    if (q == eol) { p = eol + 1; continue; }
+    if (*p == '%') { p = eol + 1; continue; }
+    std::string line(p, eol);
+    p = eol + 1;
+    if (n < 0) {
+      long long rx, cy, ne;
+      if (std::sscanf(line.c_str(), "%lld %lld %lld", &rx, &cy, &ne) != 3) {
+        mg_set_error("mg_read_market: invalid problem description");
+        return MG_ERR_ARG;
+      }
+      if (rx != cy) {
+        mg_set_error("mg_read_market: not square (%lld, %lld)", rx, cy);
+        return MG_ERR_ARG;
+      }
+      if (rx < 0 || rx > INT32_MAX - 1 || ne < 0 || ne * (undirected ? 2 : 1) > INT32_MAX) {
+        mg_set_error("mg_read_market: sizes exceed int32");
+        return MG_ERR_ARG;
+      }
+      n = rx;
+      declared = ne;
+      coo.src.reserve(ne * (undirected ? 2 : 1));
+      coo.dst.reserve(ne * (undirected ? 2 : 1));
+      vals.reserve(ne * (undirected ? 2 : 1));
+      continue;
+    }
+    if (read_edges >= declared) {
+      mg_set_error("mg_read_market: more than %lld entries", (long long)declared);
+      return MG_ERR_ARG;
+    }
+    long long r, c;
+    double v = 1.0;
+    int nr = std::sscanf(line.c_str(), "%lld %lld %lf", &r, &c, &v);
+    if (nr != 2 && nr != 3) {
+      mg_set_error("mg_read_market: badly formed entry %lld", (long long)read_edges);
+      return MG_ERR_ARG;
+    }
+    if (r < 1 || r > n || c < 1 || c > n) {
+      mg_set_error("mg_read_market: entry %lld out of range", (long long)read_edges);
+      return MG_ERR_ARG;
+    }
+    coo.src.push_back((int32_t)(r - 1));
+    coo.dst.push_back((int32_t)(c - 1));
+    vals.push_back(v);
+    if (undirected) {
+      coo.src.push_back((int32_t)(c - 1));
+      coo.dst.push_back((int32_t)(r - 1));
+      vals.push_back(v);
+    }
+    read_edges++;
+  }
+  if (n < 0) {
+    mg_set_error("mg_read_market: no graph found");
+    return MG_ERR_ARG;
+  }
+  if (read_edges != declared) {
+    mg_set_error("mg_read_market: only %lld/%lld entries read", (long long)read_edges, (long long)declared);
+    return MG_ERR_ARG;
+  }
+  const size_t mm = coo.src.size();
+  coo.wi.resize(mm);
+  for (size_t e = 0; e < mm; e++) coo.wi[e] = (int32_t)vals[e];
+  mg_status st2 = coo_to_csr(n, coo, MG_W_UNIFORM_INT, false, out);
+  if (st2 != MG_OK) return st2;
+  // Float view of the same values (the PageRank program reads Value = float).
+  std::vector<float> vf(mm);
+  for (size_t e = 0; e < mm; e++) vf[e] = (float)vals[e];
+  out->weights_f32 = (float *)std::malloc(sizeof(float) * std::max<size_t>(mm, 1));
+  if (!out->weights_f32) {
+    mg_host_csr_free(out);
+    return MG_ERR_OOM;
+  }
+  // Re-run the stable row placement for the float values.
+  std::vector<int64_t> cur((size_t)n + 1);
+  for (int64_t v = 0; v <= n; v++) cur[v] = out->row_offsets[v];
+  for (size_t e = 0; e < mm; e++) out->weights_f32[cur[coo.src[e]]++] = vf[e];
+  return MG_OK;
+}
+
+mg_status mg_host_csr_to_csc(int64_t n, int64_t m, const int32_t *row_offsets, const int32_t *col_idx,
+                             int32_t *col_offsets, int32_t *row_idx, int32_t *perm) {
+  if (n < 0 || m < 0 || !row_offsets || !col_offsets || (m > 0 && (!col_idx || !row_idx || !perm))) {
+    mg_set_error("mg_host_csr_to_csc: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  std::vector<int64_t> cnt((size_t)n + 1, 0);
+  for (int64_t e = 0; e < m; e++) cnt[col_idx[e]]++;
+  int64_t run = 0;
+  for (int64_t v = 0; v < n; v++) {
+    int64_t c = cnt[v];
+    col_offsets[v] = (int32_t)run;
+    cnt[v] = run;
+    run += c;
+  }
+  col_offsets[n] = (int32_t)run;
+  for (int64_t v = 0; v < n; v++) {
+    for (int64_t e = row_offsets[v]; e < row_offsets[v + 1]; e++) {
+      int64_t s = cnt[col_idx[e]]++;
+      row_idx[s] = (int32_t)v;
+      perm[s] = (int32_t)e;
+    }
+  }
+  return MG_OK;
+}
+
+}  // extern "C"

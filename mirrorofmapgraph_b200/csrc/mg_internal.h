@@ -1,0 +1,118 @@
+// mg_internal.h -- shared host-side definitions of the engine (not installed).
+#pragma once
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <initializer_list>
+#include <vector>
+
+#include "mapgraph_b200.h"
+
+// Thread-local error detail behind mg_last_error().
+void mg_set_error(const char *fmt, ...);
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+
+#define MG_CUDA_TRY(expr)                                                                        \
+  do {                                                                                           \
+    cudaError_t _e = (expr);                                                                     \
+    if (_e != cudaSuccess) {                                                                     \
+      mg_set_error("%s:%d: %s failed: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(_e));  \
+      return _e == cudaErrorMemoryAllocation ? MG_ERR_OOM : MG_ERR_CUDA;                         \
+    }                                                                                            \
+  } while (0)
+
+#define MG_TRY(expr)                 \
+  do {                               \
+    mg_status _s = (expr);           \
+    if (_s != MG_OK) return _s;      \
+  } while (0)
+
+// Device control block of one run: frontier sizes, level, direction and the
+// counters the engine reports. Lives in device memory; a mapped/pinned mirror is
+// read back once at the end of a run.
+struct DevCtl {
+  int32_t qlen[2];           // frontier sizes: [cur & 1] is the input of the current level
+  int32_t level;             // current iteration
+  int32_t dir;               // BFS: 0 push, 1 pull
+  int32_t done;              // 1 when the loop must stop
+  int32_t status;            // mg_status raised on the device (queue overflow, ...)
+  int32_t iter_cap;          // stop after this many iterations
+  uint32_t blocks_done;      // last-block-done counter of the current kernel
+  int32_t cur;               // ping-pong selector of the frontier queues
+  int32_t nf_next;           // vertices in the next frontier
+  int64_t mf_next;           // out-edges of the next frontier (push/pull heuristic)
+  int64_t visited_deg;       // sum of out-degrees of every vertex reached so far
+  int64_t edges_inspected;   // edges read by the expansion kernels
+  int64_t vertices_expanded; // frontier vertices processed
+  int64_t vertices_updated;  // vertices whose value changed
+  double dsum[4];            // FP64 reductions (PageRank residual, dangling mass, ...)
+  double dprev[4];           // FP64 values of the previous iteration
+  int32_t levels_pull;       // levels run bottom-up
+  int32_t overflow;          // set by a kernel whose frontier append ran past capacity
+  int32_t body_iters;        // WHILE-body executions so far (loop guard)
+  int32_t pad;
+};
+
+// Reusable device workspace of a graph, grown on demand.
+struct Workspace {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct mg_graph {
+  int device = 0;
+  int64_t n = 0, m = 0;
+  uint32_t flags = 0;
+  mg_dtype vtype = MG_DTYPE_NONE;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  // CSR
+  int32_t *ro = nullptr, *ci = nullptr;
+  void *vals = nullptr;
+  // CSC (aliases the CSR when symmetric)
+  int32_t *co = nullptr, *ri = nullptr, *perm = nullptr;
+  void *cvals = nullptr;
+  bool has_csc = false, csc_owned = false;
+  // per-vertex out-degree sum helpers
+  int64_t max_outdeg = 0;
+  // ragged batch
+  std::vector<int64_t> vbase;
+  // workspaces
+  Workspace ws_main, ws_aux;
+  DevCtl *ctl = nullptr;       // device control block
+  DevCtl *ctl_host = nullptr;  // pinned host mirror
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  void *cache = nullptr;       // cached executable loop graphs (engine.cu)
+};
+
+// Grows a workspace to at least `bytes` (contents are not preserved).
+mg_status ws_reserve(Workspace &w, size_t bytes);
+
+// Carves aligned sub-buffers out of a workspace.
+struct Carve {
+  char *base;
+  size_t off = 0;
+  explicit Carve(void *p) : base((char *)p) {}
+  template <typename T>
+  T *take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T *p = (T *)(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+  static size_t need(std::initializer_list<size_t> sizes) {
+    size_t off = 0;
+    for (size_t s : sizes) off = ((off + 255) & ~(size_t)255) + s;
+    return off + 256;
+  }
+};
+
+// Makes the graph's device current; returns MG_ERR_CUDA on failure.
+mg_status graph_enter(mg_graph *g);
+
+// Copies a device int32 array into a host or device destination.
+mg_status copy_out(mg_graph *g, void *dst, const void *src, size_t bytes, int device_output);
+#endif  // __CUDACC__

@@ -1,0 +1,172 @@
+"""Host-side logic without a GPU: the C-ABI library loads and exports every
+declared symbol, generators are deterministic, ingest matches the reference's
+semantics, the reference-shaped API validates its inputs, and compute calls fail
+loudly (no CPU fallback) when there is no device."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+import mirrorofmapgraph_b200 as mg
+from mirrorofmapgraph_b200 import _lib as L
+from conftest import ROOT
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(mg_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load()
+    declared = _declared_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(L.SIGNATURES) == declared
+
+
+def test_status_strings_and_version():
+    lib = L.load()
+    for st in range(8):
+        assert lib.mg_status_string(st).decode().startswith("MG_")
+    assert b"sm_100a" in lib.mg_version()
+
+
+@pytest.mark.skipif(mg.device_count() > 0, reason="checks the no-device path")
+def test_no_device_fails_loudly():
+    g = mg.gen_er(16, 40, 1)
+    with pytest.raises(mg.MapGraphError) as e:
+        mg.Graph(g.row_offsets, g.col_idx)
+    assert e.value.status == L.MG_ERR_NO_DEVICE
+
+
+def test_null_arguments_are_rejected():
+    lib = L.load()
+    out = C.c_void_p()
+    assert lib.mg_graph_create(None, None, None, 0, 4, 0, 0, C.byref(out)) == L.MG_ERR_ARG
+    assert lib.mg_graph_create(None, None, None, 0, -1, 0, 0, C.byref(out)) == L.MG_ERR_ARG
+    assert lib.mg_bfs(None, None, 1, None, None, None) == L.MG_ERR_ARG
+    assert lib.mg_graph_destroy(None) == L.MG_OK
+
+
+def test_generators_are_deterministic():
+    a = mg.gen_rmat(12, 8, 99, weights="int", p0=1, p1=255)
+    b = mg.gen_rmat(12, 8, 99, weights="int", p0=1, p1=255)
+    assert (a.row_offsets == b.row_offsets).all() and (a.col_idx == b.col_idx).all()
+    assert (a.weights_i32 == b.weights_i32).all()
+    c = mg.gen_rmat(12, 8, 100, weights="int", p0=1, p1=255)
+    assert not (a.col_idx.size == c.col_idx.size and (a.col_idx == c.col_idx).all())
+
+
+def test_er_counts_and_ranges():
+    g = mg.gen_er(4096, 65536, 5, weights="int", p0=1, p1=64)
+    assert g.n == 4096 and g.m == 65536
+    rows = np.repeat(np.arange(g.n), np.diff(g.row_offsets))
+    assert (rows != g.col_idx).all(), "self-loops must be redrawn"
+    assert g.weights_i32.min() >= 1 and g.weights_i32.max() <= 64
+
+
+def _edge_multiset(ro, ci, w=None):
+    rows = np.repeat(np.arange(ro.size - 1), np.diff(ro))
+    keys = [rows, ci] + ([w] if w is not None else [])
+    return np.lexsort(keys[::-1]), rows
+
+
+def test_rmat_symmetrised_is_its_own_transpose():
+    g = mg.gen_rmat(10, 16, 3, symmetrize=True, weights="int", p0=1, p1=255)
+    rows = np.repeat(np.arange(g.n), np.diff(g.row_offsets)).astype(np.int64)
+    fw = np.stack([rows, g.col_idx, g.weights_i32])
+    bw = np.stack([g.col_idx, rows, g.weights_i32])
+    fw = fw[:, np.lexsort(fw[::-1])]
+    bw = bw[:, np.lexsort(bw[::-1])]
+    assert (fw == bw).all()
+    assert (rows != g.col_idx).all()
+    assert g.m % 2 == 0 and g.m <= 2 * 16 * 1024
+
+
+def test_lattice_shape():
+    g = mg.gen_lattice(64, 32, 0.001, 4, weights="int", p0=1, p1=1000)
+    und = 64 * 31 + 63 * 32
+    nlong = round(0.001 * 2 * und)
+    assert g.n == 64 * 32 and g.m == 2 * (und + nlong)
+    deg = np.diff(g.row_offsets)
+    assert deg[0] >= 2  # corner
+
+
+def test_csr_to_csc_is_stable(tmp_path):
+    g = mg.gen_er(200, 900, 8)
+    co, ri, perm = mg.csr_to_csc(g)
+    co2, ri2, perm2 = oracle.csc_of(g.row_offsets, g.col_idx)
+    assert (co == co2).all() and (ri == ri2).all() and (perm == perm2).all()
+
+
+def test_market_reader_semantics(tmp_path, mtx_fixtures):
+    # Round trip of the chesapeake edge list through a file written with comments,
+    # blank lines and pattern (value-less) entries.
+    d = mtx_fixtures["chesapeake"]
+    ro, ci = np.array(d["row_offsets"]), np.array(d["col_idx"])
+    rows = np.repeat(np.arange(ro.size - 1), np.diff(ro))
+    p = tmp_path / "g.mtx"
+    with open(p, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern symmetric\n% comment\n\n")
+        f.write(f"{d['n']} {d['n']} {ci.size}\n")
+        for r, c in zip(rows, ci):
+            f.write(f"{r + 1} {c + 1}\n")
+    g = mg.read_market(str(p))
+    assert (g.row_offsets == ro).all() and (g.col_idx == ci).all() and (g.weights_i32 == 1).all()
+    gu = mg.read_market(str(p), undirected=True)
+    assert gu.m == 2 * ci.size
+    # values are read as double and truncated for int32 (market.cuh:122-126)
+    q = tmp_path / "v.mtx"
+    q.write_text("%%MatrixMarket matrix coordinate real general\n3 3 3\n1 2 2.7\n2 3 -1.5\n3 1 4\n")
+    h = mg.read_market(str(q))
+    assert h.weights_i32.tolist() == [2, -1, 4]
+    assert np.allclose(h.weights_f32, [2.7, -1.5, 4.0])
+
+
+@pytest.mark.parametrize("text", [
+    "",                                             # no graph
+    "%%MatrixMarket\n3 4 1\n1 2\n",                 # not square
+    "%%MatrixMarket\n3 3 2\n1 2\n",                 # truncated
+    "%%MatrixMarket\n3 3 1\n1 2\n2 3\n",            # too many entries
+    "%%MatrixMarket\n3 3 1\n1 9\n",                 # out of range
+    "%%MatrixMarket\n3 3 1\nx y\n",                 # malformed
+])
+def test_market_reader_rejects_malformed(tmp_path, text):
+    p = tmp_path / "bad.mtx"
+    p.write_text(text)
+    with pytest.raises(RuntimeError):
+        mg.read_market(str(p))
+
+
+def test_config_registry():
+    cfg = mg.Config(mg.bfs)
+    assert cfg.getParameter("src") == 1 and cfg.getParameter("threshold") == 10000
+    cfg.parseParameterString("src=5 directed=0,iter_num=3")
+    assert (cfg.getParameter("src"), cfg.getParameter("directed"), cfg.getParameter("iter_num")) == (5, 0, 3)
+    with pytest.raises(KeyError):
+        cfg.parseParameterString("nonsense=1")
+    with pytest.raises(KeyError):
+        cfg.getParameter("tol")
+    pr = mg.Config(mg.pagerank)
+    assert pr.getParameter("tol") == 0.1 and pr.getParameter("threshold") == 1000
+    with pytest.raises(KeyError):
+        pr.getParameter("src")
+    assert "max_queue_sizing" in cfg.printOptions()
+
+
+def test_program_selectors_mirror_reference():
+    assert mg.bfs.INIT_VALUE == -1 and mg.bfs.allow_duplicates
+    assert mg.sssp.INIT_VALUE == 2**31 - 1 and mg.sssp.applyOverEdges() == "APPLY_FRONTIER"
+    assert mg.cc.srcVertex() == "ALL"
+    assert mg.pagerank.gatherOverEdges() == "GATHER_IN_EDGES" and not mg.pagerank.allow_duplicates
