@@ -31,12 +31,12 @@
 
 #include "common.cuh"
 #include "engine.cuh"
+#include "expand.cuh"
 
 namespace mg {
 
 constexpr int BFS_NT = 256;
 constexpr int BFS_CTA_TH = 512;   // out-degree at or above which a CTA expands the vertex
-constexpr int BFS_WARP_TH = 32;   // out-degree at or above which a warp expands the vertex
 constexpr int PULL_SERIAL = 8;    // in-edges a lane scans alone before the warp helps
 constexpr int64_t BEAMER_ALPHA = 14, BEAMER_BETA = 24;
 
@@ -56,11 +56,6 @@ struct BfsArgs {
   cudaGraphConditionalHandle h;
   int32_t use_cond;
 };
-
-template <typename T>
-__device__ __forceinline__ T vload(const T *p) {
-  return *(const volatile T *)p;
-}
 
 __device__ void bfs_level_end(const BfsArgs &a) {
   DevCtl *c = a.ctl;
@@ -138,61 +133,8 @@ __device__ __forceinline__ void bfs_visit(PushCtx &x, int32_t u) {
   warp_append(disc, u, x.qout, x.qlen_out, x.qcap, x.overflow);
 }
 
-// Expands the edge lists (offsets `off`, targets `tgt`) of a tile of frontier
-// vertices with thread/warp/CTA degree bins.
-__device__ __forceinline__ void expand_tile(PushCtx &x, const int32_t *__restrict__ off,
-                                            const int32_t *__restrict__ tgt, int32_t v, int64_t &insp,
-                                            int32_t *s_scan, int32_t *s_beg, int32_t *s_red, int32_t *s_cta) {
-  const int tid = threadIdx.x, lane = lane_id();
-  int32_t beg = 0, deg = 0;
-  if (v >= 0) {
-    beg = off[v];
-    deg = off[v + 1] - beg;
-    insp += deg;
-  }
-  // CTA bin.
-  while (__syncthreads_or(deg >= BFS_CTA_TH)) {
-    if (deg >= BFS_CTA_TH) s_cta[0] = tid;
-    __syncthreads();
-    if (s_cta[0] == tid) {
-      s_cta[1] = beg;
-      s_cta[2] = beg + deg;
-      deg = 0;
-    }
-    __syncthreads();
-    const int32_t b = s_cta[1], e = s_cta[2];
-    for (int32_t k = b + tid; k < e; k += BFS_NT) bfs_visit(x, tgt[k]);
-  }
-  // Warp bin.
-  for (;;) {
-    unsigned wm = __ballot_sync(FULL, deg >= BFS_WARP_TH);
-    if (!wm) break;
-    const int l = __ffs(wm) - 1;
-    const int32_t b = __shfl_sync(FULL, beg, l), e = __shfl_sync(FULL, beg + deg, l);
-    if (lane == l) deg = 0;
-    for (int32_t k = b + lane; k < e; k += 32) bfs_visit(x, tgt[k]);
-  }
-  // Thread bin: block-wide scan of the remaining degrees, then the CTA walks
-  // the concatenated edge slots; each slot finds its owner by binary search.
-  int32_t total;
-  const int32_t ex = block_exclusive_scan<BFS_NT>(deg, s_red, &total);
-  s_scan[tid] = ex;
-  s_beg[tid] = beg;
-  __syncthreads();
-  for (int32_t k = tid; k < total; k += BFS_NT) {
-    int lo = 0, hi = BFS_NT;
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (s_scan[mid] <= k) lo = mid;
-      else hi = mid;
-    }
-    bfs_visit(x, tgt[s_beg[lo] + (k - s_scan[lo])]);
-  }
-  __syncthreads();
-}
-
 __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
-  __shared__ int32_t s_scan[BFS_NT], s_beg[BFS_NT], s_red[BFS_NT / 32 + 1], s_cta[4];
+  __shared__ ExpandSmem<BFS_NT> sm;
   __shared__ int64_t s_sum[BFS_NT / 32 + 1];
   if (bfs_skip(a, 0)) return;
   DevCtl *c = a.ctl;
@@ -205,8 +147,10 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
     nexp += v >= 0;
-    expand_tile(x, a.ro, a.ci, v, insp, s_scan, s_beg, s_red, s_cta);
-    if (a.both) expand_tile(x, a.co, a.ri, v, insp, s_scan, s_beg, s_red, s_cta);
+    const int32_t *ci = a.ci, *ri = a.ri;
+    expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+    if (a.both)
+      expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
   }
   const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
   const int64_t bins = block_sum<BFS_NT>(insp, s_sum);

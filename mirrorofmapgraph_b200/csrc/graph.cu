@@ -455,6 +455,7 @@ static void graph_free_device(mg_graph *g) {
   if (s) cudaStreamSynchronize(s);
   if (g->ws_main.ptr) cudaFree(g->ws_main.ptr);
   if (g->ws_aux.ptr) cudaFree(g->ws_aux.ptr);
+  if (g->ws_out.ptr) cudaFree(g->ws_out.ptr);
   if (g->ctl) cudaFree(g->ctl);
   if (g->ctl_host) cudaFreeHost(g->ctl_host);
   if (g->ev0) cudaEventDestroy(g->ev0);

@@ -76,12 +76,16 @@ struct mg_graph {
   int32_t *co = nullptr, *ri = nullptr, *perm = nullptr;
   void *cvals = nullptr;
   bool has_csc = false, csc_owned = false;
-  // per-vertex out-degree sum helpers
-  int64_t max_outdeg = 0;
+  // cached checks of the edge values
+  bool weights_checked = false;
+  int32_t min_weight = 0;
   // ragged batch
   std::vector<int64_t> vbase;
-  // workspaces
-  Workspace ws_main, ws_aux;
+  // workspaces: ws_main per-run state, ws_aux graph build scratch, ws_out staged
+  // results of host-output calls, ws_plan per-graph plans that outlive one call
+  Workspace ws_main, ws_aux, ws_out;
+  void *plan_csc = nullptr;  // PageRank gather plan over the CSC (pagerank.cu)
+  void *plan_csr = nullptr;  // the same over the CSR (adjoint)
   DevCtl *ctl = nullptr;       // device control block
   DevCtl *ctl_host = nullptr;  // pinned host mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -1,0 +1,312 @@
+// sssp.cu -- single-source shortest paths (struct sssp, Algorithms/SSSP/sssp.h:33-409).
+//
+// The reference runs a push Bellman-Ford in five phases per iteration: apply
+// (min of dist and gathered candidate), post-apply (commit, reset gather_tmp),
+// expand (emit neighbour + candidate distance for every improving edge into an
+// edge-sized queue), contract (atomicMin into gather_tmp, cull duplicates)
+// (sssp.h:242-402, GASengine/enactor_vertex_centric.cuh:2561-2822).
+//
+// Here one kernel per iteration does all of it: each frontier vertex's edges are
+// expanded with the degree-binned tile expansion; an improving edge lowers
+// dist[u] directly with atomicMin, and the thread whose atomicMin won the
+// improvement claims u's bit in the next frontier's bitmap and appends it with a
+// warp-aggregated atomic. No edge-sized queue exists and duplicates never enter
+// the frontier. Distances are unique fixed points, so the result equals the
+// reference's bit for bit for any schedule.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "expand.cuh"
+
+namespace mg {
+
+constexpr int SSSP_NT = 256;
+constexpr int SSSP_CTA_TH = 512;
+
+struct SsspArgs {
+  const int32_t *ro, *ci, *w;   // CSR with weights (w == nullptr: unit weights)
+  const int32_t *co, *ri, *cw;  // CSC with permuted weights (directed == 0 only)
+  int32_t *dist;
+  uint32_t *inq0, *inq1;        // next-frontier dedup bitmaps (ping-pong)
+  int32_t *q0, *q1;
+  int32_t qcap;
+  int32_t both;
+  int64_t n;
+  DevCtl *ctl;
+  cudaGraphConditionalHandle h;
+  int32_t use_cond;
+};
+
+struct RelaxCtx {
+  int32_t *dist;
+  uint32_t *inq_next;
+  const int32_t *ro;
+  int32_t *qout, *qlen_out, *overflow;
+  int32_t qcap;
+  int64_t reach_deg;  // out-degrees of vertices reached for the first time
+  int64_t updates;
+};
+
+__device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t w) {
+  const int32_t dv = vload(x.dist + v);
+  const int64_t nd64 = (int64_t)dv + (int64_t)w;
+  bool push = false;
+  if (nd64 < (int64_t)vload(x.dist + u)) {
+    const int32_t nd = (int32_t)nd64;
+    const int32_t old = atomicMin(x.dist + u, nd);
+    if (nd < old) {
+      x.updates++;
+      if (old == INT_MAX) x.reach_deg += x.ro[u + 1] - x.ro[u];
+      const uint32_t bit = 1u << (u & 31);
+      push = !(atomicOr(x.inq_next + (u >> 5), bit) & bit);
+    }
+  }
+  warp_append(push, u, x.qout, x.qlen_out, x.qcap, x.overflow);
+}
+
+__device__ void sssp_level_end(const SsspArgs &a) {
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const int32_t nf = vload(&c->qlen[cur ^ 1]);
+  const int lvl = vload(&c->level) + 1;
+  c->visited_deg = vload(&c->visited_deg) + vload(&c->mf_next);
+  c->mf_next = 0;
+  c->level = lvl;
+  c->qlen[cur] = 0;
+  c->cur = cur ^ 1;
+  c->blocks_done = 0;
+  const bool over = vload(&c->overflow) != 0;
+  const bool done = nf == 0 || lvl >= c->iter_cap || over;
+  if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+  __threadfence();
+  c->done = done ? 1 : 0;
+  if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+}
+
+__global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
+  __shared__ ExpandSmem<SSSP_NT> sm;
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
+  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, 0, 0};
+  int64_t insp = 0, nexp = 0;
+  const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
+  for (int64_t tile = (int64_t)blockIdx.x * SSSP_NT; tile < nin; tile += (int64_t)gridDim.x * SSSP_NT) {
+    const int64_t i = tile + threadIdx.x;
+    const int32_t v = i < nin ? qin[i] : -1;
+    if (v >= 0) {
+      // The whole bitmap of the current frontier is cleared here, one word at a
+      // time: nothing sets bits in it during this level.
+      inq_cur[v >> 5] = 0u;
+      nexp++;
+    }
+    expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) {
+      relax(x, sv, ci[k], w ? w[k] : 1);
+    });
+    if (a.both)
+      expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) {
+        relax(x, sv, ri[k], cw ? cw[k] : 1);
+      });
+  }
+  const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
+  const int64_t b1 = block_sum<SSSP_NT>(insp, s_sum);
+  const int64_t b2 = block_sum<SSSP_NT>(nexp, s_sum);
+  const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
+  if (threadIdx.x == 0) {
+    if (b0) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b0);
+    if (b1) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)b1);
+    if (b2) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)b2);
+    if (b3) atomicAdd((unsigned long long *)&c->vertices_updated, (unsigned long long)b3);
+  }
+  if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
+}
+
+__global__ void sssp_clear_kernel(int32_t *dist, uint32_t *b0, uint32_t *b1, int64_t n) {
+  const int64_t nw = (n + 31) >> 5;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dist[i] = INT_MAX;
+    if (i < nw) {
+      b0[i] = 0;
+      b1[i] = 0;
+    }
+  }
+}
+
+__global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, int32_t iter_cap) {
+  __shared__ int64_t s_sum[1024 / 32 + 1];
+  DevCtl *c = a.ctl;
+  int64_t deg = 0;
+  for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
+    const int32_t s = srcs[i];
+    const uint32_t bit = 1u << (s & 31);
+    if (!(atomicOr(&a.inq0[s >> 5], bit) & bit)) {
+      a.dist[s] = 0;
+      deg += a.ro[s + 1] - a.ro[s];
+      const int pos = atomicAdd(&c->qlen[0], 1);
+      if (pos < a.qcap) a.q0[pos] = s;
+      else c->overflow = 1;
+    }
+  }
+  const int64_t t = block_sum<1024>(deg, s_sum);
+  if (threadIdx.x == 0) {
+    c->visited_deg = t;
+    c->iter_cap = iter_cap;
+    c->done = c->overflow ? 1 : 0;
+    if (c->overflow) c->status = MG_ERR_QUEUE_OVERFLOW;
+  }
+}
+
+__global__ void min_i32_kernel(const int32_t *__restrict__ v, int64_t m, int *__restrict__ out) {
+  int mn = INT_MAX;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    mn = min(mn, v[i]);
+  mn = __reduce_min_sync(FULL, mn);
+  if (lane_id() == 0 && mn != INT_MAX) atomicMin(out, mn);
+}
+
+}  // namespace mg
+
+// Checks once per graph that int32 weights are non-negative (cached).
+static mg_status check_weights_nonnegative(mg_graph *g) {
+  if (g->vtype != MG_DTYPE_I32 || g->m == 0 || g->weights_checked) return MG_OK;
+  int *d = reinterpret_cast<int *>(reinterpret_cast<char *>(g->ctl) + sizeof(DevCtl));
+  int h = INT_MAX;
+  MG_CUDA_TRY(cudaMemcpyAsync(d, &h, sizeof(int), cudaMemcpyHostToDevice, g->stream));
+  mg::min_i32_kernel<<<g->num_sms * 4, 256, 0, g->stream>>>((const int32_t *)g->vals, g->m, d);
+  MG_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+  MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  g->weights_checked = true;
+  g->min_weight = h;
+  return MG_OK;
+}
+
+// Runs a (multi-source) SSSP into `dist` (device, n entries).
+static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts &o,
+                          mg_stats *stats) {
+  using namespace mg;
+  for (int32_t i = 0; i < nsrc; i++) {
+    if (srcs[i] < 0 || srcs[i] >= g->n) {
+      mg_set_error("mg_sssp: source %d out of range [0, %lld)", srcs[i], (long long)g->n);
+      return MG_ERR_ARG;
+    }
+  }
+  if (g->vtype == MG_DTYPE_F32) {
+    mg_set_error("mg_sssp: float edge values are not supported (int32 distances)");
+    return MG_ERR_UNSUPPORTED;
+  }
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  const bool both = o.directed == 0 && !symmetric;
+  if (both && !g->has_csc) {
+    mg_set_error("mg_sssp: directed=0 needs the CSC");
+    return MG_ERR_UNSUPPORTED;
+  }
+  MG_TRY(check_weights_nonnegative(g));
+  if (g->vtype == MG_DTYPE_I32 && g->min_weight < 0) {
+    mg_set_error("mg_sssp: negative edge weight %d", g->min_weight);
+    return MG_ERR_ARG;
+  }
+  const int64_t n = g->n;
+  int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)n) : n;
+  const int32_t qcap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(qcap64, n));
+  const int64_t nwords = (n + 31) / 32;
+  const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
+                                   sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
+                                   sizeof(int32_t) * (size_t)nsrc});
+  MG_TRY(ws_reserve(g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  SsspArgs a;
+  a.inq0 = cv.take<uint32_t>(nwords);
+  a.inq1 = cv.take<uint32_t>(nwords);
+  a.q0 = cv.take<int32_t>(qcap);
+  a.q1 = cv.take<int32_t>(qcap);
+  int32_t *dsrc = cv.take<int32_t>(nsrc);
+  a.ro = g->ro;
+  a.ci = g->ci;
+  a.w = g->vtype == MG_DTYPE_I32 ? (const int32_t *)g->vals : nullptr;
+  a.co = g->has_csc ? g->co : g->ro;
+  a.ri = g->has_csc ? g->ri : g->ci;
+  a.cw = g->vtype == MG_DTYPE_I32 ? (const int32_t *)(g->has_csc ? g->cvals : g->vals) : nullptr;
+  a.dist = dist;
+  a.qcap = qcap;
+  a.both = both ? 1 : 0;
+  a.n = n;
+  a.ctl = g->ctl;
+  a.h = 0;
+  a.use_cond = 0;
+  cudaStream_t s = g->stream;
+  const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
+  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, n);
+  sssp_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap);
+  MG_CUDA_TRY(cudaGetLastError());
+  const int grid = g->num_sms * 4;
+  struct Sig {
+    SsspArgs a;
+    int grid;
+  } sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.a = a;
+  sig.grid = grid;
+  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+    SsspArgs b = a;
+    b.h = h;
+    b.use_cond = use_cond;
+    sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+  };
+  MG_TRY(run_loop(g, SLOT_SSSP, &sig, sizeof(sig), o.use_graph >= 0, body, (int64_t)n + 2));
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = hc.visited_deg;
+    stats->edges_inspected = hc.edges_inspected;
+    stats->bytes_compulsory = (a.w ? 8 : 4) * hc.edges_inspected + 16 * hc.vertices_expanded + 8 * hc.vertices_updated;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_sssp: device status %d (queue capacity %d)", hc.status, qcap);
+    return (mg_status)hc.status;
+  }
+  return MG_OK;
+}
+
+extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts *opts,
+                             mg_stats *stats) {
+  if (!g || !srcs || nsrc <= 0 || !dist) {
+    mg_set_error("mg_sssp: null argument or nsrc <= 0");
+    return MG_ERR_ARG;
+  }
+  mg_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.directed = 1;
+  if (opts) o = *opts;
+  MG_TRY(graph_enter(g));
+  int32_t *out = dist;
+  if (!o.device_output) {
+    MG_TRY(ws_reserve(g->ws_out, sizeof(int32_t) * (size_t)g->n + 256));
+    out = (int32_t *)g->ws_out.ptr;
+  }
+  MG_TRY(sssp_run(g, srcs, nsrc, out, o, stats));
+  if (!o.device_output) {
+    MG_TRY(copy_out(g, dist, out, sizeof(int32_t) * g->n, 0));
+    MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
+  return MG_OK;
+}
