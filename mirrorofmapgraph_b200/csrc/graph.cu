@@ -93,15 +93,6 @@ __global__ void validate_kernel(const int32_t *__restrict__ ro, const int32_t *_
   if (b) atomicOr(bad, b);
 }
 
-// Minimum of int32 edge values (SSSP needs them non-negative).
-__global__ void min_value_kernel(const int32_t *__restrict__ v, int64_t m, int *__restrict__ out) {
-  int mn = INT_MAX;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-    mn = min(mn, v[i]);
-  mn = min(mn, __reduce_min_sync(FULL, mn));
-  if (lane_id() == 0 && mn != INT_MAX) atomicMin(out, mn);
-}
-
 // ---------------------------------------------------------------------------
 // Exclusive scan of int32 counts (n items) into int32 offsets (n + 1 items),
 // three passes over tiles of 2048.
@@ -465,6 +456,7 @@ static void graph_free_device(mg_graph *g) {
 }
 
 void engine_release_cached(mg_graph *g);  // defined with the iteration drivers
+void pr_release_plans(mg_graph *g);       // defined with PageRank
 
 extern "C" {
 
@@ -603,6 +595,7 @@ mg_status mg_graph_destroy(mg_graph *g) {
   if (!g) return MG_OK;
   cudaSetDevice(g->device);
   engine_release_cached(g);
+  pr_release_plans(g);
   graph_free_device(g);
   delete g;
   return MG_OK;

@@ -1,0 +1,771 @@
+// pagerank.cu -- PageRank (struct pagerank, Algorithms/PageRank/PageRank.h:33-409)
+// and its adjoint.
+//
+// Two modes:
+//  NORMALIZED  x' = alpha * (P^T x + d t) + (1 - alpha) t over all vertices each
+//              iteration; P_uv = a_uv / s_u (a = 1 unweighted), d = rank mass on
+//              dangling vertices, t = teleport. One iteration is two kernels: the
+//              merge-path gather over the CSC (pr_gather.cuh) with the update fused
+//              into its epilogue (new x, new x/s for the next gather, |dx| and
+//              dangling-mass partials), then the fix-up of rows split across tiles,
+//              whose last CTA sums the FP64 partials in a fixed order and decides
+//              convergence on the device (L1 change < tol or max_iter).
+//  REFCOMPAT   the reference's program: x' = 0.15 + 0.85 * sum x_u / deg_u over the
+//              in-edges of the frontier, a vertex stays active while |dx| >= 0.01,
+//              the next frontier is the out-neighbourhood of the changed vertices
+//              (gather_edge/apply/expand_edge, PageRank.h:233-363); deg = outdeg,
+//              or outdeg + indeg with directed == 0 (PageRank.h:141-161).
+//
+// The adjoint of the NORMALIZED fixed point reuses the same gather on the CSR
+// (the reversed graph) and one edge kernel for the weight gradients.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "expand.cuh"
+#include "pr_gather.cuh"
+
+namespace mg {
+
+// ---------------------------------------------------------------------------
+// Plans: merge-path tile coordinates of one adjacency, cached per graph.
+struct GatherPlan {
+  int32_t ntiles = 0;
+  int32_t *tx = nullptr, *ty = nullptr;
+};
+
+struct PlanSet {
+  GatherPlan csc, csr;
+};
+
+}  // namespace mg
+
+static mg::PlanSet *plans_of(mg_graph *g) {
+  if (!g->plan_csc) g->plan_csc = new mg::PlanSet();
+  return static_cast<mg::PlanSet *>(g->plan_csc);
+}
+
+void pr_release_plans(mg_graph *g) {
+  if (!g->plan_csc) return;
+  mg::PlanSet *ps = static_cast<mg::PlanSet *>(g->plan_csc);
+  for (mg::GatherPlan *p : {&ps->csc, &ps->csr}) {
+    if (p->tx) cudaFree(p->tx);
+    if (p->ty) cudaFree(p->ty);
+  }
+  delete ps;
+  g->plan_csc = nullptr;
+}
+
+static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
+  using namespace mg;
+  PlanSet *ps = plans_of(g);
+  GatherPlan &p = csr ? ps->csr : ps->csc;
+  if (!p.tx) {
+    const int64_t items = g->n + g->m;
+    const int64_t nt = (items + PRG_IPC - 1) / PRG_IPC;
+    p.ntiles = (int32_t)std::max<int64_t>(nt, 1);
+    MG_CUDA_TRY(cudaMalloc((void **)&p.tx, sizeof(int32_t) * (p.ntiles + 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&p.ty, sizeof(int32_t) * (p.ntiles + 1)));
+    prg_plan_kernel<<<(p.ntiles + 256) / 256, 256, 0, g->stream>>>(csr ? g->ro : g->co, g->n, g->m, p.ntiles, p.tx,
+                                                                    p.ty);
+    MG_CUDA_TRY(cudaGetLastError());
+  }
+  *out = &p;
+  return MG_OK;
+}
+
+namespace mg {
+
+constexpr int PR_K1_PER_SM = 4;
+
+// Shared arguments of the gather-based solvers (forward and adjoint).
+struct SolveArgs {
+  const int32_t *off, *idx;   // adjacency gathered over (CSC forward, CSR adjoint)
+  const float *wts;           // its edge weights (nullptr unweighted)
+  const int32_t *tx, *ty;
+  int32_t ntiles;
+  int64_t n;
+  int32_t *carry_row, *head_row;
+  Comp *carry_val, *head_val;
+  float *v0, *v1;             // iterate ping-pong (x forward, lambda adjoint)
+  float *g0, *g1;             // gathered values ping-pong (x/s forward; unused adjoint)
+  const float *srow;          // s_u, 0 for dangling
+  const float *tele;          // teleport (nullptr: uniform tn)
+  const float *wvec;          // adjoint right-hand side dL/dx (nullptr forward)
+  double tn, alpha, tol;
+  int32_t max_iter;
+  int32_t adjoint;
+  double *part1, *part2;      // per-CTA FP64 partials of the two kernels
+  int32_t grid1, grid2;
+  DevCtl *ctl;
+  cudaGraphConditionalHandle h;
+  int32_t use_cond;
+};
+
+__device__ __forceinline__ double tele_of(const SolveArgs &a, int64_t r) {
+  return a.tele ? (double)a.tele[r] : a.tn;
+}
+
+// Per-row update. Forward: x' = alpha (acc + d t) + (1 - alpha) t, g' = x'/s.
+// Adjoint: lambda' = w + alpha * (s > 0 ? acc / s : t.lambda). Partials: |change|
+// and (forward) dangling mass of x' / (adjoint) t . lambda'.
+struct RowUpdate {
+  const SolveArgs *a;
+  const float *vold;
+  float *vnew, *gnew;
+  double scal;  // forward: dangling mass d of the current iterate; adjoint: t.lambda
+  double resid = 0.0, red2 = 0.0;
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) {
+    const double acc = (double)v.hi + (double)v.lo;
+    const double s = (double)a->srow[r];
+    double nv;
+    if (!a->adjoint) {
+      const double t = tele_of(*a, r);
+      nv = a->alpha * (acc + scal * t) + (1.0 - a->alpha) * t;
+      if (s > 0.0) gnew[r] = (float)(nv / s);
+      else {
+        gnew[r] = 0.f;
+        red2 += nv;
+      }
+    } else {
+      nv = (double)a->wvec[r] + a->alpha * (s > 0.0 ? acc / s : scal);
+      red2 += tele_of(*a, r) * nv;
+    }
+    const float nf = (float)nv;
+    resid += fabs((double)nf - (double)vold[r]);
+    vnew[r] = nf;
+  }
+};
+
+__device__ __forceinline__ bool solve_skip(const SolveArgs &a) {
+  if (vload(&a.ctl->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return true;
+  }
+  return false;
+}
+
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
+  __shared__ PrgShared sm;
+  __shared__ double s_red[PRG_NT / 32 + 1];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *vold = cur ? a.v1 : a.v0;
+  const float *gold = a.adjoint ? vold : (cur ? a.g1 : a.g0);
+  RowUpdate up{&a, vold, cur ? a.v0 : a.v1, cur ? a.g0 : a.g1, vload(&c->dprev[1])};
+  for (int32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    prg_tile<WEIGHTED>(sm, a.off, a.idx, a.wts, a.n, t, a.tx[t], a.ty[t], a.tx[t + 1], a.ty[t + 1], a.carry_row,
+                       a.carry_val, a.head_row, a.head_val, [&](int32_t col) { return gold[col]; }, up);
+  }
+  const double r = block_sum<PRG_NT>(up.resid, s_red);
+  const double d = block_sum<PRG_NT>(up.red2, s_red);
+  if (threadIdx.x == 0) {
+    a.part1[2 * blockIdx.x] = r;
+    a.part1[2 * blockIdx.x + 1] = d;
+  }
+}
+
+__global__ void __launch_bounds__(PRG_NT) solve_fixup_kernel(SolveArgs a) {
+  __shared__ double s_red[PRG_NT / 32 + 1];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *vold = cur ? a.v1 : a.v0;
+  RowUpdate up{&a, vold, cur ? a.v0 : a.v1, cur ? a.g0 : a.g1, vload(&c->dprev[1])};
+  for (int64_t t = (int64_t)blockIdx.x * PRG_NT + threadIdx.x; t < a.ntiles; t += (int64_t)gridDim.x * PRG_NT)
+    prg_fixup_tile((int32_t)t, a.carry_row, a.carry_val, a.head_row, a.head_val, up);
+  {
+    const double r = block_sum<PRG_NT>(up.resid, s_red);
+    const double d = block_sum<PRG_NT>(up.red2, s_red);
+    if (threadIdx.x == 0) {
+      a.part2[2 * blockIdx.x] = r;
+      a.part2[2 * blockIdx.x + 1] = d;
+    }
+  }
+  if (!last_block(&c->blocks_done)) return;
+  // Fixed-order FP64 reduction of every CTA's partials.
+  double r = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < a.grid1; i += PRG_NT) {
+    r += a.part1[2 * i];
+    d += a.part1[2 * i + 1];
+  }
+  for (int i = threadIdx.x; i < a.grid2; i += PRG_NT) {
+    r += a.part2[2 * i];
+    d += a.part2[2 * i + 1];
+  }
+  r = block_sum<PRG_NT>(r, s_red);
+  d = block_sum<PRG_NT>(d, s_red);
+  if (threadIdx.x == 0) {
+    const int lvl = c->level + 1;
+    c->level = lvl;
+    c->dsum[0] = r;
+    c->dprev[1] = d;
+    c->cur = cur ^ 1;
+    c->blocks_done = 0;
+    const bool done = r < a.tol || lvl >= a.max_iter;
+    __threadfence();
+    c->done = done ? 1 : 0;
+    if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+  }
+}
+
+// Initial iterate. Forward: x0 = t, g0 = t/s; partial sums of the dangling mass.
+// Adjoint: lambda0 = w; partial sums of t . w.
+__global__ void __launch_bounds__(256) solve_init_kernel(SolveArgs a) {
+  __shared__ double s_red[256 / 32 + 1];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double t = tele_of(a, i);
+    if (!a.adjoint) {
+      const double s = (double)a.srow[i];
+      a.v0[i] = (float)t;
+      if (s > 0.0) a.g0[i] = (float)(t / s);
+      else {
+        a.g0[i] = 0.f;
+        acc += (double)(float)t;
+      }
+    } else {
+      a.v0[i] = a.wvec[i];
+      acc += t * (double)a.wvec[i];
+    }
+  }
+  acc = block_sum<256>(acc, s_red);
+  if (threadIdx.x == 0) a.part1[2 * blockIdx.x + 1] = acc;
+}
+
+__global__ void __launch_bounds__(256) solve_init_reduce_kernel(SolveArgs a, int32_t ginit) {
+  __shared__ double s_red[256 / 32 + 1];
+  double d = 0.0;
+  for (int i = threadIdx.x; i < ginit; i += 256) d += a.part1[2 * i + 1];
+  d = block_sum<256>(d, s_red);
+  if (threadIdx.x == 0) {
+    DevCtl *c = a.ctl;
+    c->dprev[1] = d;
+    c->level = 0;
+    c->cur = 0;
+    c->iter_cap = a.max_iter;
+    c->done = a.max_iter <= 0 ? 1 : 0;
+  }
+}
+
+// Row sums s_u of the CSR (outdeg unweighted; sum of weights otherwise, through
+// the same compensated merge-path gather with unit gathered values).
+__global__ void outdeg_kernel(const int32_t *__restrict__ ro, int64_t n, float *__restrict__ s) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s[i] = (float)(ro[i + 1] - ro[i]);
+}
+
+struct RowSumWrite {
+  float *s;
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) { s[r] = v.hi + v.lo; }
+};
+
+__global__ void __launch_bounds__(PRG_NT) rowsum_kernel(SolveArgs a, float *s) {
+  __shared__ PrgShared sm;
+  RowSumWrite wr{s};
+  for (int32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x)
+    prg_tile<true>(sm, a.off, a.idx, a.wts, a.n, t, a.tx[t], a.ty[t], a.tx[t + 1], a.ty[t + 1], a.carry_row,
+                   a.carry_val, a.head_row, a.head_val, [](int32_t) { return 1.0f; }, wr);
+}
+
+__global__ void rowsum_fixup_kernel(SolveArgs a, float *s) {
+  RowSumWrite wr{s};
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.ntiles; t += (int64_t)gridDim.x * blockDim.x)
+    prg_fixup_tile((int32_t)t, a.carry_row, a.carry_val, a.head_row, a.head_val, wr);
+}
+
+__global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+}  // namespace mg
+
+// ---------------------------------------------------------------------------
+// Host side of the gather-based solvers.
+
+struct SolveBuffers {
+  mg::SolveArgs a;
+  float *srow_csr;
+};
+
+// Carves the solver's buffers out of ws_main and computes the row sums s_u.
+static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, mg::SolveArgs &a, size_t extra_floats,
+                             float **extra) {
+  using namespace mg;
+  GatherPlan *plan = nullptr;
+  MG_TRY(get_plan(g, adjoint, &plan));
+  GatherPlan *plan_rows = nullptr;
+  if (weighted) MG_TRY(get_plan(g, true, &plan_rows));
+  const int64_t n = g->n;
+  const int32_t nt = std::max(plan->ntiles, plan_rows ? plan_rows->ntiles : 0);
+  const int g1 = g->num_sms * PR_K1_PER_SM;
+  const int g2 = std::max(1, (nt + PRG_NT - 1) / PRG_NT);
+  const int ginit = g->num_sms * 8;
+  const int gp = std::max(std::max(g1, g2), ginit);
+  const size_t need = Carve::need({sizeof(float) * (size_t)n, sizeof(float) * (size_t)n, sizeof(float) * (size_t)n,
+                                   sizeof(float) * (size_t)n, sizeof(float) * (size_t)n,
+                                   sizeof(int32_t) * (size_t)nt, sizeof(int32_t) * (size_t)nt,
+                                   sizeof(Comp) * (size_t)nt, sizeof(Comp) * (size_t)nt,
+                                   sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp,
+                                   sizeof(float) * extra_floats});
+  MG_TRY(ws_reserve(g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  std::memset(&a, 0, sizeof(a));
+  a.v0 = cv.take<float>(n);
+  a.v1 = cv.take<float>(n);
+  a.g0 = cv.take<float>(n);
+  a.g1 = cv.take<float>(n);
+  float *srow = cv.take<float>(n);
+  a.carry_row = cv.take<int32_t>(nt);
+  a.head_row = cv.take<int32_t>(nt);
+  a.carry_val = cv.take<Comp>(nt);
+  a.head_val = cv.take<Comp>(nt);
+  a.part1 = cv.take<double>(2 * (size_t)gp);
+  a.part2 = cv.take<double>(2 * (size_t)gp);
+  if (extra) *extra = cv.take<float>(extra_floats);
+  a.n = n;
+  a.srow = srow;
+  a.grid1 = g1;
+  a.grid2 = g2;
+  a.ctl = g->ctl;
+  cudaStream_t s = g->stream;
+  fill_i32_kernel<<<g->num_sms * 4, 256, 0, s>>>(a.head_row, nt, -1);
+  if (!weighted) {
+    outdeg_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, n, srow);
+  } else {
+    SolveArgs r = a;
+    r.off = g->ro;
+    r.idx = g->ci;
+    r.wts = (const float *)g->vals;
+    r.tx = plan_rows->tx;
+    r.ty = plan_rows->ty;
+    r.ntiles = plan_rows->ntiles;
+    rowsum_kernel<<<g1, PRG_NT, 0, s>>>(r, srow);
+    rowsum_fixup_kernel<<<g2, PRG_NT, 0, s>>>(r, srow);
+  }
+  a.off = adjoint ? g->ro : g->co;
+  a.idx = adjoint ? g->ci : g->ri;
+  a.wts = weighted ? (const float *)(adjoint ? g->vals : g->cvals) : nullptr;
+  a.tx = plan->tx;
+  a.ty = plan->ty;
+  a.ntiles = plan->ntiles;
+  MG_CUDA_TRY(cudaGetLastError());
+  return MG_OK;
+}
+
+// Runs the solver loop described by `a` (initial iterate set up by the init
+// kernels). Returns after the loop; results stay in a.v0/a.v1 at ctl->cur.
+static mg_status solve_run(mg_graph *g, mg::SolveArgs &a, bool weighted, int use_graph, int slot) {
+  using namespace mg;
+  cudaStream_t s = g->stream;
+  const int ginit = g->num_sms * 8;
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  solve_init_kernel<<<ginit, 256, 0, s>>>(a);
+  solve_init_reduce_kernel<<<1, 256, 0, s>>>(a, ginit);
+  MG_CUDA_TRY(cudaGetLastError());
+  struct Sig {
+    SolveArgs a;
+    int w;
+  } sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.a = a;
+  sig.w = weighted;
+  const int g1 = a.grid1, g2 = a.grid2;
+  LoopBody body = [a, weighted, g1, g2](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+    SolveArgs b = a;
+    b.h = h;
+    b.use_cond = use_cond;
+    if (weighted) solve_gather_kernel<true><<<g1, PRG_NT, 0, st>>>(b);
+    else solve_gather_kernel<false><<<g1, PRG_NT, 0, st>>>(b);
+    solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
+  };
+  MG_TRY(run_loop(g, slot, &sig, sizeof(sig), use_graph >= 0, body, (int64_t)a.max_iter + 2));
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// REFCOMPAT: the reference program's delta-frontier iteration.
+namespace mg {
+
+constexpr int PRR_NT = 256;
+
+struct RefArgs {
+  const int32_t *ro, *ci, *co, *ri;
+  int32_t both;
+  float *x, *xn;
+  const float *deg;
+  uint8_t *chg;
+  uint32_t *inq0, *inq1;
+  int32_t *q0, *q1;
+  int32_t qcap;
+  int64_t n;
+  float delta;
+  int32_t compensated;
+  DevCtl *ctl;
+  cudaGraphConditionalHandle h;
+  int32_t use_cond;
+};
+
+__device__ __forceinline__ void warp_comp_reduce(Comp &c) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Comp d{__shfl_xor_sync(FULL, c.hi, o), __shfl_xor_sync(FULL, c.lo, o)};
+    comp_add(c, d);
+  }
+}
+
+__device__ __forceinline__ void ref_term(Comp &acc, const RefArgs &a, int32_t u) {
+  const float t = a.x[u] / a.deg[u];
+  if (a.compensated) two_sum_add(acc, t);
+  else acc.hi += t;
+}
+
+// Gather + apply for a tile of frontier vertices: thread bin (< 32 in-edges)
+// sums sequentially, warp bin with a fixed shuffle tree, CTA bin with a fixed
+// shared-memory tree, so every sum has a fixed order.
+__global__ void __launch_bounds__(PRR_NT) prr_gather_kernel(RefArgs a) {
+  __shared__ float s_hi[PRR_NT], s_lo[PRR_NT];
+  __shared__ int32_t s_v, s_owner;
+  __shared__ int64_t s_sum[PRR_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  const int lane = lane_id();
+  int64_t insp = 0;
+  for (int64_t tile = (int64_t)blockIdx.x * PRR_NT; tile < nin; tile += (int64_t)gridDim.x * PRR_NT) {
+    const int64_t i = tile + threadIdx.x;
+    const int32_t v = i < nin ? qin[i] : -1;
+    int32_t d1 = 0, d2 = 0;
+    if (v >= 0) {
+      d1 = a.co[v + 1] - a.co[v];
+      d2 = a.both ? a.ro[v + 1] - a.ro[v] : 0;
+      insp += d1 + d2;
+    }
+    int32_t deg = d1 + d2;
+    Comp acc{0.f, 0.f};
+    bool mine = v >= 0 && deg < 32;
+    if (mine) {
+      for (int32_t e = a.co[v]; e < a.co[v + 1]; e++) ref_term(acc, a, a.ri[e]);
+      if (a.both)
+        for (int32_t e = a.ro[v]; e < a.ro[v + 1]; e++) ref_term(acc, a, a.ci[e]);
+    }
+    // CTA bin.
+    while (__syncthreads_or(deg >= 2048 && !mine)) {
+      if (deg >= 2048 && !mine) s_owner = threadIdx.x;
+      __syncthreads();
+      const int owner = s_owner;
+      if (threadIdx.x == owner) s_v = v;
+      __syncthreads();
+      const int32_t vv = s_v;
+      Comp part{0.f, 0.f};
+      for (int32_t e = a.co[vv] + threadIdx.x; e < a.co[vv + 1]; e += PRR_NT) ref_term(part, a, a.ri[e]);
+      if (a.both)
+        for (int32_t e = a.ro[vv] + threadIdx.x; e < a.ro[vv + 1]; e += PRR_NT) ref_term(part, a, a.ci[e]);
+      s_hi[threadIdx.x] = part.hi;
+      s_lo[threadIdx.x] = part.lo;
+      __syncthreads();
+      for (int st = PRR_NT / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) {
+          Comp x{s_hi[threadIdx.x], s_lo[threadIdx.x]};
+          comp_add(x, Comp{s_hi[threadIdx.x + st], s_lo[threadIdx.x + st]});
+          s_hi[threadIdx.x] = x.hi;
+          s_lo[threadIdx.x] = x.lo;
+        }
+        __syncthreads();
+      }
+      if (threadIdx.x == owner) {
+        acc = Comp{s_hi[0], s_lo[0]};
+        mine = true;
+      }
+      __syncthreads();
+    }
+    // Warp bin.
+    for (;;) {
+      const unsigned wm = __ballot_sync(FULL, deg >= 32 && !mine);
+      if (!wm) break;
+      const int l = __ffs(wm) - 1;
+      const int32_t wv = __shfl_sync(FULL, v, l);
+      Comp part{0.f, 0.f};
+      for (int32_t e = a.co[wv] + lane; e < a.co[wv + 1]; e += 32) ref_term(part, a, a.ri[e]);
+      if (a.both)
+        for (int32_t e = a.ro[wv] + lane; e < a.ro[wv + 1]; e += 32) ref_term(part, a, a.ci[e]);
+      warp_comp_reduce(part);
+      if (lane == l) {
+        acc = part;
+        mine = true;
+      }
+    }
+    if (v >= 0) {
+      const float g = acc.hi + acc.lo;
+      const float nv = 0.15f + (1.0f - 0.15f) * g;
+      a.chg[v] = fabsf(a.x[v] - nv) >= a.delta ? 1 : 0;
+      a.xn[v] = nv;
+    }
+  }
+  const int64_t b = block_sum<PRR_NT>(insp, s_sum);
+  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)b);
+}
+
+__global__ void __launch_bounds__(PRR_NT) prr_expand_kernel(RefArgs a) {
+  __shared__ ExpandSmem<PRR_NT> sm;
+  __shared__ int64_t s_sum[PRR_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
+  uint32_t *inq_next = cur ? a.inq0 : a.inq1;
+  int32_t *qout = cur ? a.q0 : a.q1;
+  int32_t *qlen_out = &c->qlen[cur ^ 1];
+  int64_t insp = 0, nchg = 0;
+  const int32_t *ci = a.ci, *ri = a.ri;
+  auto claim = [&](int32_t, int32_t u) {
+    const uint32_t bit = 1u << (u & 31);
+    const bool push = !(atomicOr(inq_next + (u >> 5), bit) & bit);
+    warp_append(push, u, qout, qlen_out, a.qcap, &c->overflow);
+  };
+  for (int64_t tile = (int64_t)blockIdx.x * PRR_NT; tile < nin; tile += (int64_t)gridDim.x * PRR_NT) {
+    const int64_t i = tile + threadIdx.x;
+    int32_t v = i < nin ? qin[i] : -1;
+    if (v >= 0) {
+      inq_cur[v >> 5] = 0u;
+      a.x[v] = a.xn[v];
+      if (a.chg[v]) nchg++;
+      else v = -1;
+    }
+    expand_tile<PRR_NT, 1024>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) { claim(sv, ci[k]); });
+    if (a.both) expand_tile<PRR_NT, 1024>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) { claim(sv, ri[k]); });
+  }
+  const int64_t b = block_sum<PRR_NT>(nchg, s_sum);
+  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&c->vertices_updated, (unsigned long long)b);
+  if (last_block(&c->blocks_done) && threadIdx.x == 0) {
+    const int32_t nf = vload(&c->qlen[cur ^ 1]);
+    const int lvl = c->level + 1;
+    c->level = lvl;
+    c->qlen[cur] = 0;
+    c->cur = cur ^ 1;
+    c->blocks_done = 0;
+    const bool over = vload(&c->overflow) != 0;
+    if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+    const bool done = nf == 0 || lvl >= c->iter_cap || over;
+    __threadfence();
+    c->done = done ? 1 : 0;
+    if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+  }
+}
+
+__global__ void prr_init_kernel(RefArgs a, float *deg, int32_t iter_cap) {
+  const int64_t nw = (a.n + 31) >> 5;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    a.x[i] = 0.15f;
+    a.q0[i] = (int32_t)i;
+    a.chg[i] = 0;
+    int32_t d = a.ro[i + 1] - a.ro[i];
+    if (a.both) d += a.co[i + 1] - a.co[i];
+    deg[i] = (float)d;
+    if (i < nw) {
+      a.inq0[i] = 0;
+      a.inq1[i] = 0;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ctl->qlen[0] = (int32_t)a.n;
+    a.ctl->iter_cap = iter_cap;
+    a.ctl->done = (a.n == 0 || iter_cap <= 0) ? 1 : 0;
+  }
+}
+
+}  // namespace mg
+
+static mg_status pagerank_refcompat(mg_graph *g, float *ranks, const mg_pr_opts &o, mg_stats *stats) {
+  using namespace mg;
+  if (!g->has_csc) {
+    mg_set_error("mg_pagerank: the gather over in-edges needs the CSC");
+    return MG_ERR_UNSUPPORTED;
+  }
+  const int64_t n = g->n;
+  const int64_t nwords = (n + 31) / 32;
+  const size_t need = Carve::need({4 * (size_t)n, 4 * (size_t)n, 4 * (size_t)n, (size_t)n, 4 * (size_t)nwords,
+                                   4 * (size_t)nwords, 4 * (size_t)n, 4 * (size_t)n});
+  MG_TRY(ws_reserve(g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  RefArgs a;
+  std::memset(&a, 0, sizeof(a));
+  float *xws = cv.take<float>(n);
+  a.xn = cv.take<float>(n);
+  float *deg = cv.take<float>(n);
+  a.chg = cv.take<uint8_t>(n);
+  a.inq0 = cv.take<uint32_t>(nwords);
+  a.inq1 = cv.take<uint32_t>(nwords);
+  a.q0 = cv.take<int32_t>(n);
+  a.q1 = cv.take<int32_t>(n);
+  a.x = o.device_output ? ranks : xws;
+  a.deg = deg;
+  a.ro = g->ro;
+  a.ci = g->ci;
+  a.co = g->co;
+  a.ri = g->ri;
+  a.both = o.directed == 0 ? 1 : 0;
+  a.qcap = (int32_t)std::max<int64_t>(n, 1);
+  a.n = n;
+  a.delta = o.tol > 0 ? (float)o.tol : 0.01f;
+  a.compensated = o.compensated >= 0 ? 1 : 0;
+  a.ctl = g->ctl;
+  cudaStream_t s = g->stream;
+  // The reference iterates until the frontier empties (iter_num = INT_MAX); the
+  // delta rule always empties it, far below this bound.
+  const int32_t cap = o.max_iter > 0 ? o.max_iter : 100000;
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  prr_init_kernel<<<g->num_sms * 8, 256, 0, s>>>(a, deg, cap);
+  MG_CUDA_TRY(cudaGetLastError());
+  const int grid = g->num_sms * 4;
+  struct Sig {
+    RefArgs a;
+    int grid;
+  } sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.a = a;
+  sig.grid = grid;
+  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+    RefArgs b = a;
+    b.h = h;
+    b.use_cond = use_cond;
+    prr_gather_kernel<<<grid, PRR_NT, 0, st>>>(b);
+    prr_expand_kernel<<<grid, PRR_NT, 0, st>>>(b);
+  };
+  MG_TRY(run_loop(g, SLOT_PR_REF, &sig, sizeof(sig), o.use_graph >= 0, body, (int64_t)cap + 2));
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  if (!o.device_output) MG_TRY(copy_out(g, ranks, a.x, sizeof(float) * n, 0));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = hc.edges_inspected;
+    stats->edges_inspected = hc.edges_inspected;
+    stats->bytes_compulsory = 8 * hc.edges_inspected;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_pagerank: device status %d", hc.status);
+    return (mg_status)hc.status;
+  }
+  return MG_OK;
+}
+
+// NORMALIZED, one vector.
+static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *ranks_out, int out_is_device,
+                                     const mg_pr_opts &o, mg_stats *stats) {
+  using namespace mg;
+  const bool weighted = o.weighted != 0;
+  if (!g->has_csc) {
+    mg_set_error("mg_pagerank: the gather over in-edges needs the CSC");
+    return MG_ERR_UNSUPPORTED;
+  }
+  if (weighted && g->vtype != MG_DTYPE_F32) {
+    mg_set_error("mg_pagerank: weighted mode needs float edge values");
+    return MG_ERR_ARG;
+  }
+  SolveArgs a;
+  MG_TRY(solve_setup(g, false, weighted, a, 0, nullptr));
+  a.tele = tele_dev;
+  a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
+  a.alpha = o.alpha > 0 ? o.alpha : 0.85;
+  a.tol = o.tol > 0 ? o.tol : 1e-6;
+  a.max_iter = o.max_iter > 0 ? o.max_iter : 50;
+  a.adjoint = 0;
+  cudaStream_t s = g->stream;
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_TRY(solve_run(g, a, weighted, o.use_graph, SLOT_PR));
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  const float *res = hc.cur ? a.v1 : a.v0;
+  MG_CUDA_TRY(cudaMemcpyAsync(ranks_out, res, sizeof(float) * g->n,
+                              out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = g->m * hc.level;
+    stats->edges_inspected = g->m * hc.level;
+    stats->residual = hc.dsum[0];
+    // per iteration: offsets 4(n+1), indices 4m (+4m weights), x read, x and x/s written
+    stats->bytes_compulsory = hc.level * (4 * (g->n + 1) + (weighted ? 8 : 4) * g->m + 12 * g->n);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+  }
+  return MG_OK;
+}
+
+extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nvec, float *ranks,
+                                 const mg_pr_opts *opts, mg_stats *stats) {
+  if (!g || !ranks || nvec <= 0) {
+    mg_set_error("mg_pagerank: null argument or nvec <= 0");
+    return MG_ERR_ARG;
+  }
+  mg_pr_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.directed = 1;
+  if (opts) o = *opts;
+  if (o.mode != MG_PR_REFCOMPAT && o.mode != MG_PR_NORMALIZED) {
+    mg_set_error("mg_pagerank: unknown mode %d", o.mode);
+    return MG_ERR_ARG;
+  }
+  if (o.alpha < 0 || o.alpha >= 1) {
+    mg_set_error("mg_pagerank: alpha must be in [0, 1)");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  if (o.mode == MG_PR_REFCOMPAT) {
+    if (nvec != 1 || teleport) {
+      mg_set_error("mg_pagerank: REFCOMPAT takes no teleport vector and nvec == 1");
+      return MG_ERR_ARG;
+    }
+    return pagerank_refcompat(g, ranks, o, stats);
+  }
+  const int64_t n = g->n;
+  // Teleport vectors and outputs are staged through device memory.
+  float *tele_dev = nullptr;
+  if (teleport) {
+    if (o.device_output) tele_dev = const_cast<float *>(teleport);
+    else {
+      MG_TRY(ws_reserve(g->ws_out, sizeof(float) * (size_t)n * nvec + 256));
+      tele_dev = (float *)g->ws_out.ptr;
+      MG_CUDA_TRY(cudaMemcpyAsync(tele_dev, teleport, sizeof(float) * n * nvec, cudaMemcpyHostToDevice, g->stream));
+    }
+  }
+  mg_stats total;
+  std::memset(&total, 0, sizeof(total));
+  for (int32_t k = 0; k < nvec; k++) {
+    mg_stats st;
+    MG_TRY(pagerank_normalized(g, tele_dev ? tele_dev + (size_t)k * n : nullptr, ranks + (size_t)k * n,
+                               o.device_output, o, &st));
+    total.iterations += st.iterations;
+    total.edges_traversed += st.edges_traversed;
+    total.edges_inspected += st.edges_inspected;
+    total.bytes_compulsory += st.bytes_compulsory;
+    total.kernel_ms += st.kernel_ms;
+    total.residual = std::max(total.residual, st.residual);
+  }
+  if (stats) *stats = total;
+  return MG_OK;
+}

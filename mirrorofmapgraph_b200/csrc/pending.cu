@@ -2,7 +2,6 @@
 #include "mg_internal.h"
 
 extern "C" {
-mg_status mg_pagerank(mg_graph *, const float *, int32_t, float *, const mg_pr_opts *, mg_stats *) { mg_set_error("mg_pagerank: not implemented"); return MG_ERR_UNSUPPORTED; }
 mg_status mg_bfs_batch(mg_graph *, const int32_t *, int32_t, int32_t *, const mg_opts *, mg_stats *) { mg_set_error("not implemented"); return MG_ERR_UNSUPPORTED; }
 mg_status mg_sssp_batch(mg_graph *, const int32_t *, int32_t, int32_t *, const mg_opts *, mg_stats *) { mg_set_error("not implemented"); return MG_ERR_UNSUPPORTED; }
 mg_status mg_bfs_ragged(mg_graph *, const int32_t *, int32_t *, const mg_opts *, mg_stats *) { mg_set_error("not implemented"); return MG_ERR_UNSUPPORTED; }

@@ -1,0 +1,153 @@
+"""PageRank on the GPU through the C ABI.
+
+Reference-compatible mode: against the reference's CPUPR with the reference's own
+check (relative L2 < tol = 0.1, Algorithms/PageRank/PageRank.cu:315-327) and
+against the FP64 replay of the engine schedule. Normalised / personalised mode:
+L1 <= 1e-6 against the FP64 oracle run for the same number of iterations."""
+import numpy as np
+import pytest
+
+import oracle
+import mirrorofmapgraph_b200 as mg
+
+pytestmark = pytest.mark.gpu
+
+L1_TOL = 1e-6  # FP32 engine vs FP64 oracle, same iteration schedule
+
+
+def _fixture_graph(d):
+    return mg.Graph(np.array(d["row_offsets"], dtype=np.int32), np.array(d["col_idx"], dtype=np.int32),
+                    np.array(d["values"], dtype=np.float32))
+
+
+@pytest.mark.parametrize("name", ["small", "trivialGraph", "chesapeake"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_refcompat_fixtures(mtx_fixtures, name, use_graph):
+    d = mtx_fixtures[name]
+    ro, ci = np.array(d["row_offsets"]), np.array(d["col_idx"])
+    with _fixture_graph(d) as g:
+        x, st = g.pagerank(mode="refcompat", use_graph=use_graph)
+    ref = np.array(d["cpupr"])
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 0.1
+    x64, it = oracle.pr_refcompat(ro, ci, 1)
+    assert st["iterations"] == it
+    assert np.abs(x - x64).max() < 1e-5
+
+
+def test_refcompat_golden_and_undirected(synthetic_golden):
+    from golden.make_golden import er_graph, rmat_graph
+    for key, h in (("er", er_graph()), ("rmat", rmat_graph())):
+        with mg.Graph(h.row_offsets, h.col_idx) as g:
+            x, st = g.pagerank(mode="refcompat")
+            ref = synthetic_golden[key + "_pr"].astype(np.float64)
+            assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 0.1
+            x64, it = oracle.pr_refcompat(h.row_offsets, h.col_idx, 1)
+            assert st["iterations"] == it
+            assert np.abs(x - x64).max() < 1e-4
+            xu, stu = g.pagerank(mode="refcompat", directed=0)
+            xu64, itu = oracle.pr_refcompat(h.row_offsets, h.col_idx, 0)
+            assert stu["iterations"] == itu
+            assert np.abs(xu - xu64).max() < 1e-4
+
+
+def _check_normalized(h, weights=None, teleport=None, symmetric=False, **kw):
+    vals = None if weights is None else weights
+    with mg.Graph(h.row_offsets, h.col_idx, vals, symmetric=symmetric) as g:
+        x, st = g.pagerank(teleport=teleport, mode="normalized", weighted=weights is not None, **kw)
+        it = st["iterations"]
+        xr, it_r, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, weights, kw.get("alpha", 0.85), 0.0, it,
+                                           None if teleport is None else teleport.astype(np.float64))
+        assert it_r == it
+        err = np.abs(x.astype(np.float64) - xr).sum()
+        assert err <= L1_TOL, err
+        return x, st, err
+
+
+@pytest.mark.parametrize("scale,sym", [(10, True), (14, True), (14, False)])
+def test_normalized_rmat(scale, sym):
+    h = mg.gen_rmat(scale, 16, 3 + scale, symmetrize=sym)
+    x, st, err = _check_normalized(h, symmetric=sym)
+    assert st["iterations"] <= 50
+    assert abs(x.astype(np.float64).sum() - 1.0) < 1e-5
+
+
+def test_normalized_weighted_lognormal_directed():
+    h = mg.gen_rmat(13, 16, 99, symmetrize=False, weights="lognormal", p0=0, p1=1)
+    _check_normalized(h, weights=h.weights_f32)
+
+
+def test_normalized_converges_on_tolerance():
+    h = mg.gen_er(3000, 30000, 5)
+    with mg.Graph(h.row_offsets, h.col_idx) as g:
+        x, st = g.pagerank(mode="normalized", tol=1e-6, max_iter=500)
+    assert st["residual"] < 1e-6 and st["iterations"] < 500
+    xr, it, r = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 1e-6, 500)
+    assert it == st["iterations"]
+    assert np.abs(x - xr).sum() <= L1_TOL
+
+
+def test_personalized_vectors_and_loop_modes():
+    h = mg.gen_rmat(12, 8, 17, symmetrize=False)
+    rng = np.random.default_rng(1)
+    nvec = 5
+    tele = np.zeros((nvec, h.n), dtype=np.float32)
+    for k in range(nvec):
+        sup = rng.choice(h.n, size=rng.integers(1, 33), replace=False)
+        tele[k, sup] = 1.0 / sup.size
+    with mg.Graph(h.row_offsets, h.col_idx) as g:
+        xs, st = g.pagerank(teleport=tele, nvec=nvec, mode="normalized")
+        xs2, _ = g.pagerank(teleport=tele, nvec=nvec, mode="normalized", use_graph=False)
+        assert (xs == xs2).all()
+        for k in range(nvec):
+            x1, st1 = g.pagerank(teleport=tele[k], mode="normalized")
+            assert (x1 == xs[k]).all()
+            xr, it, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st1["iterations"],
+                                             tele[k].astype(np.float64))
+            assert np.abs(x1 - xr).sum() <= L1_TOL
+
+
+def test_pagerank_deterministic_and_hub_split():
+    # a star: one row with far more edges than a tile holds, split over many tiles
+    n = 20000
+    ro = np.zeros(n + 1, dtype=np.int32)
+    ro[1:] = n - 1  # vertex 0 -> all others
+    ro[0] = 0
+    ci = np.arange(1, n, dtype=np.int32)
+    rows = np.concatenate([ro[:1], ro[1:]])
+    # add the reverse edges: every leaf points back to 0
+    src = np.concatenate([np.zeros(n - 1, dtype=np.int64), np.arange(1, n)])
+    dst = np.concatenate([np.arange(1, n), np.zeros(n - 1, dtype=np.int64)])
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    ro = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(ro, src + 1, 1)
+    ro = np.cumsum(ro).astype(np.int32)
+    h = mg.HostCsr(ro, dst.astype(np.int32))
+    x, st, err = _check_normalized(h, symmetric=True)
+    with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+        a, _ = g.pagerank(mode="normalized")
+        b, _ = g.pagerank(mode="normalized")
+        assert (a == b).all()
+
+
+def test_compensation_improves_accuracy():
+    h = mg.gen_rmat(15, 16, 4, symmetrize=True)
+    with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+        xc, st = g.pagerank(mode="normalized", compensated=True)
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+        assert np.abs(xc - xr).sum() <= L1_TOL
+
+
+def test_api_pagerank_program(mtx_fixtures):
+    d = mtx_fixtures["small"]
+    ro, ci = np.array(d["row_offsets"], dtype=np.int32), np.array(d["col_idx"], dtype=np.int32)
+    cfg = mg.Config(mg.pagerank)
+    csr_problem = mg.CsrProblem(mg.pagerank, cfg)
+    csr_problem.FromHostProblem(False, 7, 11, ci, ro, np.array(d["values"]), None, None, 1,
+                                cfg.getParameter("directed"))
+    mg.EnactorVertexCentric(csr_problem, mg.pagerank, cfg).EnactIterativeSearch(
+        csr_problem, ro, cfg.getParameter("directed"), 7, None, cfg.getParameter("iter_num"),
+        cfg.getParameter("threshold"))
+    x = csr_problem.ExtractResults()
+    ref = np.array(d["cpupr"])
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < cfg.getParameter("tol")
