@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Benchmark of the GAS engine on one B200 per rank.
+
+Workload (R-MAT scale 22, edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05, no vertex
+permutation, symmetrised, int32 CSR, weights U{1..255}, seeded synthetic graph):
+one step runs, on the device-resident graph,
+
+  BFS from a seeded source  -> TEPS edges = sum of out-degrees of reached vertices
+  CC                        -> TEPS edges = m
+  PageRank (normalised, alpha 0.85, L1 residual < 1e-6 or 50 iterations)
+                            -> TEPS edges = m * iterations
+
+value = sum of TEPS edges / sum of their device times (GTEPS, CUDA events on the
+engine's stream, L2 flushed between steps). SSSP is timed after the steps and
+reported under "per_algorithm" only: the reference's CPU SSSP is O(n^2) and has no
+CPU baseline at this size.
+
+--impl reference times the reference's own CPU functions (CPUBFS, CPUCC, CPUPR,
+compiled from the reference tree into oracle/_ref) on the host, on a bounded
+sample of the same workload (the same generator at scale 20).
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torch.distributed.run (one replica per GPU, no data-path collective: every rank
+runs the full workload on its own graph, "scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS (BFS + CC + PageRank aggregate, R-MAT s22 ef16 symmetric)"
+SEED = 20140601
+ALPHA, PR_TOL, PR_MAX_IT = 0.85, 1e-6, 50
+CPU_SAMPLE_SCALE = 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--host-loop", action="store_true",
+                   help="drive iterations from the host instead of a CUDA-graph WHILE node (for profilers "
+                        "that cannot see kernels inside conditional graphs)")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def sources(h, k, seed):
+    deg = np.diff(h.row_offsets)
+    cand = np.flatnonzero(deg > 0)
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.choice(cand, size=k, replace=False)]
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/mg_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_reference_run(h, src):
+    """One pass of the reference's CPU functions (BFS from src, CC, PageRank)."""
+    import oracle
+    R = oracle.Ref
+    csc = (h.row_offsets, h.col_idx, None)  # symmetric: CSC = CSR
+    deg = np.diff(h.row_offsets).astype(np.int64)
+    d, tb = R.bfs(h.row_offsets, h.col_idx, src, 1, csc)
+    eb = int(deg[d >= 0].sum())
+    _, tc = R.cc(h.row_offsets, h.col_idx, csc)
+    _, tp, sweeps = R.pr(h.row_offsets, h.col_idx, csc, with_sweeps=True)
+    return {"bfs": (eb, tb), "cc": (h.m, tc), "pagerank": (h.m * max(sweeps, 0), tp), "pr_sweeps": sweeps}
+
+
+def cpu_sample_graph():
+    import mirrorofmapgraph_b200 as mg
+    return mg.gen_rmat(CPU_SAMPLE_SCALE, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    t_all = time.time()
+    try:
+        import oracle
+        if not oracle.have_ref():
+            raise RuntimeError("oracle/_ref/libmgref.so missing (reference CPU path not built)")
+        h = cpu_sample_graph()
+        srcs = sources(h, max(1, args.steps), SEED + 1)
+        for i in range(args.warmup):
+            cpu_reference_run(h, srcs[i % len(srcs)])
+        edges = secs = 0.0
+        per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
+        for i in range(args.steps):
+            r = cpu_reference_run(h, srcs[i % len(srcs)])
+            for k in per:
+                per[k][0] += r[k][0]
+                per[k][1] += r[k][1]
+                edges += r[k][0]
+                secs += r[k][1]
+        value = edges / secs / 1e9
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32",
+            "data": "synthetic (seeded R-MAT)",
+            "config": {"workload": f"rmat_s{CPU_SAMPLE_SCALE}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
+                                   "CPUBFS + CPUCC + CPUPR", "scale": CPU_SAMPLE_SCALE, "n": h.n, "m": h.m},
+            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": 1, "kind": "reference",
+                             "sample": f"reference CPUBFS/CPUCC/CPUPR (serial) on R-MAT scale {CPU_SAMPLE_SCALE} "
+                                       f"per step; CPUPR alone takes ~35 s at scale 22"},
+            "per_algorithm": {k: {"gteps": v[0] / v[1] / 1e9 if v[1] else None, "seconds": v[1]}
+                              for k, v in per.items()},
+            "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.time() - t_all,
+        }
+    except Exception as e:  # the reference path could not run here
+        line = {"impl": "reference", "unavailable": f"{type(e).__name__}: {e}"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import mirrorofmapgraph_b200 as mg
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    peak, peak_kind = peaks()
+
+    h = mg.gen_rmat(args.scale, args.edge_factor, SEED, symmetrize=True, weights="int", p0=1, p1=255)
+    n, m = h.n, h.m
+    srcs = sources(h, max(args.steps + args.warmup, 8), SEED + 1)
+    g = mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True)
+    stream = torch.cuda.ExternalStream(g.stream_ptr)
+    depth = torch.empty(n, dtype=torch.int32, device="cuda")
+    label = torch.empty(n, dtype=torch.int32, device="cuda")
+    rank_v = torch.empty(n, dtype=torch.float32, device="cuda")
+    dist_v = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    deg = np.diff(h.row_offsets).astype(np.int64)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    ug = not args.host_loop
+
+    def step(i):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        s = srcs[i % len(srcs)]
+        (_, st_b), tb = timed(lambda: g.bfs([s], out=depth, use_graph=ug))
+        (_, st_c), tc = timed(lambda: g.cc(out=label))
+        (_, st_p), tp = timed(lambda: g.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT,
+                                                 out=rank_v, use_graph=ug))
+        return {"bfs": (st_b["edges_traversed"], tb, st_b), "cc": (m, tc, st_c),
+                "pagerank": (m * st_p["iterations"], tp, st_p)}
+
+    for i in range(args.warmup):
+        step(i)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
+    launches = 0
+    pr_iters = 0
+    pr_ms = 0.0
+    bfs_stats = []
+    for i in range(args.steps):
+        r = step(args.warmup + i)
+        for k in per:
+            per[k][0] += r[k][0]
+            per[k][1] += r[k][1]
+            launches += r[k][2]["launches"]
+        pr_iters += r["pagerank"][2]["iterations"]
+        pr_ms += r["pagerank"][1]
+        bfs_stats.append(r["bfs"][2])
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    if dist:
+        dist.barrier()
+    edges = sum(v[0] for v in per.values())
+    ms = sum(v[1] for v in per.values())
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        e = torch.tensor([float(edges)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(e)
+        edges = float(e.item())
+    value = edges / (ms * 1e-3) / 1e9
+
+    # SSSP, reported per algorithm (not in the headline; see the module docstring).
+    sssp_edges = sssp_ms = 0.0
+    for i in range(min(3, args.steps)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        (_, st), t = timed(lambda: g.sssp([srcs[i]], out=dist_v, use_graph=ug))
+        sssp_edges += st["edges_traversed"]
+        sssp_ms += t
+
+    # Roofline of the dominant kernel pair: one PageRank iteration (merge-path
+    # gather + row fix-up), algorithmic bytes per iteration = offsets 4(n+1) +
+    # indices 4m + read x 4n + write x 4n + write x/s 4n.
+    pr_bytes_iter = 4 * (n + 1) + 4 * m + 12 * n
+    pr_s_iter = (pr_ms / max(pr_iters, 1)) * 1e-3
+    achieved = pr_bytes_iter / pr_s_iter / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        t = tj.get("solve_gather_kernel", {})
+        if t.get("scale") == args.scale:
+            traffic = t.get("dram_bytes_per_launch")
+    except Exception:
+        pass
+    per_alg = {k: {"gteps": v[0] / (v[1] * 1e-3) / 1e9, "ms_per_run": v[1] / args.steps} for k, v in per.items()}
+    per_alg["sssp"] = {"gteps": sssp_edges / (sssp_ms * 1e-3) / 1e9 if sssp_ms else None,
+                       "ms_per_run": sssp_ms / max(1, min(3, args.steps)), "in_headline": False}
+    # compulsory-byte roofline fractions per algorithm (stats.bytes_compulsory / time)
+    for k, key in (("bfs", "bfs"),):
+        bc = sum(s["bytes_compulsory"] for s in bfs_stats)
+        per_alg[k]["hbm_frac"] = bc / (per[k][1] * 1e-3) / 1e9 / peak
+    per_alg["pagerank"]["hbm_frac"] = achieved / peak
+
+    # End to end through the public API with host buffers: upload from pinned host
+    # memory, run the three programs with host outputs, read them back, release.
+    ro_pin = torch.from_numpy(h.row_offsets).pin_memory()
+    ci_pin = torch.from_numpy(h.col_idx).pin_memory()
+    e2e_edges = 0.0
+    e2e_s = 0.0
+    h2d = (n + 1) * 4 + m * 4
+    d2h = 3 * n * 4
+    for i in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with mg.Graph(ro_pin, ci_pin, symmetric=True) as ge:
+            d, sb = ge.bfs([srcs[i % len(srcs)]])
+            _, sc = ge.cc()
+            _, sp = ge.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT)
+        e2e_s += time.perf_counter() - t0
+        e2e_edges += sb["edges_traversed"] + m + m * sp["iterations"]
+    e2e = e2e_edges / e2e_s / 1e9 * (world if world > 1 else 1) if e2e_s > 0 else None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32 (BFS/CC), f32 + f64 reductions (PageRank)",
+        "data": "synthetic (seeded R-MAT, no vertex permutation)",
+        "config": {"workload": f"rmat_s{args.scale}_ef{args.edge_factor}_sym: BFS + CC + PageRank(normalized, "
+                               f"alpha {ALPHA}, tol {PR_TOL}, <= {PR_MAX_IT} it)",
+                   "scale": args.scale, "edge_factor": args.edge_factor, "n": n, "m": m,
+                   "l2": "256 MiB buffer written between steps; graph (CSR 537 MB) larger than L2",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "PageRank iteration (solve_gather_kernel + solve_fixup_kernel)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": pr_bytes_iter},
+        "per_algorithm": per_alg,
+        "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": args.e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            if oracle.have_ref():
+                hs = cpu_sample_graph()
+                r = cpu_reference_run(hs, sources(hs, 1, SEED + 1)[0])
+                ce = sum(r[k][0] for k in ("bfs", "cc", "pagerank"))
+                cs = sum(r[k][1] for k in ("bfs", "cc", "pagerank"))
+                line["cpu_baseline"] = {
+                    "value": ce / cs / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
+                    "sample": f"reference CPUBFS + CPUCC + CPUPR (serial, oracle/_ref) once on R-MAT scale "
+                              f"{CPU_SAMPLE_SCALE} (same generator); {cs:.1f} s of CPU work",
+                    "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")}}
+            else:
+                line["cpu_baseline"] = {"value": None, "unavailable": "oracle/_ref not built"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
+    g.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

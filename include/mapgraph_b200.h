@@ -84,7 +84,8 @@ typedef struct mg_stats {
   int64_t bytes_compulsory; /* algorithmic DRAM bytes (see the engine's documentation) */
   double kernel_ms;         /* device time of the iteration loop (CUDA events) */
   double residual;          /* PageRank: last L1 residual (normalised mode) */
-  int32_t status_detail;    /* engine-specific detail of a non-OK status */
+  int64_t launches;         /* kernels launched by the call */
+  int32_t status_detail;    /* BFS: levels run bottom-up; otherwise detail of a non-OK status */
   int32_t reserved;
 } mg_stats;
 
@@ -122,6 +123,10 @@ mg_status mg_graph_create(const int32_t *row_offsets, const int32_t *col_idx, co
 
 /* Replaces ~CsrProblem / ~GraphSlice (GASengine/csr_problem.cuh:217-309). NULL is a no-op. */
 mg_status mg_graph_destroy(mg_graph *g);
+
+/* The CUDA stream (a cudaStream_t) every call on g is issued on, so a caller can
+ * order its own work or CUDA events with the engine's. Owned by the graph. */
+mg_status mg_graph_stream(const mg_graph *g, void **stream);
 
 /* Sizes and flags of a graph (CsrProblem::nodes/edges, csr_problem.cuh:312-314). */
 mg_status mg_graph_info(const mg_graph *g, int64_t *n, int64_t *m, uint32_t *flags, int32_t *device);

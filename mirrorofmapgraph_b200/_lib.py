@@ -36,7 +36,7 @@ class MgOpts(C.Structure):
 class MgStats(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("edges_traversed", C.c_int64), ("edges_inspected", C.c_int64),
                 ("bytes_compulsory", C.c_int64), ("kernel_ms", C.c_double), ("residual", C.c_double),
-                ("status_detail", C.c_int32), ("reserved", C.c_int32)]
+                ("launches", C.c_int64), ("status_detail", C.c_int32), ("reserved", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -66,6 +66,7 @@ SIGNATURES = {
     "mg_graph_create": (C.c_int, [_P, _P, _P, C.c_int, C.c_int64, C.c_int64, C.c_uint32, C.POINTER(_P)]),
     "mg_graph_destroy": (C.c_int, [_P]),
     "mg_graph_info": (C.c_int, [_P, _I64P, _I64P, C.POINTER(C.c_uint32), _I32P]),
+    "mg_graph_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mg_graph_device_arrays": (C.c_int, [_P] + [C.POINTER(_P)] * 6),
     "mg_bfs": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_sssp": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),

@@ -378,6 +378,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
     stats->status_detail = hc.levels_pull;
+    stats->launches = 2 + (use_graph ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
   }
   if (hc.status != 0) {
     mg_set_error("mg_bfs: frontier exceeded queue capacity %d", qcap);

@@ -174,6 +174,16 @@ mg_status device_exclusive_scan(const int32_t *in, int32_t *out, int64_t n, int6
 
 namespace mg {
 
+// Pads of an offsets array (INT_MAX after entry n) and of its edge arrays (0).
+__global__ void fill_pad_kernel(int32_t *off, int64_t n, int32_t *edges, void *vals, int64_t m) {
+  const int t = threadIdx.x;
+  if (t < MG_OFF_PAD) off[n + 1 + t] = INT_MAX;
+  if (t < MG_EDGE_PAD) {
+    edges[m + t] = 0;
+    if (vals) reinterpret_cast<int32_t *>(vals)[m + t] = 0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // CSC build kernels.
 __global__ void count_cols_kernel(const int32_t *__restrict__ ci, int64_t m, int32_t *__restrict__ cnt) {
@@ -388,10 +398,11 @@ static mg_status build_csc(mg_graph *g) {
   const int64_t n = g->n, m = g->m;
   cudaStream_t s = g->stream;
   const size_t vbytes = g->vtype == MG_DTYPE_NONE ? 0 : 4;
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->co, sizeof(int32_t) * (n + 1), s));
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->ri, sizeof(int32_t) * std::max<int64_t>(m, 1), s));
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->perm, sizeof(int32_t) * std::max<int64_t>(m, 1), s));
-  if (vbytes) MG_CUDA_TRY(cudaMallocAsync(&g->cvals, vbytes * std::max<int64_t>(m, 1), s));
+  MG_CUDA_TRY(cudaMallocAsync((void **)&g->co, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
+  MG_CUDA_TRY(cudaMallocAsync((void **)&g->ri, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  MG_CUDA_TRY(cudaMallocAsync((void **)&g->perm, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  if (vbytes) MG_CUDA_TRY(cudaMallocAsync(&g->cvals, vbytes * (m + MG_EDGE_PAD), s));
+  mg::fill_pad_kernel<<<1, 32, 0, s>>>(g->co, n, g->ri, g->cvals, m);
   g->csc_owned = true;
   g->has_csc = true;
   const int64_t ntiles = std::max<int64_t>(1, (n + SCAN_TILE - 1) / SCAN_TILE);
@@ -543,9 +554,10 @@ static mg_status create_impl(const int32_t *row_offsets, const int32_t *col_idx,
       return fail(_e == cudaErrorMemoryAllocation ? MG_ERR_OOM : MG_ERR_CUDA);                  \
     }                                                                                           \
   } while (0)
-  CREATE_TRY(cudaMallocAsync((void **)&g->ro, sizeof(int32_t) * (n + 1), s));
-  CREATE_TRY(cudaMallocAsync((void **)&g->ci, sizeof(int32_t) * std::max<int64_t>(m, 1), s));
-  if (vb) CREATE_TRY(cudaMallocAsync(&g->vals, vb * std::max<int64_t>(m, 1), s));
+  CREATE_TRY(cudaMallocAsync((void **)&g->ro, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
+  CREATE_TRY(cudaMallocAsync((void **)&g->ci, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  if (vb) CREATE_TRY(cudaMallocAsync(&g->vals, vb * (m + MG_EDGE_PAD), s));
+  mg::fill_pad_kernel<<<1, 32, 0, s>>>(g->ro, n, g->ci, g->vals, m);
   CREATE_TRY(cudaMemcpyAsync(g->ro, row_offsets, sizeof(int32_t) * (n + 1), kind, s));
   if (m > 0) CREATE_TRY(cudaMemcpyAsync(g->ci, col_idx, sizeof(int32_t) * m, kind, s));
   if (vb && m > 0) CREATE_TRY(cudaMemcpyAsync(g->vals, edge_vals, vb * m, kind, s));
@@ -598,6 +610,15 @@ mg_status mg_graph_destroy(mg_graph *g) {
   pr_release_plans(g);
   graph_free_device(g);
   delete g;
+  return MG_OK;
+}
+
+mg_status mg_graph_stream(const mg_graph *g, void **stream) {
+  if (!g || !stream) {
+    mg_set_error("mg_graph_stream: null argument");
+    return MG_ERR_ARG;
+  }
+  *stream = (void *)g->stream;
   return MG_OK;
 }
 

@@ -56,6 +56,13 @@ struct DevCtl {
   int32_t pad;
 };
 
+// Padding of the device graph arrays. Offsets arrays hold n + 1 + MG_OFF_PAD
+// entries (the pad is INT_MAX) and edge arrays m + MG_EDGE_PAD entries (the pad is
+// 0), so 16-byte-aligned bulk copies that round a range outwards stay inside the
+// allocation, and an offset read one past the end compares as "no more edges".
+constexpr int64_t MG_OFF_PAD = 7;
+constexpr int64_t MG_EDGE_PAD = 8;
+
 // Reusable device workspace of a graph, grown on demand.
 struct Workspace {
   void *ptr = nullptr;

@@ -79,8 +79,6 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
 
 namespace mg {
 
-constexpr int PR_K1_PER_SM = 4;
-
 // Shared arguments of the gather-based solvers (forward and adjoint).
 struct SolveArgs {
   const int32_t *off, *idx;   // adjacency gathered over (CSC forward, CSR adjoint)
@@ -148,19 +146,25 @@ __device__ __forceinline__ bool solve_skip(const SolveArgs &a) {
   return false;
 }
 
+__device__ __forceinline__ PrgGraph prg_graph_of(const SolveArgs &a) {
+  return PrgGraph{a.off, a.idx, a.wts, a.tx, a.ty, a.ntiles, a.n, a.carry_row, a.head_row, a.carry_val, a.head_val};
+}
+
 template <bool WEIGHTED>
 __global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
-  __shared__ PrgShared sm;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PrgSmem<WEIGHTED> &sm = *reinterpret_cast<PrgSmem<WEIGHTED> *>(smem_raw);
   __shared__ double s_red[PRG_NT / 32 + 1];
   if (solve_skip(a)) return;
   DevCtl *c = a.ctl;
   const int cur = vload(&c->cur);
   const float *vold = cur ? a.v1 : a.v0;
-  const float *gold = a.adjoint ? vold : (cur ? a.g1 : a.g0);
+  const float *__restrict__ gold = a.adjoint ? vold : (cur ? a.g1 : a.g0);
   RowUpdate up{&a, vold, cur ? a.v0 : a.v1, cur ? a.g0 : a.g1, vload(&c->dprev[1])};
-  for (int32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    prg_tile<WEIGHTED>(sm, a.off, a.idx, a.wts, a.n, t, a.tx[t], a.ty[t], a.tx[t + 1], a.ty[t + 1], a.carry_row,
-                       a.carry_val, a.head_row, a.head_val, [&](int32_t col) { return gold[col]; }, up);
+  const bool ok = prg_run<WEIGHTED>(sm, prg_graph_of(a), [&](int32_t col) { return __ldg(gold + col); }, up);
+  if (!ok && threadIdx.x == 0) {
+    c->status = MG_ERR_TIMEOUT;
+    c->done = 1;
   }
   const double r = block_sum<PRG_NT>(up.resid, s_red);
   const double d = block_sum<PRG_NT>(up.red2, s_red);
@@ -266,11 +270,13 @@ struct RowSumWrite {
 };
 
 __global__ void __launch_bounds__(PRG_NT) rowsum_kernel(SolveArgs a, float *s) {
-  __shared__ PrgShared sm;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PrgSmem<true> &sm = *reinterpret_cast<PrgSmem<true> *>(smem_raw);
   RowSumWrite wr{s};
-  for (int32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x)
-    prg_tile<true>(sm, a.off, a.idx, a.wts, a.n, t, a.tx[t], a.ty[t], a.tx[t + 1], a.ty[t + 1], a.carry_row,
-                   a.carry_val, a.head_row, a.head_val, [](int32_t) { return 1.0f; }, wr);
+  if (!prg_run<true>(sm, prg_graph_of(a), [](int32_t) { return 1.0f; }, wr) && threadIdx.x == 0) {
+    a.ctl->status = MG_ERR_TIMEOUT;
+    a.ctl->done = 1;
+  }
 }
 
 __global__ void rowsum_fixup_kernel(SolveArgs a, float *s) {
@@ -288,10 +294,20 @@ __global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
 // ---------------------------------------------------------------------------
 // Host side of the gather-based solvers.
 
-struct SolveBuffers {
-  mg::SolveArgs a;
-  float *srow_csr;
-};
+// Opts the pipelined gather kernels into their dynamic shared memory and returns
+// the persistent grid size (SMs x resident CTAs per SM).
+static int gather_grid(mg_graph *g, bool weighted) {
+  using namespace mg;
+  const int sm_w = (int)prg_smem_bytes<true>(), sm_u = (int)prg_smem_bytes<false>();
+  cudaFuncSetAttribute(solve_gather_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_w);
+  cudaFuncSetAttribute(solve_gather_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_u);
+  cudaFuncSetAttribute(rowsum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_w);
+  int occ = 0;
+  if (weighted) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_gather_kernel<true>, PRG_NT, sm_w);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_gather_kernel<false>, PRG_NT, sm_u);
+  cudaGetLastError();
+  return g->num_sms * std::max(1, std::min(occ, 8));
+}
 
 // Carves the solver's buffers out of ws_main and computes the row sums s_u.
 static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, mg::SolveArgs &a, size_t extra_floats,
@@ -303,7 +319,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, mg::Solve
   if (weighted) MG_TRY(get_plan(g, true, &plan_rows));
   const int64_t n = g->n;
   const int32_t nt = std::max(plan->ntiles, plan_rows ? plan_rows->ntiles : 0);
-  const int g1 = g->num_sms * PR_K1_PER_SM;
+  const int g1 = gather_grid(g, weighted);
   const int g2 = std::max(1, (nt + PRG_NT - 1) / PRG_NT);
   const int ginit = g->num_sms * 8;
   const int gp = std::max(std::max(g1, g2), ginit);
@@ -345,7 +361,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, mg::Solve
     r.tx = plan_rows->tx;
     r.ty = plan_rows->ty;
     r.ntiles = plan_rows->ntiles;
-    rowsum_kernel<<<g1, PRG_NT, 0, s>>>(r, srow);
+    rowsum_kernel<<<g1, PRG_NT, prg_smem_bytes<true>(), s>>>(r, srow);
     rowsum_fixup_kernel<<<g2, PRG_NT, 0, s>>>(r, srow);
   }
   a.off = adjoint ? g->ro : g->co;
@@ -380,8 +396,8 @@ static mg_status solve_run(mg_graph *g, mg::SolveArgs &a, bool weighted, int use
     SolveArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
-    if (weighted) solve_gather_kernel<true><<<g1, PRG_NT, 0, st>>>(b);
-    else solve_gather_kernel<false><<<g1, PRG_NT, 0, st>>>(b);
+    if (weighted) solve_gather_kernel<true><<<g1, PRG_NT, prg_smem_bytes<true>(), st>>>(b);
+    else solve_gather_kernel<false><<<g1, PRG_NT, prg_smem_bytes<false>(), st>>>(b);
     solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
   };
   MG_TRY(run_loop(g, slot, &sig, sizeof(sig), use_graph >= 0, body, (int64_t)a.max_iter + 2));
@@ -662,6 +678,7 @@ static mg_status pagerank_refcompat(mg_graph *g, float *ranks, const mg_pr_opts 
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
+    stats->launches = 1 + (o.use_graph >= 0 ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
   }
   if (hc.status != 0) {
     mg_set_error("mg_pagerank: device status %d", hc.status);
@@ -712,6 +729,8 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
+    // fill + row sums (1 or 2) + init + init reduce + per iteration gather, fix-up (+ loop guard)
+    stats->launches = (weighted ? 5 : 4) + (o.use_graph >= 0 ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
   }
   return MG_OK;
 }
@@ -764,6 +783,7 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
     total.edges_inspected += st.edges_inspected;
     total.bytes_compulsory += st.bytes_compulsory;
     total.kernel_ms += st.kernel_ms;
+    total.launches += st.launches;
     total.residual = std::max(total.residual, st.residual);
   }
   if (stats) *stats = total;

@@ -4,9 +4,17 @@
 //
 // Work split (merge path): the n row ends and the m edges form one sequence of
 // n + m items; tile t owns items [t*IPC, (t+1)*IPC). Tile coordinates (first row,
-// first edge) are precomputed once per graph. A tile stages its row ends and its
-// edge indices (and weights) in shared memory, each thread consumes IPT items,
-// and per-row sums are finished in three deterministic steps:
+// first edge) are precomputed once per graph.
+//
+// Each CTA is persistent and double-buffered: while it reduces tile k out of one
+// shared-memory stage, thread 0 has already issued the TMA bulk copies
+// (cp.async.bulk global->shared, completion counted on an mbarrier) of tile k+1's
+// row offsets, edge indices and edge weights into the other stage. The ranges are
+// widened to 16-byte boundaries (the graph arrays are padded for that), so the
+// copies are legal for any tile. Every mbarrier wait is bounded; a wait that runs
+// out sets MG_ERR_TIMEOUT and the CTA leaves.
+//
+// Per-row sums are finished in three deterministic steps:
 //   - inside a thread, rows that start and end in the thread are complete;
 //   - a thread's first completed row adds the carries of the preceding threads
 //     of the CTA that were still inside that row (in thread order);
@@ -26,6 +34,8 @@ namespace mg {
 constexpr int PRG_NT = 256;
 constexpr int PRG_IPT = 8;
 constexpr int PRG_IPC = PRG_NT * PRG_IPT;
+constexpr int PRG_STAGE = PRG_IPC + 8;  // widened to 16-byte boundaries on both sides
+constexpr uint32_t PRG_WAIT_LIMIT = 1u << 24;
 
 struct Comp {
   float hi, lo;
@@ -42,6 +52,48 @@ __device__ __forceinline__ void two_sum_add(Comp &c, float v) {
 __device__ __forceinline__ void comp_add(Comp &c, const Comp &d) {
   two_sum_add(c, d.hi);
   c.lo += d.lo;
+}
+
+// ---- mbarrier / bulk-copy primitives (sm_90+ PTX, single-CTA use) ----------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on phase `parity`; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t i = 0; i < PRG_WAIT_LIMIT; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
 }
 
 // Merge-path split of diagonal `diag`: number of row ends among the first
@@ -72,42 +124,67 @@ __global__ void prg_plan_kernel(const int32_t *__restrict__ off, int64_t n, int6
   }
 }
 
-struct PrgShared {
-  int32_t row_end[PRG_IPC + 1];
-  int32_t idx[PRG_IPC];
-  float w[PRG_IPC];
+// One shared-memory stage: widened copies of the tile's offsets (raw[k] =
+// off[xa + k]), edge indices (idx[k] = idx[ya + k]) and weights.
+template <bool WEIGHTED>
+struct PrgStage {
+  int32_t raw[PRG_STAGE];
+  int32_t idx[PRG_STAGE];
+  float w[WEIGHTED ? PRG_STAGE : 4];
+};
+
+template <bool WEIGHTED>
+struct PrgSmem {
+  PrgStage<WEIGHTED> st[2];
+  uint64_t bar[2];
   int32_t crow[PRG_NT];
   float chi[PRG_NT];
   float clo[PRG_NT];
-  int32_t beg0;
+  int32_t abort;
 };
 
-// One tile. `val(j)` returns the gathered value of local edge j (the neighbour's
-// value, times the edge weight when weighted, as an exact hi/lo pair through
-// `prod`). `finish(row, Comp)` consumes a completed row; rows begun in an earlier
-// tile are written to the head arrays instead.
+// The adjacency a gather runs over, with its plan and the carry arrays.
+struct PrgGraph {
+  const int32_t *off, *idx;
+  const float *wts;
+  const int32_t *tx, *ty;
+  int32_t ntiles;
+  int64_t n;
+  int32_t *carry_row, *head_row;
+  Comp *carry_val, *head_val;
+};
+
+// Issues the bulk copies of tile t into stage s (thread 0 only).
+template <bool WEIGHTED>
+__device__ __forceinline__ void prg_issue(PrgSmem<WEIGHTED> &sm, int s, const PrgGraph &g, int32_t t) {
+  const int64_t x0 = g.tx[t], y0 = g.ty[t], x1 = g.tx[t + 1], y1 = g.ty[t + 1];
+  const int64_t ya = y0 & ~(int64_t)3, yb = (y1 + 3) & ~(int64_t)3;
+  const int64_t xa = x0 & ~(int64_t)3, xb = (x1 + 2 + 3) & ~(int64_t)3;
+  const uint32_t bi = (uint32_t)((yb - ya) * 4), br = (uint32_t)((xb - xa) * 4);
+  fence_proxy_async();
+  mbar_arrive_expect_tx(&sm.bar[s], br + (WEIGHTED ? 2 : 1) * bi);
+  bulk_g2s(sm.st[s].raw, g.off + xa, br, &sm.bar[s]);
+  if (bi) {
+    bulk_g2s(sm.st[s].idx, g.idx + ya, bi, &sm.bar[s]);
+    if (WEIGHTED) bulk_g2s(sm.st[s].w, g.wts + ya, bi, &sm.bar[s]);
+  }
+}
+
+// Reduces one staged tile. `gather(col)` returns the neighbour's value;
+// `finish(row, Comp)` consumes a completed row.
 template <bool WEIGHTED, typename Gather, typename Finish>
-__device__ __forceinline__ void prg_tile(PrgShared &sm, const int32_t *__restrict__ off,
-                                         const int32_t *__restrict__ idx, const float *__restrict__ wts, int64_t n,
-                                         int32_t t, int32_t x0, int32_t y0, int32_t x1, int32_t y1,
-                                         int32_t *__restrict__ carry_row, Comp *__restrict__ carry_val,
-                                         int32_t *__restrict__ head_row, Comp *__restrict__ head_val,
-                                         Gather &&gather, Finish &&finish) {
+__device__ __forceinline__ void prg_compute(PrgSmem<WEIGHTED> &sm, const PrgStage<WEIGHTED> &st, const PrgGraph &g,
+                                            int32_t t, Gather &gather, Finish &finish) {
   const int tid = threadIdx.x;
+  const int32_t x0 = g.tx[t], y0 = g.ty[t], x1 = g.tx[t + 1], y1 = g.ty[t + 1];
   const int nrows = x1 - x0, nedges = y1 - y0;
-  for (int i = tid; i < nrows; i += PRG_NT) sm.row_end[i] = off[x0 + i + 1];
-  if (tid == 0) {
-    sm.row_end[nrows] = (x1 < n) ? off[x1 + 1] : INT_MAX;
-    sm.beg0 = off[x0];
-  }
-  for (int j = tid; j < nedges; j += PRG_NT) {
-    sm.idx[j] = idx[y0 + j];
-    if (WEIGHTED) sm.w[j] = wts[y0 + j];
-  }
-  __syncthreads();
+  const int32_t *rend = st.raw + (x0 & 3) + 1;  // rend[i] = off[x0 + i + 1]; rend[nrows] is INT_MAX past n
+  const int32_t beg0 = st.raw[x0 & 3];          // off[x0]
+  const int32_t *sidx = st.idx + (y0 & 3);
+  const float *sw = st.w + (y0 & 3);
   const int total = nrows + nedges;
   const int d0 = min(tid * PRG_IPT, total);
-  int lx = merge_split(sm.row_end, nrows, y0, nedges, d0);
+  int lx = merge_split(rend, nrows, y0, nedges, d0);
   int ly = d0 - lx;
   // Pass 1: classify the thread's items and issue every neighbour load.
   int e_of[PRG_IPT];
@@ -118,7 +195,7 @@ __device__ __forceinline__ void prg_tile(PrgShared &sm, const int32_t *__restric
     for (int k = 0; k < PRG_IPT; k++) {
       e_of[k] = -2;  // past the tile
       if (d0 + k < total) {
-        if (cy < nedges && y0 + cy < sm.row_end[cx]) {
+        if (cy < nedges && y0 + cy < rend[cx]) {
           e_of[k] = cy;
           cy++;
         } else {
@@ -132,13 +209,13 @@ __device__ __forceinline__ void prg_tile(PrgShared &sm, const int32_t *__restric
       v_hi[k] = 0.f;
       v_lo[k] = 0.f;
       if (e_of[k] >= 0) {
-        const float g = gather(sm.idx[e_of[k]]);
+        const float gv = gather(sidx[e_of[k]]);
         if (WEIGHTED) {
-          const float a = sm.w[e_of[k]];
-          v_hi[k] = a * g;
-          v_lo[k] = __fmaf_rn(a, g, -v_hi[k]);
+          const float a = sw[e_of[k]];
+          v_hi[k] = a * gv;
+          v_lo[k] = __fmaf_rn(a, gv, -v_hi[k]);
         } else {
-          v_hi[k] = g;
+          v_hi[k] = gv;
         }
       }
     }
@@ -176,9 +253,9 @@ __device__ __forceinline__ void prg_tile(PrgShared &sm, const int32_t *__restric
     Comp tot{0.f, 0.f};
     for (int q = t0; q < tid; q++) comp_add(tot, Comp{sm.chi[q], sm.clo[q]});
     comp_add(tot, f_val);
-    if (f_row == 0 && y0 > sm.beg0) {
-      head_row[t] = x0;
-      head_val[t] = tot;
+    if (f_row == 0 && y0 > beg0) {
+      g.head_row[t] = x0;
+      g.head_val[t] = tot;
     } else {
       finish(x0 + f_row, tot);
     }
@@ -189,10 +266,39 @@ __device__ __forceinline__ void prg_tile(PrgShared &sm, const int32_t *__restric
     while (t0 > 0 && sm.crow[t0 - 1] == r) t0--;
     Comp tot{0.f, 0.f};
     for (int q = t0; q < PRG_NT; q++) comp_add(tot, Comp{sm.chi[q], sm.clo[q]});
-    carry_row[t] = x0 + r;
-    carry_val[t] = tot;
+    g.carry_row[t] = x0 + r;
+    g.carry_val[t] = tot;
+  }
+}
+
+// Persistent double-buffered loop over tiles blockIdx.x, +gridDim.x, ...
+// Returns false if a bounded wait ran out (the caller reports MG_ERR_TIMEOUT).
+template <bool WEIGHTED, typename Gather, typename Finish>
+__device__ __forceinline__ bool prg_run(PrgSmem<WEIGHTED> &sm, const PrgGraph &g, Gather &&gather, Finish &&finish) {
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.bar[0], 1);
+    mbar_init(&sm.bar[1], 1);
+    fence_barrier_init();
+    if ((int32_t)blockIdx.x < g.ntiles) prg_issue<WEIGHTED>(sm, 0, g, blockIdx.x);
   }
   __syncthreads();
+  uint32_t phase[2] = {0u, 0u};
+  int k = 0;
+  for (int32_t t = blockIdx.x; t < g.ntiles; t += gridDim.x, k++) {
+    const int s = k & 1;
+    const int32_t tn = t + gridDim.x;
+    if (threadIdx.x == 0 && tn < g.ntiles) prg_issue<WEIGHTED>(sm, s ^ 1, g, tn);
+    const bool ok = mbar_wait_bounded(&sm.bar[s], phase[s]);
+    if (__syncthreads_or(!ok)) {
+      // Give the copy in flight for the next tile a bounded chance to land.
+      if (tn < g.ntiles) mbar_wait_bounded(&sm.bar[s ^ 1], phase[s ^ 1]);
+      return false;
+    }
+    phase[s] ^= 1u;
+    prg_compute<WEIGHTED>(sm, sm.st[s], g, t, gather, finish);
+    __syncthreads();
+  }
+  return true;
 }
 
 // Cross-tile fix-up of the row begun before tile t (if any): adds the carries of
@@ -210,6 +316,11 @@ __device__ __forceinline__ void prg_fixup_tile(int32_t t, const int32_t *__restr
   comp_add(tot, head_val[t]);
   head_row[t] = -1;
   finish(r, tot);
+}
+
+template <bool WEIGHTED>
+constexpr size_t prg_smem_bytes() {
+  return sizeof(PrgSmem<WEIGHTED>);
 }
 
 }  // namespace mg

@@ -279,6 +279,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
+    stats->launches = 2 + (o.use_graph >= 0 ? 2 * (int64_t)hc.body_iters : (int64_t)hc.level);
   }
   if (hc.status != 0) {
     mg_set_error("mg_sssp: device status %d (queue capacity %d)", hc.status, qcap);

@@ -159,6 +159,13 @@ class Graph:
     def __exit__(self, *a):
         self.close()
 
+    @property
+    def stream_ptr(self) -> int:
+        """cudaStream_t of the graph as an integer (for torch.cuda.ExternalStream)."""
+        p = C.c_void_p()
+        _check(self._lib.mg_graph_stream(self._h, C.byref(p)), "mg_graph_stream")
+        return p.value or 0
+
     def device_arrays(self) -> dict:
         ptrs = [C.c_void_p() for _ in range(6)]
         _check(self._lib.mg_graph_device_arrays(self._h, *[C.byref(p) for p in ptrs]), "mg_graph_device_arrays")

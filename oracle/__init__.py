@@ -96,7 +96,7 @@ def _ref_lib():
         lib.mgref_sssp.restype = C.c_double
         lib.mgref_cc.argtypes = [C.c_int, C.c_int, _I, _I, _I, _I, _I]
         lib.mgref_cc.restype = C.c_double
-        lib.mgref_pr.argtypes = [C.c_int, C.c_int, _I, _I, _I, _I, _F]
+        lib.mgref_pr.argtypes = [C.c_int, C.c_int, _I, _I, _I, _I, _F, _I]
         lib.mgref_pr.restype = C.c_double
         lib.mgref_load_market.argtypes = [C.c_char_p, _I, _I]
         lib.mgref_load_market.restype = C.c_void_p
@@ -289,14 +289,16 @@ class Ref:
         return out, t
 
     @staticmethod
-    def pr(ro, ci, csc=None):
+    def pr(ro, ci, csc=None, with_sweeps=False):
         lib = _ref_lib()
         n, m = len(ro) - 1, len(ci)
         co, ri, _ = Ref._csc(ro, ci, csc)
         out = np.empty(n, dtype=np.float32)
+        sweeps = C.c_int32(-1)
         keep = [_keep_i(a) for a in (ro, ci, co, ri)]
-        t = lib.mgref_pr(n, m, keep[0][1], keep[1][1], keep[2][1], keep[3][1], out.ctypes.data_as(_F))
-        return out, t
+        t = lib.mgref_pr(n, m, keep[0][1], keep[1][1], keep[2][1], keep[3][1], out.ctypes.data_as(_F),
+                         C.byref(sweeps))
+        return (out, t, sweeps.value) if with_sweeps else (out, t)
 
     @staticmethod
     def load_market(path):

@@ -19,6 +19,7 @@
 #include <set>
 #include <numeric>
 #include <iostream>
+#include <string>
 #include <algorithm>
 #include <unistd.h>
 #include <fcntl.h>
@@ -42,19 +43,30 @@ struct cc { typedef int DataType; static const int INIT_VALUE = INT_MAX; };
 
 namespace {
 
+// Redirects stdout (fd 1) to a temporary file for the lifetime of the object;
+// text() returns what was printed meanwhile.
 struct Quiet {
   int saved;
+  FILE *tmp;
   Quiet() {
     fflush(stdout);
     saved = dup(1);
-    int devnull = open("/dev/null", O_WRONLY);
-    dup2(devnull, 1);
-    close(devnull);
+    tmp = tmpfile();
+    dup2(fileno(tmp), 1);
+  }
+  std::string text() {
+    fflush(stdout);
+    long len = ftell(tmp);
+    std::string s(len > 0 ? (size_t)len : 0, '\0');
+    rewind(tmp);
+    if (len > 0) fread(&s[0], 1, (size_t)len, tmp);
+    return s;
   }
   ~Quiet() {
     fflush(stdout);
     dup2(saved, 1);
     close(saved);
+    fclose(tmp);
   }
 };
 
@@ -114,13 +126,18 @@ double mgref_cc(int n, int m, const int* ro, const int* ci, const int* co, const
 
 // CPUPR (Algorithms/PageRank/PageRank.cu:108-163): Gauss-Seidel sweeps of
 // x = 0.15 + 0.85 * sum x_u/outdeg_u over the CSC, stopping when no |dx| >= 0.01.
+// *sweeps gets the sweep count the function prints ("CPU iterations: N").
 double mgref_pr(int n, int m, const int* ro, const int* ci, const int* co, const int* ri,
-                float* rank) {
+                float* rank, int* sweeps) {
   CsrGraph<int, float, int> g = view<float>(n, m, ro, ci, co, ri, NULL);
   Quiet q;
   auto t0 = std::chrono::steady_clock::now();
   CPUPR<int, float, int>(g, rank);
-  return seconds_since(t0);
+  double t = seconds_since(t0);
+  std::string out = q.text();
+  size_t at = out.find("CPU iterations:");
+  *sweeps = at == std::string::npos ? -1 : atoi(out.c_str() + at + 15);
+  return t;
 }
 
 // The reference's Matrix Market ingest: BuildMarketGraph<true> with undirected=false
