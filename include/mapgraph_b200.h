@@ -101,7 +101,9 @@ typedef struct mg_pr_opts {
   int32_t compensated;   /* 1: two-sum compensated FP32 accumulation [1]; -1 plain FP32 sums */
   int32_t device_output; /* 1: ranks/teleport/gradient arrays are device pointers */
   int32_t use_graph;     /* as mg_opts.use_graph */
-  int32_t reserved[3];
+  int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps [default],
+                            1 merge-path tiles staged in shared memory by TMA bulk copies */
+  int32_t reserved[2];
 } mg_pr_opts;
 
 /* ---- status ------------------------------------------------------------- */

@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "engine.cuh"
 #include "expand.cuh"
+#include "pr_binned.cuh"
 #include "pr_gather.cuh"
 
 namespace mg {
@@ -39,6 +40,8 @@ struct GatherPlan {
 
 struct PlanSet {
   GatherPlan csc, csr;
+  BinPlan bcsc, bcsr;
+  bool bcsc_ok = false, bcsr_ok = false;
 };
 
 }  // namespace mg
@@ -54,6 +57,11 @@ void pr_release_plans(mg_graph *g) {
   for (mg::GatherPlan *p : {&ps->csc, &ps->csr}) {
     if (p->tx) cudaFree(p->tx);
     if (p->ty) cudaFree(p->ty);
+  }
+  for (mg::BinPlan *b : {&ps->bcsc, &ps->bcsr}) {
+    for (void *q : {(void *)b->rows, (void *)b->hrows, (void *)b->hbase, (void *)b->hcount, (void *)b->hpart,
+                    (void *)b->hcontrib})
+      if (q) cudaFree(q);
   }
   delete ps;
   g->plan_csc = nullptr;
@@ -77,7 +85,91 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
   return MG_OK;
 }
 
+// Degree-binned plan of the CSC (forward gather) or the CSR (adjoint, row sums).
+static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
+  using namespace mg;
+  PlanSet *ps = plans_of(g);
+  BinPlan &bp = csr ? ps->bcsr : ps->bcsc;
+  bool &ok = csr ? ps->bcsr_ok : ps->bcsc_ok;
+  if (!ok) {
+    const int32_t *off = csr ? g->ro : g->co;
+    const int64_t n = g->n;
+    cudaStream_t s = g->stream;
+    unsigned long long *dcnt = nullptr, *dcur = nullptr;
+    int64_t *dboff = nullptr;
+    MG_CUDA_TRY(cudaMalloc((void **)&dcnt, sizeof(unsigned long long) * 2 * (PRB_BINS + 1) + sizeof(int64_t) * (PRB_BINS + 1)));
+    dcur = dcnt + (PRB_BINS + 1);
+    dboff = reinterpret_cast<int64_t *>(dcur + (PRB_BINS + 1));
+    MG_CUDA_TRY(cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 2 * (PRB_BINS + 1), s));
+    prb_count_kernel<<<g->num_sms * 4, 256, 0, s>>>(off, n, dcnt);
+    unsigned long long cnt[PRB_BINS + 1];
+    MG_CUDA_TRY(cudaMemcpyAsync(cnt, dcnt, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t acc = 0;
+    for (int b = 0; b < PRB_BINS; b++) {
+      bp.boff[b] = acc;
+      if (b < 6) acc += (int64_t)cnt[b];
+    }
+    bp.boff[PRB_BINS] = acc;
+    bp.boff[6] = acc;
+    bp.nheavy = (int64_t)cnt[6];
+    bp.ntasks = (int64_t)cnt[PRB_BINS];
+    const int groups[6] = {1, 2, 4, 8, 16, 32};
+    int64_t w = 0;
+    for (int b = 0; b < PRB_BINS; b++) {
+      bp.wstart[b] = w;
+      if (b < 5) w += ((int64_t)cnt[b] * groups[b] + 31) / 32;
+      else if (b == 5) w += (int64_t)cnt[5];
+      else w += bp.ntasks;
+    }
+    bp.wstart[PRB_BINS] = w;
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.rows, sizeof(int32_t) * std::max<int64_t>(acc, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.hrows, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.hbase, sizeof(int32_t) * (bp.nheavy + 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.hcount, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.hpart, sizeof(Comp) * std::max<int64_t>(bp.ntasks, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
+    MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
+    MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
+    prb_scatter_kernel<<<g->num_sms * 4, 256, 0, s>>>(off, n, dboff, dcur, bp.rows, bp.hrows);
+    prb_hubs_kernel<<<1, 32, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
+    MG_CUDA_TRY(cudaGetLastError());
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(dcnt);
+    ok = true;
+  }
+  *out = &bp;
+  return MG_OK;
+}
+
+static mg::PrbArgs prb_args_of(const mg_graph *g, const mg::BinPlan &bp, bool csr, const float *wts) {
+  mg::PrbArgs p;
+  p.off = csr ? g->ro : g->co;
+  p.idx = csr ? g->ci : g->ri;
+  p.wts = wts;
+  p.rows = bp.rows;
+  p.hrows = bp.hrows;
+  p.hbase = bp.hbase;
+  p.hcount = bp.hcount;
+  p.hpart = bp.hpart;
+  p.hcontrib = bp.hcontrib;
+  for (int b = 0; b <= mg::PRB_BINS; b++) {
+    p.boff[b] = bp.boff[b];
+    p.wstart[b] = bp.wstart[b];
+  }
+  p.nheavy = bp.nheavy;
+  return p;
+}
+
 namespace mg {
+
+// Per-row inputs of the row update.
+struct RowIn {
+  float vold;  // previous iterate
+  float s;     // row sum s_r (0: dangling)
+  double t;    // teleport entry
+  float w;     // adjoint right-hand side
+};
 
 // Shared arguments of the gather-based solvers (forward and adjoint).
 struct SolveArgs {
@@ -93,6 +185,8 @@ struct SolveArgs {
   const float *srow;          // s_u, 0 for dangling
   const float *tele;          // teleport (nullptr: uniform tn)
   const float *wvec;          // adjoint right-hand side dL/dx (nullptr forward)
+  int32_t soff;               // row sums are the gathered adjacency's degrees (read from its offsets)
+  int32_t ri_srow, ri_tele, ri_wvec;  // stage slots of the per-row arrays (-1: not staged; slot 0: iterate)
   double tn, alpha, tol;
   int32_t max_iter;
   int32_t adjoint;
@@ -116,25 +210,45 @@ struct RowUpdate {
   float *vnew, *gnew;
   double scal;  // forward: dangling mass d of the current iterate; adjoint: t.lambda
   double resid = 0.0, red2 = 0.0;
-  __device__ __forceinline__ void operator()(int32_t r, Comp v) {
+
+  __device__ __forceinline__ void apply(int32_t r, Comp v, const RowIn &in) {
     const double acc = (double)v.hi + (double)v.lo;
-    const double s = (double)a->srow[r];
+    const double s = (double)in.s;
     double nv;
     if (!a->adjoint) {
-      const double t = tele_of(*a, r);
-      nv = a->alpha * (acc + scal * t) + (1.0 - a->alpha) * t;
+      nv = a->alpha * (acc + scal * in.t) + (1.0 - a->alpha) * in.t;
       if (s > 0.0) gnew[r] = (float)(nv / s);
       else {
         gnew[r] = 0.f;
         red2 += nv;
       }
     } else {
-      nv = (double)a->wvec[r] + a->alpha * (s > 0.0 ? acc / s : scal);
-      red2 += tele_of(*a, r) * nv;
+      nv = (double)in.w + a->alpha * (s > 0.0 ? acc / s : scal);
+      red2 += in.t * nv;
     }
     const float nf = (float)nv;
-    resid += fabs((double)nf - (double)vold[r]);
+    resid += fabs((double)nf - (double)in.vold);
     vnew[r] = nf;
+  }
+  // Row inputs from global memory (rows finished by the fix-up kernel).
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) {
+    RowIn in;
+    in.vold = vold[r];
+    in.s = a->soff ? (float)(a->off[r + 1] - a->off[r]) : a->srow[r];
+    in.t = tele_of(*a, r);
+    in.w = a->wvec ? a->wvec[r] : 0.f;
+    apply(r, v, in);
+  }
+  // Row inputs from the staged tile.
+  template <typename Stage>
+  __device__ __forceinline__ void operator()(int32_t r, Comp v, const Stage &st) {
+    const int j = r - st.coord[4];
+    RowIn in;
+    in.vold = st.rows[0][j];
+    in.s = a->soff ? (float)(st.raw[j + 1] - st.raw[j]) : st.rows[a->ri_srow][j];
+    in.t = a->ri_tele >= 0 ? (double)st.rows[a->ri_tele][j] : a->tn;
+    in.w = a->ri_wvec >= 0 ? st.rows[a->ri_wvec][j] : 0.f;
+    apply(r, v, in);
   }
 };
 
@@ -147,13 +261,15 @@ __device__ __forceinline__ bool solve_skip(const SolveArgs &a) {
 }
 
 __device__ __forceinline__ PrgGraph prg_graph_of(const SolveArgs &a) {
-  return PrgGraph{a.off, a.idx, a.wts, a.tx, a.ty, a.ntiles, a.n, a.carry_row, a.head_row, a.carry_val, a.head_val};
+  PrgGraph g{a.off, a.idx, a.wts, a.tx, a.ty, a.ntiles, a.n, a.carry_row, a.head_row, a.carry_val, a.head_val,
+             {nullptr, nullptr, nullptr, nullptr}};
+  return g;
 }
 
-template <bool WEIGHTED>
+template <bool WEIGHTED, int NR>
 __global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  PrgSmem<WEIGHTED> &sm = *reinterpret_cast<PrgSmem<WEIGHTED> *>(smem_raw);
+  PrgSmem<WEIGHTED, NR> &sm = *reinterpret_cast<PrgSmem<WEIGHTED, NR> *>(smem_raw);
   __shared__ double s_red[PRG_NT / 32 + 1];
   if (solve_skip(a)) return;
   DevCtl *c = a.ctl;
@@ -161,7 +277,12 @@ __global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
   const float *vold = cur ? a.v1 : a.v0;
   const float *__restrict__ gold = a.adjoint ? vold : (cur ? a.g1 : a.g0);
   RowUpdate up{&a, vold, cur ? a.v0 : a.v1, cur ? a.g0 : a.g1, vload(&c->dprev[1])};
-  const bool ok = prg_run<WEIGHTED>(sm, prg_graph_of(a), [&](int32_t col) { return __ldg(gold + col); }, up);
+  PrgGraph pg = prg_graph_of(a);
+  pg.rowsrc[0] = vold;
+  if (a.ri_srow >= 0) pg.rowsrc[a.ri_srow] = a.srow;
+  if (a.ri_tele >= 0) pg.rowsrc[a.ri_tele] = a.tele;
+  if (a.ri_wvec >= 0) pg.rowsrc[a.ri_wvec] = a.wvec;
+  const bool ok = prg_run<WEIGHTED, NR>(sm, pg, [&](int32_t col) { return __ldg(gold + col); }, up);
   if (!ok && threadIdx.x == 0) {
     c->status = MG_ERR_TIMEOUT;
     c->done = 1;
@@ -172,6 +293,80 @@ __global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
     a.part1[2 * blockIdx.x] = r;
     a.part1[2 * blockIdx.x + 1] = d;
   }
+}
+
+// Last CTA of an iteration: fixed-order FP64 reduction of the per-CTA partials
+// (and of the hub contributions), then the convergence decision.
+__device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *hcontrib, int64_t nheavy,
+                                    double *s_red) {
+  DevCtl *c = a.ctl;
+  double r = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < a.grid1; i += blockDim.x) {
+    r += a.part1[2 * i];
+    d += a.part1[2 * i + 1];
+  }
+  for (int i = threadIdx.x; i < a.grid2; i += blockDim.x) {
+    r += a.part2[2 * i];
+    d += a.part2[2 * i + 1];
+  }
+  for (int64_t i = threadIdx.x; i < nheavy; i += blockDim.x) {
+    r += __ldcg(hcontrib + 2 * i);
+    d += __ldcg(hcontrib + 2 * i + 1);
+  }
+  r = block_sum<PRG_NT>(r, s_red);
+  d = block_sum<PRG_NT>(d, s_red);
+  if (threadIdx.x == 0) {
+    const int lvl = c->level + 1;
+    c->level = lvl;
+    c->dsum[0] = r;
+    c->dprev[1] = d;
+    c->cur = cur ^ 1;
+    c->blocks_done = 0;
+    const bool done = r < a.tol || lvl >= a.max_iter || c->status != 0;
+    __threadfence();
+    c->done = done ? 1 : 0;
+    if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+  }
+}
+
+// One whole iteration of the degree-binned solver.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(PRB_NT) solve_binned_kernel(SolveArgs a, PrbArgs p) {
+  __shared__ double s_red[PRB_NT / 32 + 1];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *vold = cur ? a.v1 : a.v0;
+  const float *__restrict__ gold = a.adjoint ? vold : (cur ? a.g1 : a.g0);
+  float *vnew = cur ? a.v0 : a.v1, *gnew = cur ? a.g0 : a.g1;
+  const double scal = vload(&c->dprev[1]);
+  RowUpdate up{&a, vold, vnew, gnew, scal};
+  auto hub = [&](int64_t h, int32_t row, Comp v) {
+    RowUpdate hu{&a, vold, vnew, gnew, scal};
+    hu(row, v);
+    p.hcontrib[2 * h] = hu.resid;
+    p.hcontrib[2 * h + 1] = hu.red2;
+    __threadfence();
+  };
+  prb_run<WEIGHTED>(p, [&](int32_t col) { return __ldg(gold + col); }, up, hub);
+  const double r = block_sum<PRB_NT>(up.resid, s_red);
+  const double d = block_sum<PRB_NT>(up.red2, s_red);
+  if (threadIdx.x == 0) {
+    a.part1[2 * blockIdx.x] = r;
+    a.part1[2 * blockIdx.x + 1] = d;
+  }
+  if (last_block(&c->blocks_done)) solve_iteration_end(a, cur, p.hcontrib, p.nheavy, s_red);
+}
+
+struct RowSumStore {
+  float *s;
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) { s[r] = v.hi + v.lo; }
+};
+
+// Row sums s_u of the weighted CSR through the binned gather (unit gathered values).
+__global__ void __launch_bounds__(PRB_NT) rowsum_binned_kernel(PrbArgs p, float *s) {
+  RowSumStore st{s};
+  prb_run<true>(p, [](int32_t) { return 1.0f; }, st, [&](int64_t, int32_t row, Comp v) { s[row] = v.hi + v.lo; });
 }
 
 __global__ void __launch_bounds__(PRG_NT) solve_fixup_kernel(SolveArgs a) {
@@ -191,31 +386,7 @@ __global__ void __launch_bounds__(PRG_NT) solve_fixup_kernel(SolveArgs a) {
       a.part2[2 * blockIdx.x + 1] = d;
     }
   }
-  if (!last_block(&c->blocks_done)) return;
-  // Fixed-order FP64 reduction of every CTA's partials.
-  double r = 0.0, d = 0.0;
-  for (int i = threadIdx.x; i < a.grid1; i += PRG_NT) {
-    r += a.part1[2 * i];
-    d += a.part1[2 * i + 1];
-  }
-  for (int i = threadIdx.x; i < a.grid2; i += PRG_NT) {
-    r += a.part2[2 * i];
-    d += a.part2[2 * i + 1];
-  }
-  r = block_sum<PRG_NT>(r, s_red);
-  d = block_sum<PRG_NT>(d, s_red);
-  if (threadIdx.x == 0) {
-    const int lvl = c->level + 1;
-    c->level = lvl;
-    c->dsum[0] = r;
-    c->dprev[1] = d;
-    c->cur = cur ^ 1;
-    c->blocks_done = 0;
-    const bool done = r < a.tol || lvl >= a.max_iter;
-    __threadfence();
-    c->done = done ? 1 : 0;
-    if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
-  }
+  if (last_block(&c->blocks_done)) solve_iteration_end(a, cur, nullptr, 0, s_red);
 }
 
 // Initial iterate. Forward: x0 = t, g0 = t/s; partial sums of the dangling mass.
@@ -264,27 +435,6 @@ __global__ void outdeg_kernel(const int32_t *__restrict__ ro, int64_t n, float *
     s[i] = (float)(ro[i + 1] - ro[i]);
 }
 
-struct RowSumWrite {
-  float *s;
-  __device__ __forceinline__ void operator()(int32_t r, Comp v) { s[r] = v.hi + v.lo; }
-};
-
-__global__ void __launch_bounds__(PRG_NT) rowsum_kernel(SolveArgs a, float *s) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  PrgSmem<true> &sm = *reinterpret_cast<PrgSmem<true> *>(smem_raw);
-  RowSumWrite wr{s};
-  if (!prg_run<true>(sm, prg_graph_of(a), [](int32_t) { return 1.0f; }, wr) && threadIdx.x == 0) {
-    a.ctl->status = MG_ERR_TIMEOUT;
-    a.ctl->done = 1;
-  }
-}
-
-__global__ void rowsum_fixup_kernel(SolveArgs a, float *s) {
-  RowSumWrite wr{s};
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.ntiles; t += (int64_t)gridDim.x * blockDim.x)
-    prg_fixup_tile((int32_t)t, a.carry_row, a.carry_val, a.head_row, a.head_val, wr);
-}
-
 __global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -294,90 +444,145 @@ __global__ void fill_i32_kernel(int32_t *p, int64_t n, int32_t v) {
 // ---------------------------------------------------------------------------
 // Host side of the gather-based solvers.
 
-// Opts the pipelined gather kernels into their dynamic shared memory and returns
-// the persistent grid size (SMs x resident CTAs per SM).
-static int gather_grid(mg_graph *g, bool weighted) {
-  using namespace mg;
-  const int sm_w = (int)prg_smem_bytes<true>(), sm_u = (int)prg_smem_bytes<false>();
-  cudaFuncSetAttribute(solve_gather_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_w);
-  cudaFuncSetAttribute(solve_gather_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_u);
-  cudaFuncSetAttribute(rowsum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_w);
-  int occ = 0;
-  if (weighted) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_gather_kernel<true>, PRG_NT, sm_w);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_gather_kernel<false>, PRG_NT, sm_u);
-  cudaGetLastError();
-  return g->num_sms * std::max(1, std::min(occ, 8));
+// Kernel variants of the pipelined gather: edge weights or not, and how many
+// per-row arrays the tiles stage (1..4).
+using GatherLaunch = void (*)(int grid, cudaStream_t st, const mg::SolveArgs &b);
+
+template <bool W, int NR>
+static void launch_gather(int grid, cudaStream_t st, const mg::SolveArgs &b) {
+  mg::solve_gather_kernel<W, NR><<<grid, mg::PRG_NT, mg::prg_smem_bytes<W, NR>(), st>>>(b);
 }
 
-// Carves the solver's buffers out of ws_main and computes the row sums s_u.
-static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, mg::SolveArgs &a, size_t extra_floats,
-                             float **extra) {
+// Opts a variant into its dynamic shared memory; returns resident CTAs per SM.
+template <bool W, int NR>
+static int prepare_gather() {
+  const int bytes = (int)mg::prg_smem_bytes<W, NR>();
+  cudaFuncSetAttribute(mg::solve_gather_kernel<W, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::solve_gather_kernel<W, NR>, mg::PRG_NT, bytes);
+  cudaGetLastError();
+  return occ;
+}
+
+static GatherLaunch gather_variant(bool w, int nr, int *occ) {
+  switch (nr + (w ? 8 : 0)) {
+    case 1: *occ = prepare_gather<false, 1>(); return launch_gather<false, 1>;
+    case 2: *occ = prepare_gather<false, 2>(); return launch_gather<false, 2>;
+    case 3: *occ = prepare_gather<false, 3>(); return launch_gather<false, 3>;
+    case 4: *occ = prepare_gather<false, 4>(); return launch_gather<false, 4>;
+    case 9: *occ = prepare_gather<true, 1>(); return launch_gather<true, 1>;
+    case 10: *occ = prepare_gather<true, 2>(); return launch_gather<true, 2>;
+    case 11: *occ = prepare_gather<true, 3>(); return launch_gather<true, 3>;
+    default: *occ = prepare_gather<true, 4>(); return launch_gather<true, 4>;
+  }
+}
+
+struct SolvePlan {
+  mg::SolveArgs a;
+  GatherLaunch gather;  // merge-path variant (use_tma)
+  mg::PrbArgs p;        // degree-binned variant (default)
+  bool weighted;
+  bool use_tma;
+};
+
+template <bool W>
+static int binned_occupancy() {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::solve_binned_kernel<W>, mg::PRB_NT, 0);
+  cudaGetLastError();
+  return std::max(1, std::min(occ, 8));
+}
+
+// Carves the solver's buffers out of ws_main (every per-vertex array padded to
+// n + 8 entries for the widened tile copies), copies the teleport vector and the
+// adjoint right-hand side into padded buffers, computes the row sums s_u and picks
+// the gather variant.
+static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const float *tele_src,
+                             const float *wvec_src, bool use_tma, SolvePlan &sp) {
   using namespace mg;
   GatherPlan *plan = nullptr;
-  MG_TRY(get_plan(g, adjoint, &plan));
-  GatherPlan *plan_rows = nullptr;
-  if (weighted) MG_TRY(get_plan(g, true, &plan_rows));
+  BinPlan *bins = nullptr, *rbins = nullptr;
+  if (use_tma) MG_TRY(get_plan(g, adjoint, &plan));
+  else MG_TRY(get_bin_plan(g, adjoint, &bins));
+  if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
-  const int32_t nt = std::max(plan->ntiles, plan_rows ? plan_rows->ntiles : 0);
-  const int g1 = gather_grid(g, weighted);
-  const int g2 = std::max(1, (nt + PRG_NT - 1) / PRG_NT);
+  const size_t np = (size_t)n + 8;
+  const int32_t nt = plan ? plan->ntiles : 1;
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  SolveArgs &a = sp.a;
+  std::memset(&a, 0, sizeof(a));
+  a.soff = adjoint ? !weighted : (symmetric && !weighted);
+  int nr = 1;
+  a.ri_srow = a.soff ? -1 : nr++;
+  a.ri_tele = tele_src ? nr++ : -1;
+  a.ri_wvec = adjoint ? nr++ : -1;
+  int occ = 0;
+  sp.use_tma = use_tma;
+  sp.weighted = weighted;
+  sp.gather = nullptr;
+  if (use_tma) sp.gather = gather_variant(weighted, nr, &occ);
+  else occ = weighted ? binned_occupancy<true>() : binned_occupancy<false>();
+  const int g1 = g->num_sms * std::max(1, std::min(occ, 8));
+  const int g2 = use_tma ? std::max(1, (nt + PRG_NT - 1) / PRG_NT) : 0;
   const int ginit = g->num_sms * 8;
   const int gp = std::max(std::max(g1, g2), ginit);
-  const size_t need = Carve::need({sizeof(float) * (size_t)n, sizeof(float) * (size_t)n, sizeof(float) * (size_t)n,
-                                   sizeof(float) * (size_t)n, sizeof(float) * (size_t)n,
+  const size_t need = Carve::need({sizeof(float) * np, sizeof(float) * np, sizeof(float) * np, sizeof(float) * np,
+                                   sizeof(float) * np, sizeof(float) * np, sizeof(float) * np,
                                    sizeof(int32_t) * (size_t)nt, sizeof(int32_t) * (size_t)nt,
                                    sizeof(Comp) * (size_t)nt, sizeof(Comp) * (size_t)nt,
-                                   sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp,
-                                   sizeof(float) * extra_floats});
+                                   sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
-  std::memset(&a, 0, sizeof(a));
-  a.v0 = cv.take<float>(n);
-  a.v1 = cv.take<float>(n);
-  a.g0 = cv.take<float>(n);
-  a.g1 = cv.take<float>(n);
-  float *srow = cv.take<float>(n);
+  a.v0 = cv.take<float>(np);
+  a.v1 = cv.take<float>(np);
+  a.g0 = cv.take<float>(np);
+  a.g1 = cv.take<float>(np);
+  float *srow = cv.take<float>(np);
+  float *tele = cv.take<float>(np);
+  float *wvec = cv.take<float>(np);
   a.carry_row = cv.take<int32_t>(nt);
   a.head_row = cv.take<int32_t>(nt);
   a.carry_val = cv.take<Comp>(nt);
   a.head_val = cv.take<Comp>(nt);
   a.part1 = cv.take<double>(2 * (size_t)gp);
   a.part2 = cv.take<double>(2 * (size_t)gp);
-  if (extra) *extra = cv.take<float>(extra_floats);
   a.n = n;
   a.srow = srow;
+  a.tele = tele_src ? tele : nullptr;
+  a.wvec = adjoint ? wvec : nullptr;
   a.grid1 = g1;
   a.grid2 = g2;
   a.ctl = g->ctl;
   cudaStream_t s = g->stream;
+  if (tele_src) MG_CUDA_TRY(cudaMemcpyAsync(tele, tele_src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+  if (adjoint && wvec_src)
+    MG_CUDA_TRY(cudaMemcpyAsync(wvec, wvec_src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
   fill_i32_kernel<<<g->num_sms * 4, 256, 0, s>>>(a.head_row, nt, -1);
   if (!weighted) {
     outdeg_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, n, srow);
   } else {
-    SolveArgs r = a;
-    r.off = g->ro;
-    r.idx = g->ci;
-    r.wts = (const float *)g->vals;
-    r.tx = plan_rows->tx;
-    r.ty = plan_rows->ty;
-    r.ntiles = plan_rows->ntiles;
-    rowsum_kernel<<<g1, PRG_NT, prg_smem_bytes<true>(), s>>>(r, srow);
-    rowsum_fixup_kernel<<<g2, PRG_NT, 0, s>>>(r, srow);
+    const PrbArgs rp = prb_args_of(g, *rbins, true, (const float *)g->vals);
+    rowsum_binned_kernel<<<g->num_sms * 8, PRB_NT, 0, s>>>(rp, srow);
   }
   a.off = adjoint ? g->ro : g->co;
   a.idx = adjoint ? g->ci : g->ri;
   a.wts = weighted ? (const float *)(adjoint ? g->vals : g->cvals) : nullptr;
-  a.tx = plan->tx;
-  a.ty = plan->ty;
-  a.ntiles = plan->ntiles;
+  if (plan) {
+    a.tx = plan->tx;
+    a.ty = plan->ty;
+    a.ntiles = plan->ntiles;
+  } else {
+    sp.p = prb_args_of(g, *bins, adjoint, a.wts);
+  }
   MG_CUDA_TRY(cudaGetLastError());
   return MG_OK;
 }
 
-// Runs the solver loop described by `a` (initial iterate set up by the init
+// Runs the solver loop described by `sp` (initial iterate set up by the init
 // kernels). Returns after the loop; results stay in a.v0/a.v1 at ctl->cur.
-static mg_status solve_run(mg_graph *g, mg::SolveArgs &a, bool weighted, int use_graph, int slot) {
+static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) {
   using namespace mg;
+  const SolveArgs &a = sp.a;
   cudaStream_t s = g->stream;
   const int ginit = g->num_sms * 8;
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
@@ -386,19 +591,32 @@ static mg_status solve_run(mg_graph *g, mg::SolveArgs &a, bool weighted, int use
   MG_CUDA_TRY(cudaGetLastError());
   struct Sig {
     SolveArgs a;
-    int w;
+    GatherLaunch gl;
+    PrbArgs p;
+    int w, tma;
   } sig;
   std::memset(&sig, 0, sizeof(sig));
   sig.a = a;
-  sig.w = weighted;
+  sig.gl = sp.gather;
+  sig.p = sp.p;
+  sig.w = sp.weighted;
+  sig.tma = sp.use_tma;
   const int g1 = a.grid1, g2 = a.grid2;
-  LoopBody body = [a, weighted, g1, g2](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+  const GatherLaunch gl = sp.gather;
+  const PrbArgs p = sp.p;
+  const bool tma = sp.use_tma, w = sp.weighted;
+  LoopBody body = [a, gl, p, g1, g2, tma, w](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
     SolveArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
-    if (weighted) solve_gather_kernel<true><<<g1, PRG_NT, prg_smem_bytes<true>(), st>>>(b);
-    else solve_gather_kernel<false><<<g1, PRG_NT, prg_smem_bytes<false>(), st>>>(b);
-    solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
+    if (tma) {
+      gl(g1, st, b);
+      solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
+    } else if (w) {
+      solve_binned_kernel<true><<<g1, PRB_NT, 0, st>>>(b, p);
+    } else {
+      solve_binned_kernel<false><<<g1, PRB_NT, 0, st>>>(b, p);
+    }
   };
   MG_TRY(run_loop(g, slot, &sig, sizeof(sig), use_graph >= 0, body, (int64_t)a.max_iter + 2));
   return MG_OK;
@@ -700,9 +918,9 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     mg_set_error("mg_pagerank: weighted mode needs float edge values");
     return MG_ERR_ARG;
   }
-  SolveArgs a;
-  MG_TRY(solve_setup(g, false, weighted, a, 0, nullptr));
-  a.tele = tele_dev;
+  SolvePlan sp;
+  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, o.gather_kernel == 1, sp));
+  SolveArgs &a = sp.a;
   a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;
   a.tol = o.tol > 0 ? o.tol : 1e-6;
@@ -710,7 +928,7 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
   a.adjoint = 0;
   cudaStream_t s = g->stream;
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
-  MG_TRY(solve_run(g, a, weighted, o.use_graph, SLOT_PR));
+  MG_TRY(solve_run(g, sp, o.use_graph, SLOT_PR));
   MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
   MG_TRY(fetch_ctl(g));
   const DevCtl &hc = *g->ctl_host;
@@ -729,8 +947,10 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
-    // fill + row sums (1 or 2) + init + init reduce + per iteration gather, fix-up (+ loop guard)
-    stats->launches = (weighted ? 5 : 4) + (o.use_graph >= 0 ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
+    // fill + row sums + init + init reduce, then per iteration the gather (merge-path:
+    // gather + fix-up), plus the loop guard when the loop runs as a graph
+    const int64_t per_it = o.gather_kernel == 1 ? 2 : 1;
+    stats->launches = 4 + (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
   }
   return MG_OK;
 }

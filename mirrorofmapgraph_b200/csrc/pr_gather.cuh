@@ -8,11 +8,14 @@
 //
 // Each CTA is persistent and double-buffered: while it reduces tile k out of one
 // shared-memory stage, thread 0 has already issued the TMA bulk copies
-// (cp.async.bulk global->shared, completion counted on an mbarrier) of tile k+1's
-// row offsets, edge indices and edge weights into the other stage. The ranges are
-// widened to 16-byte boundaries (the graph arrays are padded for that), so the
-// copies are legal for any tile. Every mbarrier wait is bounded; a wait that runs
-// out sets MG_ERR_TIMEOUT and the CTA leaves.
+// (cp.async.bulk global->shared, completion counted on an mbarrier) of tile k+1
+// into the other stage: the tile's row offsets, edge indices, edge weights, and
+// up to NR per-row arrays the row update reads (previous iterate, row sums,
+// teleport, ...). The ranges are widened to 16-byte boundaries (every array is
+// padded for that), so the copies are legal for any tile, and no thread ever
+// waits on a dependent global load in the row epilogue. Every mbarrier wait is
+// bounded; a wait that runs out makes the CTA leave with a failure the caller
+// reports as MG_ERR_TIMEOUT.
 //
 // Per-row sums are finished in three deterministic steps:
 //   - inside a thread, rows that start and end in the thread are complete;
@@ -35,6 +38,7 @@ constexpr int PRG_NT = 256;
 constexpr int PRG_IPT = 8;
 constexpr int PRG_IPC = PRG_NT * PRG_IPT;
 constexpr int PRG_STAGE = PRG_IPC + 8;  // widened to 16-byte boundaries on both sides
+constexpr int PRG_MAXR = 4;             // per-row arrays a stage can carry
 constexpr uint32_t PRG_WAIT_LIMIT = 1u << 24;
 
 struct Comp {
@@ -125,25 +129,36 @@ __global__ void prg_plan_kernel(const int32_t *__restrict__ off, int64_t n, int6
 }
 
 // One shared-memory stage: widened copies of the tile's offsets (raw[k] =
-// off[xa + k]), edge indices (idx[k] = idx[ya + k]) and weights.
-template <bool WEIGHTED>
+// off[xa + k]), edge indices (idx[k] = idx[ya + k]), weights, and per-row arrays
+// (rows[j][k] = rowsrc[j][xa + k]); coord = x0, y0, x1, y1, xa.
+template <bool WEIGHTED, int NR>
 struct PrgStage {
   int32_t raw[PRG_STAGE];
   int32_t idx[PRG_STAGE];
   float w[WEIGHTED ? PRG_STAGE : 4];
+  float rows[NR > 0 ? NR : 1][PRG_STAGE];
+  int32_t coord[8];
 };
 
-template <bool WEIGHTED>
+template <bool WEIGHTED, int NR>
 struct PrgSmem {
-  PrgStage<WEIGHTED> st[2];
+  PrgStage<WEIGHTED, NR> st[2];
   uint64_t bar[2];
   int32_t crow[PRG_NT];
   float chi[PRG_NT];
   float clo[PRG_NT];
-  int32_t abort;
+  float rhi[PRG_IPC];  // per-row sums of the current tile
+  float rlo[PRG_IPC];
+  int32_t wfirst[PRG_NT / 32];
 };
 
-// The adjacency a gather runs over, with its plan and the carry arrays.
+template <bool WEIGHTED, int NR>
+constexpr size_t prg_smem_bytes() {
+  return sizeof(PrgSmem<WEIGHTED, NR>);
+}
+
+// The adjacency a gather runs over, with its plan, carry arrays and the per-row
+// arrays to stage (each padded to n + 8 entries, 16-byte aligned).
 struct PrgGraph {
   const int32_t *off, *idx;
   const float *wts;
@@ -152,33 +167,48 @@ struct PrgGraph {
   int64_t n;
   int32_t *carry_row, *head_row;
   Comp *carry_val, *head_val;
+  const float *rowsrc[PRG_MAXR];
 };
 
-// Issues the bulk copies of tile t into stage s (thread 0 only).
-template <bool WEIGHTED>
-__device__ __forceinline__ void prg_issue(PrgSmem<WEIGHTED> &sm, int s, const PrgGraph &g, int32_t t) {
-  const int64_t x0 = g.tx[t], y0 = g.ty[t], x1 = g.tx[t + 1], y1 = g.ty[t + 1];
-  const int64_t ya = y0 & ~(int64_t)3, yb = (y1 + 3) & ~(int64_t)3;
-  const int64_t xa = x0 & ~(int64_t)3, xb = (x1 + 2 + 3) & ~(int64_t)3;
-  const uint32_t bi = (uint32_t)((yb - ya) * 4), br = (uint32_t)((xb - xa) * 4);
+// Issues the bulk copies of the tile with coordinates c = (x0, y0, x1, y1) into
+// stage s (thread 0 only).
+template <bool WEIGHTED, int NR>
+__device__ __forceinline__ void prg_issue(PrgSmem<WEIGHTED, NR> &sm, int s, const PrgGraph &g, const int4 c) {
+  PrgStage<WEIGHTED, NR> &st = sm.st[s];
+  const int32_t x0 = c.x, y0 = c.y, x1 = c.z, y1 = c.w;
+  const int32_t ya = y0 & ~3, yb = (y1 + 3) & ~3;
+  const int32_t xa = x0 & ~3, xb = (x1 + 2 + 3) & ~3;
+  const uint32_t bi = (uint32_t)(yb - ya) * 4u, br = (uint32_t)(xb - xa) * 4u;
+  st.coord[0] = x0;
+  st.coord[1] = y0;
+  st.coord[2] = x1;
+  st.coord[3] = y1;
+  st.coord[4] = xa;
   fence_proxy_async();
-  mbar_arrive_expect_tx(&sm.bar[s], br + (WEIGHTED ? 2 : 1) * bi);
-  bulk_g2s(sm.st[s].raw, g.off + xa, br, &sm.bar[s]);
+  mbar_arrive_expect_tx(&sm.bar[s], br * (1 + NR) + (WEIGHTED ? 2u : 1u) * bi);
+  bulk_g2s(st.raw, g.off + xa, br, &sm.bar[s]);
+#pragma unroll
+  for (int j = 0; j < NR; j++) bulk_g2s(st.rows[j], g.rowsrc[j] + xa, br, &sm.bar[s]);
   if (bi) {
-    bulk_g2s(sm.st[s].idx, g.idx + ya, bi, &sm.bar[s]);
-    if (WEIGHTED) bulk_g2s(sm.st[s].w, g.wts + ya, bi, &sm.bar[s]);
+    bulk_g2s(st.idx, g.idx + ya, bi, &sm.bar[s]);
+    if (WEIGHTED) bulk_g2s(st.w, g.wts + ya, bi, &sm.bar[s]);
   }
 }
 
+__device__ __forceinline__ int4 prg_coords(const PrgGraph &g, int32_t t) {
+  return make_int4(g.tx[t], g.ty[t], g.tx[t + 1], g.ty[t + 1]);
+}
+
 // Reduces one staged tile. `gather(col)` returns the neighbour's value;
-// `finish(row, Comp)` consumes a completed row.
-template <bool WEIGHTED, typename Gather, typename Finish>
-__device__ __forceinline__ void prg_compute(PrgSmem<WEIGHTED> &sm, const PrgStage<WEIGHTED> &st, const PrgGraph &g,
-                                            int32_t t, Gather &gather, Finish &finish) {
+// `finish(row, Comp, stage)` consumes a completed row whose per-row inputs are in
+// the stage.
+template <bool WEIGHTED, int NR, typename Gather, typename Finish>
+__device__ __forceinline__ void prg_compute(PrgSmem<WEIGHTED, NR> &sm, const PrgStage<WEIGHTED, NR> &st,
+                                            const PrgGraph &g, int32_t t, Gather &gather, Finish &finish) {
   const int tid = threadIdx.x;
-  const int32_t x0 = g.tx[t], y0 = g.ty[t], x1 = g.tx[t + 1], y1 = g.ty[t + 1];
+  const int32_t x0 = st.coord[0], y0 = st.coord[1], x1 = st.coord[2], y1 = st.coord[3];
   const int nrows = x1 - x0, nedges = y1 - y0;
-  const int32_t *rend = st.raw + (x0 & 3) + 1;  // rend[i] = off[x0 + i + 1]; rend[nrows] is INT_MAX past n
+  const int32_t *rend = st.raw + (x0 & 3) + 1;  // rend[i] = off[x0 + i + 1]; past n the pad is INT_MAX
   const int32_t beg0 = st.raw[x0 & 3];          // off[x0]
   const int32_t *sidx = st.idx + (y0 & 3);
   const float *sw = st.w + (y0 & 3);
@@ -220,7 +250,8 @@ __device__ __forceinline__ void prg_compute(PrgSmem<WEIGHTED> &sm, const PrgStag
       }
     }
   }
-  // Pass 2: segmented accumulation.
+  // Pass 2: segmented accumulation. Completed rows only record their sums in
+  // shared memory; the row update runs afterwards, one row per thread.
   Comp acc{0.f, 0.f};
   bool has_first = false;
   int f_row = 0;
@@ -236,50 +267,103 @@ __device__ __forceinline__ void prg_compute(PrgSmem<WEIGHTED> &sm, const PrgStag
         f_row = lx;
         f_val = acc;
       } else {
-        finish(x0 + lx, acc);
+        sm.rhi[lx] = acc.hi;
+        sm.rlo[lx] = acc.lo;
       }
       acc.hi = 0.f;
       acc.lo = 0.f;
       lx++;
     }
   }
-  sm.crow[tid] = lx;
-  sm.chi[tid] = acc.hi;
-  sm.clo[tid] = acc.lo;
+  // Segmented inclusive scan of the threads' trailing partials keyed by their
+  // trailing row (non-decreasing in tid, so equal keys are contiguous): lane
+  // shuffles inside each warp, then an 8-step pass across the warps.
+  const int lane = tid & 31, wid = tid >> 5;
+  Comp p = acc;
+  const int key = lx;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float uh = __shfl_up_sync(0xffffffffu, p.hi, o), ul = __shfl_up_sync(0xffffffffu, p.lo, o);
+    const int uk = __shfl_up_sync(0xffffffffu, key, o);
+    if (lane >= o && uk == key) {
+      Comp q{uh, ul};
+      comp_add(q, p);
+      p = q;
+    }
+  }
+  if (lane == 0) sm.wfirst[wid] = key;
+  if (lane == 31) {
+    sm.crow[wid] = key;
+    sm.chi[wid] = p.hi;
+    sm.clo[wid] = p.lo;
+  }
   __syncthreads();
+  if (tid == 0) {
+    // Warp totals become segment totals ending at each warp's last lane.
+    for (int w = 1; w < PRG_NT / 32; w++) {
+      if (sm.crow[w] == sm.crow[w - 1] && sm.wfirst[w] == sm.crow[w]) {
+        Comp q{sm.chi[w - 1], sm.clo[w - 1]};
+        comp_add(q, Comp{sm.chi[w], sm.clo[w]});
+        sm.chi[w] = q.hi;
+        sm.clo[w] = q.lo;
+      }
+    }
+  }
+  __syncthreads();
+  if (wid > 0 && sm.crow[wid - 1] == key && sm.wfirst[wid] == key) {
+    Comp q{sm.chi[wid - 1], sm.clo[wid - 1]};
+    comp_add(q, p);
+    p = q;
+  }
+  // p = sum of the run of trailing partials ending at this thread.
+  const Comp carry_in = Comp{__shfl_up_sync(0xffffffffu, p.hi, 1), __shfl_up_sync(0xffffffffu, p.lo, 1)};
+  const int key_prev = __shfl_up_sync(0xffffffffu, key, 1);
+  __syncthreads();
+  sm.crow[tid] = key;
+  sm.chi[tid] = p.hi;
+  sm.clo[tid] = p.lo;
+  __syncthreads();
+  // A row begun in an earlier tile is finished by the fix-up kernel.
+  const bool defer0 = y0 > beg0;
   if (has_first) {
-    int t0 = tid;
-    while (t0 > 0 && sm.crow[t0 - 1] == f_row) t0--;
     Comp tot{0.f, 0.f};
-    for (int q = t0; q < tid; q++) comp_add(tot, Comp{sm.chi[q], sm.clo[q]});
+    if (tid > 0) {
+      const bool cont = lane > 0 ? key_prev == f_row : sm.crow[tid - 1] == f_row;
+      if (cont) tot = lane > 0 ? carry_in : Comp{sm.chi[tid - 1], sm.clo[tid - 1]};
+    }
     comp_add(tot, f_val);
-    if (f_row == 0 && y0 > beg0) {
+    if (f_row == 0 && defer0) {
       g.head_row[t] = x0;
       g.head_val[t] = tot;
     } else {
-      finish(x0 + f_row, tot);
+      sm.rhi[f_row] = tot.hi;
+      sm.rlo[f_row] = tot.lo;
     }
   }
   if (tid == PRG_NT - 1) {
-    const int r = sm.crow[PRG_NT - 1];
-    int t0 = PRG_NT - 1;
-    while (t0 > 0 && sm.crow[t0 - 1] == r) t0--;
-    Comp tot{0.f, 0.f};
-    for (int q = t0; q < PRG_NT; q++) comp_add(tot, Comp{sm.chi[q], sm.clo[q]});
-    g.carry_row[t] = x0 + r;
-    g.carry_val[t] = tot;
+    g.carry_row[t] = x0 + key;
+    g.carry_val[t] = p;
   }
+  __syncthreads();
+  // Row updates: consecutive threads on consecutive rows (coalesced stores, no
+  // divergence from the item walk).
+  for (int j = (defer0 ? 1 : 0) + tid; j < nrows; j += PRG_NT) finish(x0 + j, Comp{sm.rhi[j], sm.rlo[j]}, st);
 }
 
 // Persistent double-buffered loop over tiles blockIdx.x, +gridDim.x, ...
-// Returns false if a bounded wait ran out (the caller reports MG_ERR_TIMEOUT).
-template <bool WEIGHTED, typename Gather, typename Finish>
-__device__ __forceinline__ bool prg_run(PrgSmem<WEIGHTED> &sm, const PrgGraph &g, Gather &&gather, Finish &&finish) {
+// Returns false if a bounded wait ran out.
+template <bool WEIGHTED, int NR, typename Gather, typename Finish>
+__device__ __forceinline__ bool prg_run(PrgSmem<WEIGHTED, NR> &sm, const PrgGraph &g, Gather &&gather,
+                                        Finish &&finish) {
+  // Thread 0 keeps the coordinates of the next tile to issue in registers,
+  // loaded one iteration ahead so the issue never waits on a global load.
+  int4 cnext = make_int4(0, 0, 0, 0);
   if (threadIdx.x == 0) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
     fence_barrier_init();
-    if ((int32_t)blockIdx.x < g.ntiles) prg_issue<WEIGHTED>(sm, 0, g, blockIdx.x);
+    if ((int32_t)blockIdx.x < g.ntiles) prg_issue<WEIGHTED, NR>(sm, 0, g, prg_coords(g, blockIdx.x));
+    if ((int32_t)(blockIdx.x + gridDim.x) < g.ntiles) cnext = prg_coords(g, blockIdx.x + gridDim.x);
   }
   __syncthreads();
   uint32_t phase[2] = {0u, 0u};
@@ -287,7 +371,10 @@ __device__ __forceinline__ bool prg_run(PrgSmem<WEIGHTED> &sm, const PrgGraph &g
   for (int32_t t = blockIdx.x; t < g.ntiles; t += gridDim.x, k++) {
     const int s = k & 1;
     const int32_t tn = t + gridDim.x;
-    if (threadIdx.x == 0 && tn < g.ntiles) prg_issue<WEIGHTED>(sm, s ^ 1, g, tn);
+    if (threadIdx.x == 0 && tn < g.ntiles) {
+      prg_issue<WEIGHTED, NR>(sm, s ^ 1, g, cnext);
+      if (tn + (int32_t)gridDim.x < g.ntiles) cnext = prg_coords(g, tn + gridDim.x);
+    }
     const bool ok = mbar_wait_bounded(&sm.bar[s], phase[s]);
     if (__syncthreads_or(!ok)) {
       // Give the copy in flight for the next tile a bounded chance to land.
@@ -295,7 +382,7 @@ __device__ __forceinline__ bool prg_run(PrgSmem<WEIGHTED> &sm, const PrgGraph &g
       return false;
     }
     phase[s] ^= 1u;
-    prg_compute<WEIGHTED>(sm, sm.st[s], g, t, gather, finish);
+    prg_compute<WEIGHTED, NR>(sm, sm.st[s], g, t, gather, finish);
     __syncthreads();
   }
   return true;
@@ -316,11 +403,6 @@ __device__ __forceinline__ void prg_fixup_tile(int32_t t, const int32_t *__restr
   comp_add(tot, head_val[t]);
   head_row[t] = -1;
   finish(r, tot);
-}
-
-template <bool WEIGHTED>
-constexpr size_t prg_smem_bytes() {
-  return sizeof(PrgSmem<WEIGHTED>);
 }
 
 }  // namespace mg

@@ -245,8 +245,9 @@ class Graph:
 
     @staticmethod
     def _pr_opts(mode="refcompat", directed=1, max_iter=0, weighted=False, alpha=0.85, tol=None,
-                 compensated=True, device_output=False, use_graph=True) -> L.MgPrOpts:
+                 compensated=True, device_output=False, use_graph=True, gather="binned") -> L.MgPrOpts:
         o = L.MgPrOpts()
+        o.gather_kernel = {"binned": 0, "tma": 1}[gather]
         o.mode = {"refcompat": L.MG_PR_REFCOMPAT, "normalized": L.MG_PR_NORMALIZED}[mode]
         o.directed = int(directed)
         o.max_iter = int(max_iter)

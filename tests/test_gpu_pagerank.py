@@ -151,3 +151,32 @@ def test_api_pagerank_program(mtx_fixtures):
     x = csr_problem.ExtractResults()
     ref = np.array(d["cpupr"])
     assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < cfg.getParameter("tol")
+
+
+@pytest.mark.parametrize("gather", ["binned", "tma"])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_gather_kernels_agree_with_fp64(gather, weighted):
+    h = mg.gen_rmat(14, 16, 61, symmetrize=False, weights="lognormal" if weighted else None, p0=0, p1=1)
+    w = h.weights_f32 if weighted else None
+    with mg.Graph(h.row_offsets, h.col_idx, w) as g:
+        x, st = g.pagerank(mode="normalized", weighted=weighted, gather=gather)
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, w, 0.85, 0.0, st["iterations"])
+        assert np.abs(x - xr).sum() <= L1_TOL
+        x2, _ = g.pagerank(mode="normalized", weighted=weighted, gather=gather)
+        assert (x == x2).all()
+
+
+def test_gather_hub_chunks_binned():
+    # one hub of 50k in-edges spans many chunks; leaves of degree 1
+    n = 50001
+    src = np.concatenate([np.arange(1, n), np.zeros(n - 1, dtype=np.int64)])
+    dst = np.concatenate([np.zeros(n - 1, dtype=np.int64), np.arange(1, n)])
+    order = np.lexsort((dst, src))
+    ro = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(ro, src[order] + 1, 1)
+    h = mg.HostCsr(np.cumsum(ro).astype(np.int32), dst[order].astype(np.int32))
+    for gather in ("binned", "tma"):
+        with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+            x, st = g.pagerank(mode="normalized", gather=gather)
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+        assert np.abs(x - xr).sum() <= L1_TOL
