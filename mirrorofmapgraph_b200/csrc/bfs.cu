@@ -52,6 +52,7 @@ struct BfsArgs {
   int32_t both;      // directed == 0 on a non-symmetric graph: expand CSR and CSC
   int64_t n;
   int64_t m_total;
+  int32_t *big_v;  // grid-strided bin of the push direction (BIG_CAP entries)
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
@@ -70,6 +71,7 @@ __device__ void bfs_level_end(const BfsArgs &a) {
   c->cur = cur ^ 1;
   c->mf_next = 0;
   c->blocks_done = 0;
+  c->big_len = 0;
   const bool over = vload(&c->overflow) != 0;
   const bool done = nf == 0 || lvl >= c->iter_cap || over;
   int dir = vload(&c->dir);
@@ -143,12 +145,13 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
   const int32_t *qin = cur ? a.q1 : a.q0;
   PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
   int64_t insp = 0, nexp = 0;
+  const BigList big{a.big_v, &c->big_len};
   for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
     nexp += v >= 0;
     const int32_t *ci = a.ci, *ri = a.ri;
-    expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+    expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big);
     if (a.both)
       expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
   }
@@ -160,6 +163,21 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
     if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
     if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
   }
+}
+
+// Grid-strided bin of a push level: the deferred hubs' edges spread over every
+// CTA; the last CTA closes the level.
+__global__ void __launch_bounds__(BFS_NT) bfs_push_big_kernel(BfsArgs a) {
+  __shared__ BigSmem<BFS_NT> sm;
+  __shared__ int64_t s_sum[BFS_NT / 32 + 1];
+  if (bfs_skip(a, 0)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
+  const int32_t *ci = a.ci;
+  expand_big<BFS_NT>(sm, a.ro, BigList{a.big_v, &c->big_len}, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+  const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
+  if (threadIdx.x == 0 && bmf) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)bmf);
   if (last_block(&c->blocks_done) && threadIdx.x == 0) bfs_level_end(a);
 }
 
@@ -308,7 +326,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   const int64_t nwords = (n + 31) / 32;
   const size_t need = Carve::need({sizeof(int32_t) * (size_t)n, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
-                                   sizeof(int32_t) * (size_t)nsrc});
+                                   sizeof(int32_t) * (size_t)nsrc, sizeof(int32_t) * (size_t)BIG_CAP});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   int32_t *label_ws = cv.take<int32_t>(n);
@@ -316,6 +334,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   int32_t *q0 = cv.take<int32_t>(qcap);
   int32_t *q1 = cv.take<int32_t>(qcap);
   int32_t *dsrc = cv.take<int32_t>(nsrc);
+  int32_t *big_v = cv.take<int32_t>(BIG_CAP);
   int32_t *label = o.device_output ? depth : label_ws;
   cudaStream_t s = g->stream;
 
@@ -334,6 +353,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   a.both = undirected ? 1 : 0;
   a.n = n;
   a.m_total = g->m;
+  a.big_v = big_v;
   a.ctl = g->ctl;
   a.h = 0;
   a.use_cond = 0;
@@ -360,6 +380,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     b.h = h;
     b.use_cond = use_cond;
     bfs_push_kernel<<<grid, BFS_NT, 0, st>>>(b);
+    bfs_push_big_kernel<<<grid, BFS_NT, 0, st>>>(b);
     bfs_pull_kernel<<<grid, BFS_NT, 0, st>>>(b);
   };
   MG_TRY(run_loop(g, SLOT_BFS, &sig, sizeof(sig), use_graph, body, n + 2));
@@ -378,7 +399,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
     stats->status_detail = hc.levels_pull;
-    stats->launches = 2 + (use_graph ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
+    stats->launches = 2 + (use_graph ? 4 * (int64_t)hc.body_iters : 3 * (int64_t)hc.level);
   }
   if (hc.status != 0) {
     mg_set_error("mg_bfs: frontier exceeded queue capacity %d", qcap);

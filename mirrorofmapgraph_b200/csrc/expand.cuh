@@ -27,9 +27,12 @@ struct ExpandSmem {
   int32_t cta[4];
 };
 
+struct BigList;
+__device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t deg);
+
 template <int NT, int CTA_TH, typename Visit>
 __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *__restrict__ off, int32_t v,
-                                            int64_t &insp, Visit &&visit) {
+                                            int64_t &insp, Visit &&visit, const BigList *big = nullptr) {
   const int tid = threadIdx.x, lane = lane_id();
   int32_t beg = 0, deg = 0;
   if (v >= 0) {
@@ -37,6 +40,8 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
     deg = off[v + 1] - beg;
     insp += deg;
   }
+  // Vertices for the grid-strided bin are expanded by a later kernel.
+  if (big && defer_big(*big, v, deg)) deg = 0;
   // CTA bin.
   while (__syncthreads_or(deg >= CTA_TH)) {
     if (deg >= CTA_TH) sm.cta[0] = tid;
@@ -83,6 +88,74 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
 template <typename T>
 __device__ __forceinline__ T vload(const T *p) {
   return *(const volatile T *)p;
+}
+
+// ---- grid-strided bin ------------------------------------------------------
+// Vertices with at least GRID_TH edges are too big for one CTA: the tile pass
+// defers them to a list, and a second kernel spreads their concatenated edges
+// evenly over every CTA of the grid.
+constexpr int GRID_TH = 4096;
+constexpr int BIG_CAP = 4096;  // deferred vertices per level (more fall back to the CTA bin)
+
+struct BigList {
+  int32_t *v;    // deferred vertices
+  int32_t *len;  // their count (reset at the end of every level)
+};
+
+// Returns true (and records v) when v goes to the grid bin.
+__device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t deg) {
+  if (v < 0 || deg < GRID_TH) return false;
+  const int32_t pos = atomicAdd(big.len, 1);
+  if (pos >= BIG_CAP) return false;
+  big.v[pos] = v;
+  return true;
+}
+
+template <int NT>
+struct BigSmem {
+  int32_t v[BIG_CAP];
+  int32_t pre[BIG_CAP + 1];
+  int32_t red[NT / 32 + 1];
+};
+
+// Every CTA takes an equal slice of the concatenated edges of the deferred
+// vertices; an edge slot finds its vertex by binary search over their prefix sums.
+template <int NT, typename Visit>
+__device__ __forceinline__ void expand_big(BigSmem<NT> &sm, const int32_t *__restrict__ off, const BigList &big,
+                                           Visit &&visit) {
+  const int32_t nb = min(*(const volatile int32_t *)big.len, BIG_CAP);
+  if (nb == 0) return;
+  // Degrees and their exclusive prefix, NT * ceil(nb / NT) at a time.
+  int32_t carry = 0;
+  for (int32_t b0 = 0; b0 < nb; b0 += NT) {
+    const int32_t i = b0 + threadIdx.x;
+    int32_t d = 0;
+    if (i < nb) {
+      const int32_t v = big.v[i];
+      sm.v[i] = v;
+      d = off[v + 1] - off[v];
+    }
+    int32_t tot;
+    const int32_t ex = block_exclusive_scan<NT>(d, sm.red, &tot);
+    if (i < nb) sm.pre[i] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sm.pre[nb] = carry;
+  __syncthreads();
+  const int64_t total = carry;
+  const int64_t lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
+  for (int64_t k = lo + threadIdx.x; k < hi; k += NT) {
+    int a = 0, b = nb;
+    while (b - a > 1) {
+      const int mid = (a + b) >> 1;
+      if (sm.pre[mid] <= k) a = mid;
+      else b = mid;
+    }
+    const int32_t v = sm.v[a];
+    visit(v, off[v] + (int32_t)(k - sm.pre[a]));
+  }
+  __syncthreads();
 }
 
 }  // namespace mg

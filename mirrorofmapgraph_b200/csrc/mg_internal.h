@@ -53,7 +53,7 @@ struct DevCtl {
   int32_t levels_pull;       // levels run bottom-up
   int32_t overflow;          // set by a kernel whose frontier append ran past capacity
   int32_t body_iters;        // WHILE-body executions so far (loop guard)
-  int32_t pad;
+  int32_t big_len;           // vertices deferred to the grid-strided bin this level
 };
 
 // Padding of the device graph arrays. Offsets arrays hold n + 1 + MG_OFF_PAD

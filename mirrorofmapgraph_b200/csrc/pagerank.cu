@@ -95,31 +95,30 @@ static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
     const int32_t *off = csr ? g->ro : g->co;
     const int64_t n = g->n;
     cudaStream_t s = g->stream;
-    unsigned long long *dcnt = nullptr, *dcur = nullptr;
-    int64_t *dboff = nullptr;
-    MG_CUDA_TRY(cudaMalloc((void **)&dcnt, sizeof(unsigned long long) * 2 * (PRB_BINS + 1) + sizeof(int64_t) * (PRB_BINS + 1)));
-    dcur = dcnt + (PRB_BINS + 1);
-    dboff = reinterpret_cast<int64_t *>(dcur + (PRB_BINS + 1));
-    MG_CUDA_TRY(cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 2 * (PRB_BINS + 1), s));
-    prb_count_kernel<<<g->num_sms * 4, 256, 0, s>>>(off, n, dcnt);
-    unsigned long long cnt[PRB_BINS + 1];
-    MG_CUDA_TRY(cudaMemcpyAsync(cnt, dcnt, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    const int64_t nchunks = std::max<int64_t>(1, (n + PRB_CHUNK_ROWS - 1) / PRB_CHUNK_ROWS);
+    int64_t *counts = nullptr;
+    MG_CUDA_TRY(cudaMallocAsync((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
+    int64_t *totals = counts + nchunks * (PRB_BINS + 1);
+    int64_t *dboff = totals + (PRB_BINS + 1);
+    prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts);
+    prb_offsets_kernel<<<1, 32, 0, s>>>(counts, nchunks, totals);
+    int64_t cnt[PRB_BINS + 1];
+    MG_CUDA_TRY(cudaMemcpyAsync(cnt, totals, sizeof(cnt), cudaMemcpyDeviceToHost, s));
     MG_CUDA_TRY(cudaStreamSynchronize(s));
     int64_t acc = 0;
     for (int b = 0; b < PRB_BINS; b++) {
       bp.boff[b] = acc;
-      if (b < 6) acc += (int64_t)cnt[b];
+      if (b < 6) acc += cnt[b];
     }
     bp.boff[PRB_BINS] = acc;
     bp.boff[6] = acc;
-    bp.nheavy = (int64_t)cnt[6];
-    bp.ntasks = (int64_t)cnt[PRB_BINS];
-    const int groups[6] = {1, 2, 4, 8, 16, 32};
+    bp.nheavy = cnt[6];
+    bp.ntasks = cnt[PRB_BINS];
+    // One warp assignment per 32 rows of bins 0..5, one per hub chunk.
     int64_t w = 0;
     for (int b = 0; b < PRB_BINS; b++) {
       bp.wstart[b] = w;
-      if (b < 5) w += ((int64_t)cnt[b] * groups[b] + 31) / 32;
-      else if (b == 5) w += (int64_t)cnt[5];
+      if (b < 6) w += (cnt[b] + 31) / 32;
       else w += bp.ntasks;
     }
     bp.wstart[PRB_BINS] = w;
@@ -131,11 +130,10 @@ static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
     MG_CUDA_TRY(cudaMalloc((void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
     MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
     MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
-    prb_scatter_kernel<<<g->num_sms * 4, 256, 0, s>>>(off, n, dboff, dcur, bp.rows, bp.hrows);
-    prb_hubs_kernel<<<1, 32, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
+    prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows);
+    prb_hubs_kernel<<<1, PRB_NT, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
     MG_CUDA_TRY(cudaGetLastError());
-    MG_CUDA_TRY(cudaStreamSynchronize(s));
-    cudaFree(dcnt);
+    MG_CUDA_TRY(cudaFreeAsync(counts, s));
     ok = true;
   }
   *out = &bp;
@@ -322,7 +320,8 @@ __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *h
     c->dprev[1] = d;
     c->cur = cur ^ 1;
     c->blocks_done = 0;
-    const bool done = r < a.tol || lvl >= a.max_iter || c->status != 0;
+    const double thr = a.adjoint ? a.tol * c->dprev[2] : a.tol;  // adjoint: relative to ||w||_1
+    const bool done = r < thr || lvl >= a.max_iter || c->status != 0;
     __threadfence();
     c->done = done ? 1 : 0;
     if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
@@ -331,7 +330,7 @@ __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *h
 
 // One whole iteration of the degree-binned solver.
 template <bool WEIGHTED>
-__global__ void __launch_bounds__(PRB_NT) solve_binned_kernel(SolveArgs a, PrbArgs p) {
+__global__ void __launch_bounds__(PRB_NT, 5) solve_binned_kernel(SolveArgs a, PrbArgs p) {
   __shared__ double s_red[PRB_NT / 32 + 1];
   if (solve_skip(a)) return;
   DevCtl *c = a.ctl;
@@ -393,7 +392,7 @@ __global__ void __launch_bounds__(PRG_NT) solve_fixup_kernel(SolveArgs a) {
 // Adjoint: lambda0 = w; partial sums of t . w.
 __global__ void __launch_bounds__(256) solve_init_kernel(SolveArgs a) {
   __shared__ double s_red[256 / 32 + 1];
-  double acc = 0.0;
+  double acc = 0.0, wabs = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
     const double t = tele_of(a, i);
     if (!a.adjoint) {
@@ -407,20 +406,30 @@ __global__ void __launch_bounds__(256) solve_init_kernel(SolveArgs a) {
     } else {
       a.v0[i] = a.wvec[i];
       acc += t * (double)a.wvec[i];
+      wabs += fabs((double)a.wvec[i]);
     }
   }
   acc = block_sum<256>(acc, s_red);
-  if (threadIdx.x == 0) a.part1[2 * blockIdx.x + 1] = acc;
+  wabs = block_sum<256>(wabs, s_red);
+  if (threadIdx.x == 0) {
+    a.part1[2 * blockIdx.x] = wabs;
+    a.part1[2 * blockIdx.x + 1] = acc;
+  }
 }
 
 __global__ void __launch_bounds__(256) solve_init_reduce_kernel(SolveArgs a, int32_t ginit) {
   __shared__ double s_red[256 / 32 + 1];
-  double d = 0.0;
-  for (int i = threadIdx.x; i < ginit; i += 256) d += a.part1[2 * i + 1];
+  double d = 0.0, wabs = 0.0;
+  for (int i = threadIdx.x; i < ginit; i += 256) {
+    wabs += a.part1[2 * i];
+    d += a.part1[2 * i + 1];
+  }
   d = block_sum<256>(d, s_red);
+  wabs = block_sum<256>(wabs, s_red);
   if (threadIdx.x == 0) {
     DevCtl *c = a.ctl;
     c->dprev[1] = d;
+    c->dprev[2] = wabs;  // adjoint: ||w||_1, the scale of the relative stopping rule
     c->level = 0;
     c->cur = 0;
     c->iter_cap = a.max_iter;
@@ -1007,5 +1016,187 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
     total.residual = std::max(total.residual, st.residual);
   }
   if (stats) *stats = total;
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint (mg_pagerank_backward).
+namespace mg {
+
+// Per-row products of the converged adjoint: pl[u] = sum_k a_uk lambda_k / s_u and
+// coef[u] = alpha * x_u / s_u (both 0 for dangling rows), in FP64.
+struct AdjRowStore {
+  const float *srow, *x;
+  double *pl, *coef;
+  double alpha;
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) {
+    const double s = (double)srow[r];
+    if (s > 0.0) {
+      pl[r] = ((double)v.hi + (double)v.lo) / s;
+      coef[r] = alpha * (double)x[r] / s;
+    } else {
+      pl[r] = 0.0;
+      coef[r] = 0.0;
+    }
+  }
+};
+
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(PRB_NT) adj_rows_kernel(PrbArgs p, const float *lam, AdjRowStore st) {
+  prb_run<WEIGHTED>(p, [&](int32_t c) { return __ldg(lam + c); }, st,
+                    [&](int64_t, int32_t row, Comp v) { st(row, v); });
+}
+
+// dL/da_uv = coef[u] * (lambda_v - pl[u]) for every CSR edge, rows expanded with
+// the degree-binned tile expansion (coalesced index loads and gradient stores).
+__global__ void __launch_bounds__(256) adj_edge_grad_kernel(const int32_t *__restrict__ ro,
+                                                            const int32_t *__restrict__ ci, int64_t n,
+                                                            const float *__restrict__ lam,
+                                                            const double *__restrict__ pl,
+                                                            const double *__restrict__ coef, float *__restrict__ grad) {
+  __shared__ ExpandSmem<256> sm;
+  int64_t insp = 0;
+  for (int64_t tile = (int64_t)blockIdx.x * 256; tile < n; tile += (int64_t)gridDim.x * 256) {
+    const int64_t i = tile + threadIdx.x;
+    const int32_t v = i < n ? (int32_t)i : -1;
+    expand_tile<256, 1024>(sm, ro, v, insp, [&](int32_t u, int32_t k) {
+      grad[k] = (float)(coef[u] * ((double)__ldg(lam + ci[k]) - pl[u]));
+    });
+  }
+}
+
+// Dangling rank mass of x: per-block partials, then one block.
+__global__ void __launch_bounds__(256) adj_dangling_kernel(const float *x, const float *srow, int64_t n,
+                                                           double *part) {
+  __shared__ double s_red[256 / 32 + 1];
+  double d = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (srow[i] == 0.f) d += (double)x[i];
+  d = block_sum<256>(d, s_red);
+  if (threadIdx.x == 0) part[blockIdx.x] = d;
+}
+
+// dL/dt_i = lambda_i * (1 - alpha + alpha * d).
+__global__ void __launch_bounds__(256) adj_tele_grad_kernel(const float *lam, const double *part, int nparts,
+                                                            int64_t n, double alpha, float *gt) {
+  __shared__ double s_d;
+  if (threadIdx.x == 0) {
+    double d = 0.0;
+    for (int i = 0; i < nparts; i++) d += part[i];
+    s_d = d;
+  }
+  __syncthreads();
+  const double f = 1.0 - alpha + alpha * s_d;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    gt[i] = (float)((double)lam[i] * f);
+}
+
+}  // namespace mg
+
+extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *ranks,
+                                          const float *dL_dranks, float *dL_dweights, float *dL_dteleport,
+                                          const mg_pr_opts *opts, mg_stats *stats) {
+  using namespace mg;
+  if (!g || !ranks || !dL_dranks) {
+    mg_set_error("mg_pagerank_backward: null argument");
+    return MG_ERR_ARG;
+  }
+  mg_pr_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.mode = MG_PR_NORMALIZED;
+  if (opts) o = *opts;
+  if (o.mode != MG_PR_NORMALIZED) {
+    mg_set_error("mg_pagerank_backward: only the NORMALIZED fixed point has an adjoint");
+    return MG_ERR_ARG;
+  }
+  if (o.alpha < 0 || o.alpha >= 1) {
+    mg_set_error("mg_pagerank_backward: alpha must be in [0, 1)");
+    return MG_ERR_ARG;
+  }
+  const bool weighted = o.weighted != 0;
+  if (weighted && g->vtype != MG_DTYPE_F32) {
+    mg_set_error("mg_pagerank_backward: weighted mode needs float edge values");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  const int64_t n = g->n, m = g->m;
+  cudaStream_t s = g->stream;
+  // Inputs staged on the device.
+  const float *x_dev = ranks, *w_dev = dL_dranks, *t_dev = teleport;
+  if (!o.device_output) {
+    MG_TRY(ws_reserve(g->ws_out, Carve::need({4 * (size_t)n, 4 * (size_t)n, 4 * (size_t)n})));
+    Carve cv(g->ws_out.ptr);
+    float *xs = cv.take<float>(n), *ws = cv.take<float>(n), *ts = cv.take<float>(n);
+    MG_CUDA_TRY(cudaMemcpyAsync(xs, ranks, 4 * n, cudaMemcpyHostToDevice, s));
+    MG_CUDA_TRY(cudaMemcpyAsync(ws, dL_dranks, 4 * n, cudaMemcpyHostToDevice, s));
+    if (teleport) MG_CUDA_TRY(cudaMemcpyAsync(ts, teleport, 4 * n, cudaMemcpyHostToDevice, s));
+    x_dev = xs;
+    w_dev = ws;
+    t_dev = teleport ? ts : nullptr;
+  }
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  SolvePlan sp;
+  MG_TRY(solve_setup(g, true, weighted, t_dev, w_dev, o.gather_kernel == 1, sp));
+  SolveArgs &a = sp.a;
+  a.tn = n > 0 ? 1.0 / (double)n : 0.0;
+  a.alpha = o.alpha > 0 ? o.alpha : 0.85;
+  a.tol = o.tol > 0 ? o.tol : 1e-7;
+  a.max_iter = o.max_iter > 0 ? o.max_iter : 200;
+  a.adjoint = 1;
+  MG_TRY(solve_run(g, sp, o.use_graph, SLOT_ADJ));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl hc = *g->ctl_host;
+  const float *lam = hc.cur ? a.v1 : a.v0;
+  // Per-row products and gradients (scratch in ws_aux).
+  const int nparts = g->num_sms * 4;
+  MG_TRY(ws_reserve(g->ws_aux, Carve::need({8 * (size_t)n, 8 * (size_t)n, 8 * (size_t)nparts, 4 * (size_t)m,
+                                            4 * (size_t)n})));
+  Carve cv(g->ws_aux.ptr);
+  double *pl = cv.take<double>(n), *coef = cv.take<double>(n), *part = cv.take<double>(nparts);
+  float *gw_ws = cv.take<float>(m), *gt_ws = cv.take<float>(n);
+  float *gw = o.device_output ? dL_dweights : gw_ws;
+  float *gt = o.device_output ? dL_dteleport : gt_ws;
+  int64_t launches = 0;
+  if (dL_dweights) {
+    BinPlan *rb = nullptr;
+    MG_TRY(get_bin_plan(g, true, &rb));
+    const PrbArgs rp = prb_args_of(g, *rb, true, weighted ? (const float *)g->vals : nullptr);
+    AdjRowStore st{a.srow, x_dev, pl, coef, a.alpha};
+    if (weighted) adj_rows_kernel<true><<<g->num_sms * 8, PRB_NT, 0, s>>>(rp, lam, st);
+    else adj_rows_kernel<false><<<g->num_sms * 8, PRB_NT, 0, s>>>(rp, lam, st);
+    adj_edge_grad_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, g->ci, n, lam, pl, coef, gw);
+    launches += 2;
+  }
+  if (dL_dteleport) {
+    adj_dangling_kernel<<<nparts, 256, 0, s>>>(x_dev, a.srow, n, part);
+    adj_tele_grad_kernel<<<g->num_sms * 8, 256, 0, s>>>(lam, part, nparts, n, a.alpha, gt);
+    launches += 2;
+  }
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  if (!o.device_output) {
+    if (dL_dweights) MG_CUDA_TRY(cudaMemcpyAsync(dL_dweights, gw, 4 * m, cudaMemcpyDeviceToHost, s));
+    if (dL_dteleport) MG_CUDA_TRY(cudaMemcpyAsync(dL_dteleport, gt, 4 * n, cudaMemcpyDeviceToHost, s));
+  }
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = m * (hc.level + (dL_dweights ? 2 : 0));
+    stats->edges_inspected = stats->edges_traversed;
+    stats->residual = hc.dsum[0];
+    // per solve iteration as the forward; the gradient pass reads col + weight,
+    // writes the gradient, and reads/writes per-row state
+    stats->bytes_compulsory = hc.level * (4 * (n + 1) + (weighted ? 8 : 4) * m + 12 * n) +
+                              (dL_dweights ? 12 * m + 24 * n : 0);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+    stats->launches = 4 + launches + (o.use_graph >= 0 ? 2 * (int64_t)hc.body_iters : (int64_t)hc.level);
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_pagerank_backward: device status %d", hc.status);
+    return (mg_status)hc.status;
+  }
   return MG_OK;
 }

@@ -52,50 +52,96 @@ __device__ __forceinline__ int prb_bin_of(int32_t deg) {
   return 6;
 }
 
-__global__ void prb_count_kernel(const int32_t *__restrict__ off, int64_t n, unsigned long long *cnt) {
-  __shared__ unsigned long long s[PRB_BINS + 1];
+// Ordered binning. Rows are cut into chunks of PRB_NT * PRB_RPT rows, one per
+// CTA; pass 1 counts every bin per chunk, a single CTA turns the counts into
+// output offsets (bin-major, chunk order), and pass 2 writes each chunk's rows in
+// row order with an in-CTA exclusive scan per bin. Bins therefore list rows in
+// ascending order and the plan is deterministic.
+constexpr int PRB_RPT = 8;
+constexpr int PRB_CHUNK_ROWS = PRB_NT * PRB_RPT;
+
+__global__ void __launch_bounds__(PRB_NT) prb_count_kernel(const int32_t *__restrict__ off, int64_t n,
+                                                           int64_t *__restrict__ counts /* [chunk][BINS+1] */) {
+  __shared__ int64_t s[PRB_BINS + 1];
   if (threadIdx.x <= PRB_BINS) s[threadIdx.x] = 0;
   __syncthreads();
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t d = off[r + 1] - off[r];
-    const int b = prb_bin_of(d);
-    atomicAdd(&s[b], 1ull);
-    if (b == 6) atomicAdd(&s[PRB_BINS], (unsigned long long)((d + PRB_CHUNK - 1) / PRB_CHUNK));
+  const int64_t base = (int64_t)blockIdx.x * PRB_CHUNK_ROWS;
+  for (int k = 0; k < PRB_RPT; k++) {
+    const int64_t r = base + (int64_t)threadIdx.x * PRB_RPT + k;
+    if (r < n) {
+      const int32_t d = off[r + 1] - off[r];
+      const int b = prb_bin_of(d);
+      atomicAdd((unsigned long long *)&s[b], 1ull);
+      if (b == 6) atomicAdd((unsigned long long *)&s[PRB_BINS], (unsigned long long)((d + PRB_CHUNK - 1) / PRB_CHUNK));
+    }
   }
   __syncthreads();
-  if (threadIdx.x <= PRB_BINS && s[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], s[threadIdx.x]);
+  if (threadIdx.x <= PRB_BINS) counts[(int64_t)blockIdx.x * (PRB_BINS + 1) + threadIdx.x] = s[threadIdx.x];
 }
 
-// Scatters rows into their bins (order inside a bin does not affect results).
-__global__ void prb_scatter_kernel(const int32_t *__restrict__ off, int64_t n, const int64_t *__restrict__ boff,
-                                   unsigned long long *cursor, int32_t *rows, int32_t *hrows) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    const int b = prb_bin_of(off[r + 1] - off[r]);
-    const unsigned long long p = atomicAdd(&cursor[b], 1ull);
-    if (b < 6) rows[boff[b] + (int64_t)p] = (int32_t)r;
-    else hrows[p] = (int32_t)r;
+// Exclusive prefix over chunks of every bin, in place; totals[b] = bin sizes.
+__global__ void prb_offsets_kernel(int64_t *counts, int64_t nchunks, int64_t *totals) {
+  const int b = threadIdx.x;
+  if (b > PRB_BINS) return;
+  int64_t acc = 0;
+  for (int64_t c = 0; c < nchunks; c++) {
+    const int64_t v = counts[c * (PRB_BINS + 1) + b];
+    counts[c * (PRB_BINS + 1) + b] = acc;
+    acc += v;
   }
+  totals[b] = acc;
 }
 
-// Sorts the hub list (tiny) and fills the chunk bases; one CTA.
-__global__ void prb_hubs_kernel(const int32_t *__restrict__ off, int32_t *hrows, int64_t nheavy, int32_t *hbase) {
-  if (threadIdx.x != 0) return;
-  for (int64_t i = 1; i < nheavy; i++) {  // insertion sort: hubs are few and the list is built once
-    const int32_t v = hrows[i];
-    int64_t j = i - 1;
-    while (j >= 0 && hrows[j] > v) {
-      hrows[j + 1] = hrows[j];
-      j--;
+__global__ void __launch_bounds__(PRB_NT) prb_scatter_kernel(const int32_t *__restrict__ off, int64_t n,
+                                                             const int64_t *__restrict__ offsets,
+                                                             const int64_t *__restrict__ boff, int32_t *rows,
+                                                             int32_t *hrows) {
+  __shared__ int32_t red[PRB_NT / 32 + 1];
+  const int64_t base = (int64_t)blockIdx.x * PRB_CHUNK_ROWS;
+  int bins[PRB_RPT];
+#pragma unroll
+  for (int k = 0; k < PRB_RPT; k++) {
+    const int64_t r = base + (int64_t)threadIdx.x * PRB_RPT + k;
+    bins[k] = r < n ? prb_bin_of(off[r + 1] - off[r]) : -1;
+  }
+  for (int b = 0; b < PRB_BINS; b++) {
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < PRB_RPT; k++) cnt += bins[k] == b;
+    int32_t tot;
+    int pos = block_exclusive_scan<PRB_NT>(cnt, red, &tot);
+    const int64_t o = offsets[(int64_t)blockIdx.x * (PRB_BINS + 1) + b];
+#pragma unroll
+    for (int k = 0; k < PRB_RPT; k++) {
+      if (bins[k] == b) {
+        const int32_t r = (int32_t)(base + (int64_t)threadIdx.x * PRB_RPT + k);
+        if (b < 6) rows[boff[b] + o + pos] = r;
+        else hrows[o + pos] = r;
+        pos++;
+      }
     }
-    hrows[j + 1] = v;
   }
-  int32_t acc = 0;
-  for (int64_t i = 0; i < nheavy; i++) {
-    hbase[i] = acc;
-    const int32_t d = off[hrows[i] + 1] - off[hrows[i]];
-    acc += (d + PRB_CHUNK - 1) / PRB_CHUNK;
+}
+
+// Chunk bases of the hubs (listed in ascending order): one CTA, exclusive scan of
+// their chunk counts PRB_NT at a time.
+__global__ void __launch_bounds__(PRB_NT) prb_hubs_kernel(const int32_t *__restrict__ off, const int32_t *hrows,
+                                                          int64_t nheavy, int32_t *hbase) {
+  __shared__ int32_t red[PRB_NT / 32 + 1];
+  int32_t carry = 0;
+  for (int64_t b0 = 0; b0 < nheavy; b0 += PRB_NT) {
+    const int64_t i = b0 + threadIdx.x;
+    int32_t c = 0;
+    if (i < nheavy) {
+      const int32_t d = off[hrows[i] + 1] - off[hrows[i]];
+      c = (d + PRB_CHUNK - 1) / PRB_CHUNK;
+    }
+    int32_t tot;
+    const int32_t ex = block_exclusive_scan<PRB_NT>(c, red, &tot);
+    if (i < nheavy) hbase[i] = carry + ex;
+    carry += tot;
   }
-  hbase[nheavy] = acc;
+  if (threadIdx.x == 0) hbase[nheavy] = carry;
 }
 
 struct PrbArgs {
@@ -136,25 +182,6 @@ __device__ __forceinline__ void group_comp_reduce(Comp &c) {
   }
 }
 
-// Rows of a light bin with G lanes per row; warp assignment `wa` within the bin.
-template <int G, bool WEIGHTED, typename Gather, typename Finish>
-__device__ __forceinline__ void prb_light(const PrbArgs &p, int bin, int64_t wa, Gather &gather, Finish &finish) {
-  const int lane = threadIdx.x & 31;
-  const int64_t i = wa * (32 / G) + lane / G;
-  const int gl = lane % G;
-  const int64_t nb = p.boff[bin + 1] - p.boff[bin];
-  int32_t row = -1, b = 0, e = 0;
-  if (i < nb) {
-    row = p.rows[p.boff[bin] + i];
-    b = __ldg(p.off + row);
-    e = __ldg(p.off + row + 1);
-  }
-  Comp acc{0.f, 0.f};
-  for (int32_t k = b + gl; k < e; k += G) prb_add<WEIGHTED>(acc, gather(__ldg(p.idx + k)), p.wts, k);
-  group_comp_reduce<G>(acc);
-  if (row >= 0 && gl == 0) finish(row, acc);
-}
-
 // One warp reduces edges [b, e) of a row: 4 independent loads in flight per lane.
 template <bool WEIGHTED, typename Gather>
 __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int32_t e, Gather &gather) {
@@ -175,6 +202,39 @@ __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int3
   return acc;
 }
 
+// 32 consecutive rows of bin `bin` (warp assignment `wa`), G lanes per row:
+// G passes of 32/G rows each; the sum of slot l ends up in lane l, whose row is
+// returned in *my_row (-1 past the bin), so the row updates then run on all
+// lanes at once.
+template <int G, bool WEIGHTED, typename Gather>
+__device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa, Gather &gather, int32_t *my_row) {
+  constexpr int RPP = 32 / G;  // rows per pass
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = p.boff[bin] + wa * 32 + lane;
+  const int32_t mine_row = slot < p.boff[bin + 1] ? p.rows[slot] : -1;
+  const int gl = lane % G, grp = lane / G;
+  Comp mine{0.f, 0.f};
+#pragma unroll 1
+  for (int q = 0; q < G; q++) {
+    const int32_t row = __shfl_sync(0xffffffffu, mine_row, q * RPP + grp);
+    Comp acc{0.f, 0.f};
+    if (G == 32) {
+      if (row >= 0) acc = prb_warp_range<WEIGHTED>(p, __ldg(p.off + row), __ldg(p.off + row + 1), gather);
+    } else {
+      if (row >= 0) {
+        const int32_t b = __ldg(p.off + row), e = __ldg(p.off + row + 1);
+        for (int32_t k = b + gl; k < e; k += G) prb_add<WEIGHTED>(acc, gather(__ldg(p.idx + k)), p.wts, k);
+      }
+      group_comp_reduce<G>(acc);
+    }
+    const int src = (lane % RPP) * G;
+    const float h = __shfl_sync(0xffffffffu, acc.hi, src), l = __shfl_sync(0xffffffffu, acc.lo, src);
+    if (lane / RPP == q) mine = Comp{h, l};
+  }
+  *my_row = mine_row;
+  return mine;
+}
+
 // Walks every assignment of the plan with a persistent grid (fixed stride).
 // finish(row, Comp) consumes a row sum; finish_hub(h, row, Comp) consumes a hub's.
 template <bool WEIGHTED, typename Gather, typename Finish, typename FinishHub>
@@ -188,18 +248,21 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
     for (int q = 1; q < PRB_BINS; q++)
       if (w >= p.wstart[q]) bin = q;
     const int64_t wa = w - p.wstart[bin];
-    switch (bin) {
-      case 0: prb_light<1, WEIGHTED>(p, 0, wa, gather, finish); break;
-      case 1: prb_light<2, WEIGHTED>(p, 1, wa, gather, finish); break;
-      case 2: prb_light<4, WEIGHTED>(p, 2, wa, gather, finish); break;
-      case 3: prb_light<8, WEIGHTED>(p, 3, wa, gather, finish); break;
-      case 4: prb_light<16, WEIGHTED>(p, 4, wa, gather, finish); break;
-      case 5: {
-        const int32_t row = p.rows[p.boff[5] + wa];
-        const Comp acc = prb_warp_range<WEIGHTED>(p, __ldg(p.off + row), __ldg(p.off + row + 1), gather);
-        if (lane == 0) finish(row, acc);
-        break;
+    if (bin < 6) {
+      int32_t row = -1;
+      Comp acc;
+      switch (bin) {
+        case 0: acc = prb_rows32<1, WEIGHTED>(p, 0, wa, gather, &row); break;
+        case 1: acc = prb_rows32<2, WEIGHTED>(p, 1, wa, gather, &row); break;
+        case 2: acc = prb_rows32<4, WEIGHTED>(p, 2, wa, gather, &row); break;
+        case 3: acc = prb_rows32<8, WEIGHTED>(p, 3, wa, gather, &row); break;
+        case 4: acc = prb_rows32<16, WEIGHTED>(p, 4, wa, gather, &row); break;
+        default: acc = prb_rows32<32, WEIGHTED>(p, 5, wa, gather, &row); break;
       }
+      if (row >= 0) finish(row, acc);
+      continue;
+    }
+    switch (bin) {
       default: {
         // Hub chunk task `wa`: find its hub by binary search over the chunk bases.
         int64_t lo = 0, hi = p.nheavy;

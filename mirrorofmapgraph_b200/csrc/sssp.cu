@@ -36,6 +36,7 @@ struct SsspArgs {
   int32_t qcap;
   int32_t both;
   int64_t n;
+  int32_t *big_v;  // grid-strided bin (BIG_CAP entries)
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
@@ -79,6 +80,7 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   c->qlen[cur] = 0;
   c->cur = cur ^ 1;
   c->blocks_done = 0;
+  c->big_len = 0;
   const bool over = vload(&c->overflow) != 0;
   const bool done = nf == 0 || lvl >= c->iter_cap || over;
   if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
@@ -102,6 +104,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, 0, 0};
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
+  const BigList big{a.big_v, &c->big_len};
   for (int64_t tile = (int64_t)blockIdx.x * SSSP_NT; tile < nin; tile += (int64_t)gridDim.x * SSSP_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
     }
     expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) {
       relax(x, sv, ci[k], w ? w[k] : 1);
-    });
+    }, &big);
     if (a.both)
       expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) {
         relax(x, sv, ri[k], cw ? cw[k] : 1);
@@ -127,6 +130,28 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
     if (b0) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b0);
     if (b1) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)b1);
     if (b2) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)b2);
+    if (b3) atomicAdd((unsigned long long *)&c->vertices_updated, (unsigned long long)b3);
+  }
+}
+
+// Grid-strided bin of a relaxation round; the last CTA closes the round.
+__global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
+  __shared__ BigSmem<SSSP_NT> sm;
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, 0, 0};
+  const int32_t *ci = a.ci, *w = a.w;
+  expand_big<SSSP_NT>(sm, a.ro, BigList{a.big_v, &c->big_len},
+                      [&](int32_t sv, int32_t k) { relax(x, sv, ci[k], w ? w[k] : 1); });
+  const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
+  const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
+  if (threadIdx.x == 0) {
+    if (b0) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b0);
     if (b3) atomicAdd((unsigned long long *)&c->vertices_updated, (unsigned long long)b3);
   }
   if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
@@ -222,7 +247,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
   const int64_t nwords = (n + 31) / 32;
   const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
-                                   sizeof(int32_t) * (size_t)nsrc});
+                                   sizeof(int32_t) * (size_t)nsrc, sizeof(int32_t) * (size_t)BIG_CAP});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   SsspArgs a;
@@ -231,6 +256,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
   a.q0 = cv.take<int32_t>(qcap);
   a.q1 = cv.take<int32_t>(qcap);
   int32_t *dsrc = cv.take<int32_t>(nsrc);
+  a.big_v = cv.take<int32_t>(BIG_CAP);
   a.ro = g->ro;
   a.ci = g->ci;
   a.w = g->vtype == MG_DTYPE_I32 ? (const int32_t *)g->vals : nullptr;
@@ -265,6 +291,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
     b.h = h;
     b.use_cond = use_cond;
     sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    sssp_relax_big_kernel<<<grid, SSSP_NT, 0, st>>>(b);
   };
   MG_TRY(run_loop(g, SLOT_SSSP, &sig, sizeof(sig), o.use_graph >= 0, body, (int64_t)n + 2));
   MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
@@ -279,7 +306,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
-    stats->launches = 2 + (o.use_graph >= 0 ? 2 * (int64_t)hc.body_iters : (int64_t)hc.level);
+    stats->launches = 2 + (o.use_graph >= 0 ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
   }
   if (hc.status != 0) {
     mg_set_error("mg_sssp: device status %d (queue capacity %d)", hc.status, qcap);

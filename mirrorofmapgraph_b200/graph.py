@@ -279,6 +279,7 @@ class Graph:
         gw, gw_p, dev1 = self._out(out_weights, self.m, np.float32) if want_weights else (None, None, r_dev)
         gt, gt_p, dev2 = self._out(out_teleport, self.n, np.float32) if want_teleport else (None, None, r_dev)
         st = L.MgStats()
+        kw.setdefault("mode", "normalized")
         o = self._pr_opts(device_output=r_dev, **kw)
         _check(self._lib.mg_pagerank_backward(self._h, t_p, r_p, w_p, gw_p, gt_p, C.byref(o), C.byref(st)),
                "mg_pagerank_backward")
