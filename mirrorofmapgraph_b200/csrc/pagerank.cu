@@ -330,7 +330,7 @@ __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *h
 
 // One whole iteration of the degree-binned solver.
 template <bool WEIGHTED>
-__global__ void __launch_bounds__(PRB_NT, 5) solve_binned_kernel(SolveArgs a, PrbArgs p) {
+__global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) solve_binned_kernel(SolveArgs a, PrbArgs p) {
   __shared__ double s_red[PRB_NT / 32 + 1];
   if (solve_skip(a)) return;
   DevCtl *c = a.ctl;

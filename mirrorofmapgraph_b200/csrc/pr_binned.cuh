@@ -26,6 +26,18 @@ namespace mg {
 
 constexpr int PRB_NT = 256;
 constexpr int PRB_BINS = 7;
+// Resident CTAs per SM the iteration kernel is compiled for, and how many passes
+// of a light bin issue their loads before the first reduction.
+#ifndef PRB_MIN_BLOCKS
+#define PRB_MIN_BLOCKS 6
+#endif
+#ifndef PRB_BATCH
+#define PRB_BATCH 8
+#endif
+// Strides of 32 edges a warp-per-row gather loads before its first add.
+#ifndef PRB_UNROLL
+#define PRB_UNROLL 8
+#endif
 constexpr int32_t PRB_HEAVY = 2048;
 constexpr int32_t PRB_CHUNK = 2048;
 
@@ -187,49 +199,75 @@ template <bool WEIGHTED, typename Gather>
 __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int32_t e, Gather &gather) {
   const int lane = threadIdx.x & 31;
   Comp acc{0.f, 0.f};
-  int32_t k = b + lane;
-  for (; k + 96 < e; k += 128) {
-    const int32_t c0 = __ldg(p.idx + k), c1 = __ldg(p.idx + k + 32), c2 = __ldg(p.idx + k + 64),
-                  c3 = __ldg(p.idx + k + 96);
-    const float g0 = gather(c0), g1 = gather(c1), g2 = gather(c2), g3 = gather(c3);
-    prb_add<WEIGHTED>(acc, g0, p.wts, k);
-    prb_add<WEIGHTED>(acc, g1, p.wts, k + 32);
-    prb_add<WEIGHTED>(acc, g2, p.wts, k + 64);
-    prb_add<WEIGHTED>(acc, g3, p.wts, k + 96);
+  // PRB_UNROLL strides of 32 edges per round, predicated: a row of up to
+  // 32 * PRB_UNROLL edges costs one index and one gather round trip.
+  for (int32_t k = b + lane; k < e; k += 32 * PRB_UNROLL) {
+    int32_t c[PRB_UNROLL];
+    float x[PRB_UNROLL];
+#pragma unroll
+    for (int j = 0; j < PRB_UNROLL; j++) c[j] = k + 32 * j < e ? __ldg(p.idx + k + 32 * j) : -1;
+#pragma unroll
+    for (int j = 0; j < PRB_UNROLL; j++) x[j] = c[j] >= 0 ? gather(c[j]) : 0.f;
+#pragma unroll
+    for (int j = 0; j < PRB_UNROLL; j++)
+      if (c[j] >= 0) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
   }
-  for (; k < e; k += 32) prb_add<WEIGHTED>(acc, gather(__ldg(p.idx + k)), p.wts, k);
   group_comp_reduce<32>(acc);
   return acc;
 }
 
 // 32 consecutive rows of bin `bin` (warp assignment `wa`), G lanes per row:
-// G passes of 32/G rows each; the sum of slot l ends up in lane l, whose row is
-// returned in *my_row (-1 past the bin), so the row updates then run on all
-// lanes at once.
+// every lane first loads its slot's row and offsets; then G passes of 32/G rows
+// each. For light bins (G < 32, at most G edges per row) all G passes issue their
+// index loads and then their gathers back to back before any reduction, so a warp
+// waits for three memory round trips per assignment rather than three per pass.
+// The sum of slot l ends up in lane l, whose row is returned in *my_row (-1 past
+// the bin), so the row updates then run on all lanes at once.
 template <int G, bool WEIGHTED, typename Gather>
 __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa, Gather &gather, int32_t *my_row) {
   constexpr int RPP = 32 / G;  // rows per pass
   const int lane = threadIdx.x & 31;
   const int64_t slot = p.boff[bin] + wa * 32 + lane;
   const int32_t mine_row = slot < p.boff[bin + 1] ? p.rows[slot] : -1;
+  const int32_t mb = mine_row >= 0 ? __ldg(p.off + mine_row) : 0;
+  const int32_t me = mine_row >= 0 ? __ldg(p.off + mine_row + 1) : 0;
   const int gl = lane % G, grp = lane / G;
   Comp mine{0.f, 0.f};
+  if (G == 32) {
 #pragma unroll 1
-  for (int q = 0; q < G; q++) {
-    const int32_t row = __shfl_sync(0xffffffffu, mine_row, q * RPP + grp);
-    Comp acc{0.f, 0.f};
-    if (G == 32) {
-      if (row >= 0) acc = prb_warp_range<WEIGHTED>(p, __ldg(p.off + row), __ldg(p.off + row + 1), gather);
-    } else {
-      if (row >= 0) {
-        const int32_t b = __ldg(p.off + row), e = __ldg(p.off + row + 1);
-        for (int32_t k = b + gl; k < e; k += G) prb_add<WEIGHTED>(acc, gather(__ldg(p.idx + k)), p.wts, k);
-      }
-      group_comp_reduce<G>(acc);
+    for (int q = 0; q < 32; q++) {
+      const int32_t b = __shfl_sync(0xffffffffu, mb, q), e = __shfl_sync(0xffffffffu, me, q);
+      const Comp acc = prb_warp_range<WEIGHTED>(p, b, e, gather);
+      if (lane == q) mine = acc;
     }
-    const int src = (lane % RPP) * G;
-    const float h = __shfl_sync(0xffffffffu, acc.hi, src), l = __shfl_sync(0xffffffffu, acc.lo, src);
-    if (lane / RPP == q) mine = Comp{h, l};
+  } else {
+    // Passes run in batches of up to 8 so the in-flight loads fit the register budget.
+    constexpr int BATCH = G < PRB_BATCH ? G : PRB_BATCH;
+#pragma unroll
+    for (int q0 = 0; q0 < G; q0 += BATCH) {
+      int32_t k_of[BATCH];
+      int32_t c_of[BATCH];
+      float v_of[BATCH];
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) {
+        const int src = (q0 + j) * RPP + grp;
+        const int32_t b = __shfl_sync(0xffffffffu, mb, src), e = __shfl_sync(0xffffffffu, me, src);
+        k_of[j] = b + gl < e ? b + gl : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) c_of[j] = k_of[j] >= 0 ? __ldg(p.idx + k_of[j]) : 0;
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) v_of[j] = k_of[j] >= 0 ? gather(c_of[j]) : 0.f;
+#pragma unroll
+      for (int j = 0; j < BATCH; j++) {
+        Comp acc{0.f, 0.f};
+        if (k_of[j] >= 0) prb_add<WEIGHTED>(acc, v_of[j], p.wts, k_of[j]);
+        group_comp_reduce<G>(acc);
+        const int src = (lane % RPP) * G;
+        const float h = __shfl_sync(0xffffffffu, acc.hi, src), l = __shfl_sync(0xffffffffu, acc.lo, src);
+        if (lane / RPP == q0 + j) mine = Comp{h, l};
+      }
+    }
   }
   *my_row = mine_row;
   return mine;
