@@ -214,6 +214,26 @@ mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *
                                const float *dL_dranks, float *dL_dweights, float *dL_dteleport,
                                const mg_pr_opts *opts, mg_stats *stats);
 
+/* ---- BFS over a fixed scratch area (no reference counterpart) --------------
+ * The same traversal and results as mg_bfs, for callers that must not allocate
+ * device memory while they run (memory reserved up front, code running inside
+ * an allocator). Frontier queues, visited bitmap, sources and the deferred-hub
+ * list live in one static device array of 8.54 MB; nothing is allocated.
+ * - depth must be DEVICE memory (n entries); opts->device_output and
+ *   opts->use_graph are ignored (the level loop is driven from the host).
+ * - Graphs of more than MG_BFS_NOALLOC_MAX_VERTICES vertices, or more than
+ *   MG_BFS_NOALLOC_MAX_SOURCES sources, are rejected with MG_ERR_ARG.
+ * - The first call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) and caches it; make that first call before any
+ *   stream capture on the device.
+ * - The array is shared by every graph on a device: two calls in flight on the
+ *   same device at the same time (other threads or streams) race on it and
+ *   corrupt each other's results. Serialise them. */
+#define MG_BFS_NOALLOC_MAX_VERTICES (1 << 20)
+#define MG_BFS_NOALLOC_MAX_SOURCES 1024
+mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth, const mg_opts *opts,
+                         mg_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

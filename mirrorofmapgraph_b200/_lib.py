@@ -25,6 +25,8 @@ MG_GRAPH_SYMMETRIC, MG_GRAPH_NO_CSC, MG_GRAPH_DEVICE_INPUT = 0x1, 0x2, 0x4
 MG_DIR_AUTO, MG_DIR_PUSH, MG_DIR_PULL = 0, 1, 2
 MG_PR_REFCOMPAT, MG_PR_NORMALIZED = 0, 1
 MG_W_NONE, MG_W_UNIFORM_INT, MG_W_LOGNORMAL = 0, 1, 2
+MG_BFS_NOALLOC_MAX_VERTICES = 1 << 20
+MG_BFS_NOALLOC_MAX_SOURCES = 1024
 
 
 class MgOpts(C.Structure):
@@ -70,6 +72,7 @@ SIGNATURES = {
     "mg_graph_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mg_graph_device_arrays": (C.c_int, [_P] + [C.POINTER(_P)] * 6),
     "mg_bfs": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
+    "mg_bfs_noalloc": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_sssp": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_cc": (C.c_int, [_P, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_pagerank": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgPrOpts), C.POINTER(MgStats)]),

@@ -28,6 +28,8 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -403,6 +405,162 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   }
   if (hc.status != 0) {
     mg_set_error("mg_bfs: frontier exceeded queue capacity %d", qcap);
+    return (mg_status)hc.status;
+  }
+  return MG_OK;
+}
+
+// ---- BFS over a fixed, statically allocated scratch area -------------------
+// mg_bfs grows the graph's workspace on demand, which allocates device memory on
+// the first call and whenever a call needs more. Some callers cannot allow that:
+// a serving process that reserved its device memory up front and must not grow it
+// while requests run, code called from inside a memory allocator (which must not
+// re-enter the allocator), or a caller that keeps every device allocation under
+// its own accounting. This variant takes its frontier queues, visited bitmap,
+// source list and deferred-hub list from one file-scope device array of fixed
+// size, writes depths straight into the caller's device buffer, and drives the
+// level loop from the host (no executable graph is instantiated).
+namespace mg {
+
+constexpr int64_t NOALLOC_MAX_N = MG_BFS_NOALLOC_MAX_VERTICES;
+constexpr int64_t NOALLOC_MAX_SRC = MG_BFS_NOALLOC_MAX_SOURCES;
+constexpr size_t noalloc_round(size_t b) { return (b + 255) & ~(size_t)255; }
+// Layout (bytes, each part 256-aligned): visited bitmap, two frontier queues,
+// sources, deferred hubs.
+constexpr size_t NOALLOC_VIS = 0;
+constexpr size_t NOALLOC_Q0 = NOALLOC_VIS + noalloc_round(sizeof(uint32_t) * ((NOALLOC_MAX_N + 31) / 32));
+constexpr size_t NOALLOC_Q1 = NOALLOC_Q0 + noalloc_round(sizeof(int32_t) * NOALLOC_MAX_N);
+constexpr size_t NOALLOC_SRC = NOALLOC_Q1 + noalloc_round(sizeof(int32_t) * NOALLOC_MAX_N);
+constexpr size_t NOALLOC_BIG = NOALLOC_SRC + noalloc_round(sizeof(int32_t) * NOALLOC_MAX_SRC);
+constexpr size_t NOALLOC_BYTES = NOALLOC_BIG + noalloc_round(sizeof(int32_t) * BIG_CAP);  // 8,540,160 bytes
+
+// Nothing in it has to start at zero: every call clears the bitmap itself and
+// writes the queues, sources and hub list before reading them.
+static __device__ __align__(256) uint32_t bfs_noalloc_scratch[NOALLOC_BYTES / sizeof(uint32_t)];
+
+// Device address of the scratch array, resolved once per device (the first call
+// on a device; later calls reuse the cached address).
+static std::mutex noalloc_mu;
+static std::vector<char *> noalloc_addr;
+
+static mg_status noalloc_scratch_of(int device, char **out) {
+  std::lock_guard<std::mutex> lk(noalloc_mu);
+  if ((int)noalloc_addr.size() <= device) noalloc_addr.resize(device + 1, nullptr);
+  if (!noalloc_addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, bfs_noalloc_scratch);
+    if (e != cudaSuccess) {
+      mg_set_error("mg_bfs_noalloc: cudaGetSymbolAddress of the scratch array failed on device %d: %s", device,
+                   cudaGetErrorString(e));
+      return MG_ERR_CUDA;
+    }
+    noalloc_addr[device] = static_cast<char *>(p);
+  }
+  *out = noalloc_addr[device];
+  return MG_OK;
+}
+
+}  // namespace mg
+
+extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth,
+                                    const mg_opts *opts, mg_stats *stats) {
+  using namespace mg;
+  if (!g || !srcs || nsrc <= 0 || !depth) {
+    mg_set_error("mg_bfs_noalloc: null argument or nsrc <= 0");
+    return MG_ERR_ARG;
+  }
+  if (g->n > NOALLOC_MAX_N) {
+    mg_set_error("mg_bfs_noalloc: graph has %lld vertices, the fixed scratch holds at most %lld (use mg_bfs)",
+                 (long long)g->n, (long long)NOALLOC_MAX_N);
+    return MG_ERR_ARG;
+  }
+  if (nsrc > NOALLOC_MAX_SRC) {
+    mg_set_error("mg_bfs_noalloc: %d sources, the fixed scratch holds at most %lld", nsrc,
+                 (long long)NOALLOC_MAX_SRC);
+    return MG_ERR_ARG;
+  }
+  mg_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.directed = 1;
+  if (opts) o = *opts;
+  if (o.direction < MG_DIR_AUTO || o.direction > MG_DIR_PULL) {
+    mg_set_error("mg_bfs_noalloc: invalid direction %d", o.direction);
+    return MG_ERR_ARG;
+  }
+  for (int32_t i = 0; i < nsrc; i++) {
+    if (srcs[i] < 0 || srcs[i] >= g->n) {
+      mg_set_error("mg_bfs_noalloc: source %d out of range [0, %lld)", srcs[i], (long long)g->n);
+      return MG_ERR_ARG;
+    }
+  }
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  const bool undirected = o.directed == 0 && !symmetric;
+  if (undirected && !g->has_csc) {
+    mg_set_error("mg_bfs_noalloc: directed=0 needs the CSC (graph created with MG_GRAPH_NO_CSC)");
+    return MG_ERR_UNSUPPORTED;
+  }
+  MG_TRY(graph_enter(g));
+  char *scratch = nullptr;
+  MG_TRY(noalloc_scratch_of(g->device, &scratch));
+  const int64_t n = g->n;
+  int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)n) : n;
+  qcap64 = std::max<int64_t>(1, std::min<int64_t>(qcap64, n));
+  const int32_t qcap = (int32_t)qcap64;
+  int32_t *dsrc = reinterpret_cast<int32_t *>(scratch + NOALLOC_SRC);
+  cudaStream_t s = g->stream;
+
+  BfsArgs a;
+  a.ro = g->ro;
+  a.ci = g->ci;
+  a.co = g->has_csc ? g->co : g->ro;
+  a.ri = g->has_csc ? g->ri : g->ci;
+  a.label = depth;
+  a.vis = reinterpret_cast<uint32_t *>(scratch + NOALLOC_VIS);
+  a.q0 = reinterpret_cast<int32_t *>(scratch + NOALLOC_Q0);
+  a.q1 = reinterpret_cast<int32_t *>(scratch + NOALLOC_Q1);
+  a.qcap = qcap;
+  a.mode = o.direction;
+  a.can_pull = g->has_csc && !undirected;
+  a.both = undirected ? 1 : 0;
+  a.n = n;
+  a.m_total = g->m;
+  a.big_v = reinterpret_cast<int32_t *>(scratch + NOALLOC_BIG);
+  a.ctl = g->ctl;
+  a.h = 0;
+  a.use_cond = 0;
+
+  const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
+  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  bfs_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(depth, a.vis, n);
+  bfs_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap, 0);
+  MG_CUDA_TRY(cudaGetLastError());
+  const int grid = g->num_sms * 4;
+  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle, int) {
+    bfs_push_kernel<<<grid, BFS_NT, 0, st>>>(a);
+    bfs_push_big_kernel<<<grid, BFS_NT, 0, st>>>(a);
+    bfs_pull_kernel<<<grid, BFS_NT, 0, st>>>(a);
+  };
+  MG_TRY(run_loop(g, SLOT_BFS, nullptr, 0, false, body, n + 2));
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = hc.visited_deg;
+    stats->edges_inspected = hc.edges_inspected;
+    stats->bytes_compulsory = 4 * hc.edges_inspected + 16 * hc.vertices_expanded + 4 * n +
+                              (int64_t)hc.levels_pull * ((n + 7) / 8);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+    stats->status_detail = hc.levels_pull;
+    stats->launches = 2 + 3 * (int64_t)hc.level;
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_bfs_noalloc: frontier exceeded queue capacity %d", qcap);
     return (mg_status)hc.status;
   }
   return MG_OK;
