@@ -30,14 +30,19 @@ struct ExpandSmem {
 struct BigList;
 __device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t deg);
 
+//
+// `vmask` maps a frontier item to the vertex whose offsets it uses (item & vmask);
+// -1 (every bit) is the identity. Batched runs pack an instance number into the
+// item's high bits and pass the low-bit mask.
 template <int NT, int CTA_TH, typename Visit>
 __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *__restrict__ off, int32_t v,
-                                            int64_t &insp, Visit &&visit, const BigList *big = nullptr) {
+                                            int64_t &insp, Visit &&visit, const BigList *big = nullptr,
+                                            int32_t vmask = -1) {
   const int tid = threadIdx.x, lane = lane_id();
   int32_t beg = 0, deg = 0;
   if (v >= 0) {
-    beg = off[v];
-    deg = off[v + 1] - beg;
+    beg = off[v & vmask];
+    deg = off[(v & vmask) + 1] - beg;
     insp += deg;
   }
   // Vertices for the grid-strided bin are expanded by a later kernel.
@@ -122,7 +127,7 @@ struct BigSmem {
 // vertices; an edge slot finds its vertex by binary search over their prefix sums.
 template <int NT, typename Visit>
 __device__ __forceinline__ void expand_big(BigSmem<NT> &sm, const int32_t *__restrict__ off, const BigList &big,
-                                           Visit &&visit) {
+                                           Visit &&visit, int32_t vmask = -1) {
   const int32_t nb = min(*(const volatile int32_t *)big.len, BIG_CAP);
   if (nb == 0) return;
   // Degrees and their exclusive prefix, NT * ceil(nb / NT) at a time.
@@ -133,7 +138,7 @@ __device__ __forceinline__ void expand_big(BigSmem<NT> &sm, const int32_t *__res
     if (i < nb) {
       const int32_t v = big.v[i];
       sm.v[i] = v;
-      d = off[v + 1] - off[v];
+      d = off[(v & vmask) + 1] - off[v & vmask];
     }
     int32_t tot;
     const int32_t ex = block_exclusive_scan<NT>(d, sm.red, &tot);
@@ -153,7 +158,7 @@ __device__ __forceinline__ void expand_big(BigSmem<NT> &sm, const int32_t *__res
       else b = mid;
     }
     const int32_t v = sm.v[a];
-    visit(v, off[v] + (int32_t)(k - sm.pre[a]));
+    visit(v, off[v & vmask] + (int32_t)(k - sm.pre[a]));
   }
   __syncthreads();
 }

@@ -28,6 +28,7 @@
 #include "expand.cuh"
 #include "pr_binned.cuh"
 #include "pr_gather.cuh"
+#include "ppr.cuh"
 
 namespace mg {
 
@@ -964,6 +965,184 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
   return MG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batched personalised PageRank (nvec > 1): groups of up to 256 vectors solved
+// together over the vertex-major layout of ppr.cuh.
+template <int VPL, bool W>
+static int ppr_occupancy() {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::ppr_iter_kernel<VPL, W>, mg::PPR_NT, 0);
+  cudaGetLastError();
+  return std::max(1, std::min(occ, 8));
+}
+
+template <int VPL, bool W>
+static void ppr_launch_iter(const mg::PprArgs &a, cudaStream_t st) {
+  mg::ppr_iter_kernel<VPL, W><<<a.grid, mg::PPR_NT, 0, st>>>(a);
+}
+
+template <int VPL>
+static void ppr_launch_init(const mg::PprArgs &a, int grid, cudaStream_t st) {
+  mg::ppr_init_kernel<VPL><<<grid, mg::PPR_NT, 0, st>>>(a);
+}
+
+static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, float *ranks_out, int out_is_device,
+                              const mg_pr_opts &o, mg_stats *stats) {
+  using namespace mg;
+  const bool weighted = o.weighted != 0;
+  if (!g->has_csc) {
+    mg_set_error("mg_pagerank: the gather over in-edges needs the CSC");
+    return MG_ERR_UNSUPPORTED;
+  }
+  if (weighted && g->vtype != MG_DTYPE_F32) {
+    mg_set_error("mg_pagerank: weighted mode needs float edge values");
+    return MG_ERR_ARG;
+  }
+  BinPlan *bins = nullptr, *rbins = nullptr;
+  MG_TRY(get_bin_plan(g, false, &bins));
+  if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
+  const int64_t n = g->n;
+  const int32_t kmax = std::min<int32_t>(nvec, PPR_MAXW);
+  const int vpl = kmax > 128 ? 8 : kmax > 64 ? 4 : kmax > 32 ? 2 : 1;
+  const int32_t W = 32 * vpl;
+  int occ = 1;
+  switch (vpl * 2 + (weighted ? 1 : 0)) {
+    case 2: occ = ppr_occupancy<1, false>(); break;
+    case 3: occ = ppr_occupancy<1, true>(); break;
+    case 4: occ = ppr_occupancy<2, false>(); break;
+    case 5: occ = ppr_occupancy<2, true>(); break;
+    case 8: occ = ppr_occupancy<4, false>(); break;
+    case 9: occ = ppr_occupancy<4, true>(); break;
+    case 16: occ = ppr_occupancy<8, false>(); break;
+    default: occ = ppr_occupancy<8, true>(); break;
+  }
+  const int grid = g->num_sms * occ;
+  const int ginit = g->num_sms * 8;
+  const int gpart = std::max(grid, ginit);
+  const size_t nw = (size_t)n * W;
+  const int64_t nchunks = bins->ntasks, nheavy = bins->nheavy;
+  const size_t need = Carve::need({sizeof(float) * nw, sizeof(float) * nw, sizeof(float) * nw, sizeof(float) * nw,
+                                   sizeof(float) * nw, sizeof(float) * ((size_t)n + 8), sizeof(double) * W,
+                                   sizeof(double) * 2 * W * (size_t)gpart,
+                                   sizeof(Comp) * W * (size_t)std::max<int64_t>(nchunks, 1),
+                                   sizeof(int32_t) * (size_t)std::max<int64_t>(nheavy, 1),
+                                   sizeof(double) * 2 * W * (size_t)std::max<int64_t>(nheavy, 1),
+                                   out_is_device ? 0 : sizeof(float) * (size_t)kmax * n});
+  MG_TRY(ws_reserve(g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  PprArgs a;
+  std::memset(&a, 0, sizeof(a));
+  float *tele = cv.take<float>(nw);
+  a.x0 = cv.take<float>(nw);
+  a.x1 = cv.take<float>(nw);
+  a.g0 = cv.take<float>(nw);
+  a.g1 = cv.take<float>(nw);
+  float *srow = cv.take<float>((size_t)n + 8);
+  a.dang = cv.take<double>(W);
+  a.part = cv.take<double>(2 * (size_t)W * gpart);
+  a.hpart = cv.take<Comp>((size_t)W * std::max<int64_t>(nchunks, 1));
+  a.hcount = cv.take<int32_t>(std::max<int64_t>(nheavy, 1));
+  a.hres = cv.take<double>(2 * (size_t)W * std::max<int64_t>(nheavy, 1));
+  float *stage = out_is_device ? nullptr : cv.take<float>((size_t)kmax * n);
+  a.off = g->co;
+  a.idx = g->ri;
+  a.wts = weighted ? (const float *)g->cvals : nullptr;
+  a.rows = bins->rows;
+  a.nlight = bins->boff[6];
+  a.hrows = bins->hrows;
+  a.hbase = bins->hbase;
+  a.nheavy = nheavy;
+  a.nchunks = nchunks;
+  a.srow = srow;
+  a.tele = tele;
+  a.n = n;
+  a.W = W;
+  a.alpha = o.alpha > 0 ? o.alpha : 0.85;
+  a.tol = o.tol > 0 ? o.tol : 1e-6;
+  a.max_iter = o.max_iter > 0 ? o.max_iter : 50;
+  a.grid = grid;
+  a.ctl = g->ctl;
+  cudaStream_t s = g->stream;
+  MG_CUDA_TRY(cudaMemsetAsync(a.hcount, 0, sizeof(int32_t) * std::max<int64_t>(nheavy, 1), s));
+  if (!weighted) {
+    outdeg_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, n, srow);
+  } else {
+    const PrbArgs rp = prb_args_of(g, *rbins, true, (const float *)g->vals);
+    rowsum_binned_kernel<<<g->num_sms * 8, PRB_NT, 0, s>>>(rp, srow);
+  }
+  MG_CUDA_TRY(cudaGetLastError());
+  mg_stats total;
+  std::memset(&total, 0, sizeof(total));
+  const dim3 tblk(32, 8), tgrid((unsigned)((n + 31) / 32), (unsigned)(W / 32));
+  for (int32_t c0 = 0; c0 < nvec; c0 += PPR_MAXW) {
+    const int32_t k = std::min<int32_t>(PPR_MAXW, nvec - c0);
+    MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+    ppr_pack_kernel<<<tgrid, tblk, 0, s>>>(tele_dev ? tele_dev + (size_t)c0 * n : nullptr, k, n, W, tele);
+    MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+    switch (vpl) {
+      case 1: ppr_launch_init<1>(a, ginit, s); break;
+      case 2: ppr_launch_init<2>(a, ginit, s); break;
+      case 4: ppr_launch_init<4>(a, ginit, s); break;
+      default: ppr_launch_init<8>(a, ginit, s); break;
+    }
+    ppr_init_reduce_kernel<<<1, 256, 0, s>>>(a, ginit);
+    MG_CUDA_TRY(cudaGetLastError());
+    struct Sig {
+      PprArgs a;
+      int vpl, w;
+    } sig;
+    std::memset(&sig, 0, sizeof(sig));
+    sig.a = a;
+    sig.vpl = vpl;
+    sig.w = weighted;
+    LoopBody body = [a, vpl, weighted](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+      PprArgs b = a;
+      b.h = h;
+      b.use_cond = use_cond;
+      switch (vpl * 2 + (weighted ? 1 : 0)) {
+        case 2: ppr_launch_iter<1, false>(b, st); break;
+        case 3: ppr_launch_iter<1, true>(b, st); break;
+        case 4: ppr_launch_iter<2, false>(b, st); break;
+        case 5: ppr_launch_iter<2, true>(b, st); break;
+        case 8: ppr_launch_iter<4, false>(b, st); break;
+        case 9: ppr_launch_iter<4, true>(b, st); break;
+        case 16: ppr_launch_iter<8, false>(b, st); break;
+        default: ppr_launch_iter<8, true>(b, st); break;
+      }
+    };
+    MG_TRY(run_loop(g, SLOT_PPR, &sig, sizeof(sig), o.use_graph >= 0, body, (int64_t)a.max_iter + 2));
+    MG_TRY(fetch_ctl(g));
+    const DevCtl &hc = *g->ctl_host;
+    const float *res = hc.cur ? a.x1 : a.x0;
+    float *dst = out_is_device ? ranks_out + (size_t)c0 * n : stage;
+    ppr_unpack_kernel<<<tgrid, tblk, 0, s>>>(res, k, n, W, dst);
+    MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+    MG_CUDA_TRY(cudaGetLastError());
+    if (!out_is_device)
+      MG_CUDA_TRY(cudaMemcpyAsync(ranks_out + (size_t)c0 * n, stage, sizeof(float) * (size_t)k * n,
+                                  cudaMemcpyDeviceToHost, s));
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hc.status != 0) {
+      mg_set_error("mg_pagerank: device status %d", hc.status);
+      return (mg_status)hc.status;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    total.kernel_ms += ms;
+    total.iterations = std::max<int64_t>(total.iterations, hc.level);
+    total.edges_traversed += g->m * hc.level * k;
+    total.edges_inspected += g->m * hc.level;
+    total.residual = std::max(total.residual, hc.dsum[0]);
+    // per iteration: offsets, indices (+ weights), W-wide rows gathered per edge,
+    // and x read, x, g written and t read per vertex
+    total.bytes_compulsory += hc.level * (4 * (n + 1) + (weighted ? 8 : 4) * g->m + (int64_t)4 * W * g->m +
+                                          (int64_t)16 * W * n);
+    total.launches += 5 + (o.use_graph >= 0 ? 2 * (int64_t)hc.body_iters : (int64_t)hc.level);
+  }
+  if (stats) *stats = total;
+  return MG_OK;
+}
+
 extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nvec, float *ranks,
                                  const mg_pr_opts *opts, mg_stats *stats) {
   if (!g || !ranks || nvec <= 0) {
@@ -1001,6 +1180,7 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
       MG_CUDA_TRY(cudaMemcpyAsync(tele_dev, teleport, sizeof(float) * n * nvec, cudaMemcpyHostToDevice, g->stream));
     }
   }
+  if (nvec > 1) return pagerank_ppr(g, tele_dev, nvec, ranks, o.device_output, o, stats);
   mg_stats total;
   std::memset(&total, 0, sizeof(total));
   for (int32_t k = 0; k < nvec; k++) {

@@ -17,6 +17,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -37,6 +38,8 @@ struct SsspArgs {
   int32_t both;
   int64_t n;
   int32_t *big_v;  // grid-strided bin (BIG_CAP entries)
+  int32_t vmask;   // item -> vertex mask: -1 for one instance; batched runs keep the
+                   // instance number in the bits above it (item = instance << s | v)
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
@@ -48,6 +51,7 @@ struct RelaxCtx {
   const int32_t *ro;
   int32_t *qout, *qlen_out, *overflow;
   int32_t qcap;
+  int32_t vmask;
   int64_t reach_deg;  // out-degrees of vertices reached for the first time
   int64_t updates;
 };
@@ -61,7 +65,7 @@ __device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t
     const int32_t old = atomicMin(x.dist + u, nd);
     if (nd < old) {
       x.updates++;
-      if (old == INT_MAX) x.reach_deg += x.ro[u + 1] - x.ro[u];
+      if (old == INT_MAX) x.reach_deg += x.ro[(u & x.vmask) + 1] - x.ro[u & x.vmask];
       const uint32_t bit = 1u << (u & 31);
       push = !(atomicOr(x.inq_next + (u >> 5), bit) & bit);
     }
@@ -101,7 +105,9 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   const int32_t nin = vload(&c->qlen[cur]);
   const int32_t *qin = cur ? a.q1 : a.q0;
   uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
-  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, 0, 0};
+  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, a.vmask,
+             0, 0};
+  const int32_t hi = ~a.vmask;  // instance bits of an item
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
   const BigList big{a.big_v, &c->big_len};
@@ -115,12 +121,12 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
       nexp++;
     }
     expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) {
-      relax(x, sv, ci[k], w ? w[k] : 1);
-    }, &big);
+      relax(x, sv, (sv & hi) | ci[k], w ? w[k] : 1);
+    }, &big, a.vmask);
     if (a.both)
       expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) {
-        relax(x, sv, ri[k], cw ? cw[k] : 1);
-      });
+        relax(x, sv, (sv & hi) | ri[k], cw ? cw[k] : 1);
+      }, nullptr, a.vmask);
   }
   const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
   const int64_t b1 = block_sum<SSSP_NT>(insp, s_sum);
@@ -144,10 +150,12 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
     return;
   }
   const int cur = vload(&c->cur);
-  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, 0, 0};
+  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, a.vmask,
+             0, 0};
+  const int32_t hi = ~a.vmask;  // instance bits of an item
   const int32_t *ci = a.ci, *w = a.w;
   expand_big<SSSP_NT>(sm, a.ro, BigList{a.big_v, &c->big_len},
-                      [&](int32_t sv, int32_t k) { relax(x, sv, ci[k], w ? w[k] : 1); });
+                      [&](int32_t sv, int32_t k) { relax(x, sv, (sv & hi) | ci[k], w ? w[k] : 1); }, a.vmask);
   const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
   const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
   if (threadIdx.x == 0) {
@@ -177,7 +185,7 @@ __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, 
     const uint32_t bit = 1u << (s & 31);
     if (!(atomicOr(&a.inq0[s >> 5], bit) & bit)) {
       a.dist[s] = 0;
-      deg += a.ro[s + 1] - a.ro[s];
+      deg += a.ro[(s & a.vmask) + 1] - a.ro[s & a.vmask];
       const int pos = atomicAdd(&c->qlen[0], 1);
       if (pos < a.qcap) a.q0[pos] = s;
       else c->overflow = 1;
@@ -216,38 +224,47 @@ static mg_status check_weights_nonnegative(mg_graph *g) {
   return MG_OK;
 }
 
-// Runs a (multi-source) SSSP into `dist` (device, n entries).
-static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts &o,
-                          mg_stats *stats) {
-  using namespace mg;
+// Checks what every SSSP call needs from the graph and the options.
+static mg_status sssp_check(mg_graph *g, const int32_t *srcs, int32_t nsrc, const mg_opts &o, const char *who) {
   for (int32_t i = 0; i < nsrc; i++) {
     if (srcs[i] < 0 || srcs[i] >= g->n) {
-      mg_set_error("mg_sssp: source %d out of range [0, %lld)", srcs[i], (long long)g->n);
+      mg_set_error("%s: source %d out of range [0, %lld)", who, srcs[i], (long long)g->n);
       return MG_ERR_ARG;
     }
   }
   if (g->vtype == MG_DTYPE_F32) {
-    mg_set_error("mg_sssp: float edge values are not supported (int32 distances)");
+    mg_set_error("%s: float edge values are not supported (int32 distances)", who);
     return MG_ERR_UNSUPPORTED;
   }
   const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
-  const bool both = o.directed == 0 && !symmetric;
-  if (both && !g->has_csc) {
-    mg_set_error("mg_sssp: directed=0 needs the CSC");
+  if (o.directed == 0 && !symmetric && !g->has_csc) {
+    mg_set_error("%s: directed=0 needs the CSC", who);
     return MG_ERR_UNSUPPORTED;
   }
   MG_TRY(check_weights_nonnegative(g));
   if (g->vtype == MG_DTYPE_I32 && g->min_weight < 0) {
-    mg_set_error("mg_sssp: negative edge weight %d", g->min_weight);
+    mg_set_error("%s: negative edge weight %d", who, g->min_weight);
     return MG_ERR_ARG;
   }
+  return MG_OK;
+}
+
+// Runs SSSP over `nitems` frontier items into `dist` (device, nitems entries),
+// seeded from the items `seeds`. One instance: items are vertices (vmask -1).
+// Batched: item = instance << s | vertex with vmask = 2^s - 1, so every instance
+// relaxes its own copy of the distances over the shared CSR.
+static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int32_t *dist, int64_t nitems,
+                           int32_t vmask, const mg_opts &o, mg_stats *stats) {
+  using namespace mg;
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  const bool both = o.directed == 0 && !symmetric;
   const int64_t n = g->n;
-  int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)n) : n;
-  const int32_t qcap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(qcap64, n));
-  const int64_t nwords = (n + 31) / 32;
+  int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)nitems) : nitems;
+  const int32_t qcap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(qcap64, nitems));
+  const int64_t nwords = (nitems + 31) / 32;
   const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
-                                   sizeof(int32_t) * (size_t)nsrc, sizeof(int32_t) * (size_t)BIG_CAP});
+                                   sizeof(int32_t) * (size_t)nseed, sizeof(int32_t) * (size_t)BIG_CAP});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   SsspArgs a;
@@ -255,7 +272,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
   a.inq1 = cv.take<uint32_t>(nwords);
   a.q0 = cv.take<int32_t>(qcap);
   a.q1 = cv.take<int32_t>(qcap);
-  int32_t *dsrc = cv.take<int32_t>(nsrc);
+  int32_t *dsrc = cv.take<int32_t>(nseed);
   a.big_v = cv.take<int32_t>(BIG_CAP);
   a.ro = g->ro;
   a.ci = g->ci;
@@ -266,17 +283,19 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
   a.dist = dist;
   a.qcap = qcap;
   a.both = both ? 1 : 0;
-  a.n = n;
+  a.n = nitems;
+  a.vmask = vmask;
   a.ctl = g->ctl;
   a.h = 0;
   a.use_cond = 0;
   cudaStream_t s = g->stream;
+  // Bellman-Ford rounds of every instance are bounded by its vertex count.
   const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
-  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, seeds, sizeof(int32_t) * nseed, cudaMemcpyHostToDevice, s));
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
-  sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, n);
-  sssp_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap);
+  sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, nitems);
+  sssp_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nseed, iter_cap);
   MG_CUDA_TRY(cudaGetLastError());
   const int grid = g->num_sms * 4;
   struct Sig {
@@ -293,7 +312,7 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
     sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
     sssp_relax_big_kernel<<<grid, SSSP_NT, 0, st>>>(b);
   };
-  MG_TRY(run_loop(g, SLOT_SSSP, &sig, sizeof(sig), o.use_graph >= 0, body, (int64_t)n + 2));
+  MG_TRY(run_loop(g, vmask == -1 ? SLOT_SSSP : SLOT_BSSSP, &sig, sizeof(sig), o.use_graph >= 0, body, n + 2));
   MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
   MG_TRY(fetch_ctl(g));
   const DevCtl &hc = *g->ctl_host;
@@ -315,6 +334,13 @@ static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_
   return MG_OK;
 }
 
+// Runs a (multi-source) SSSP into `dist` (device, n entries).
+static mg_status sssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts &o,
+                          mg_stats *stats) {
+  MG_TRY(sssp_check(g, srcs, nsrc, o, "mg_sssp"));
+  return sssp_core(g, srcs, nsrc, dist, g->n, -1, o, stats);
+}
+
 extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts *opts,
                              mg_stats *stats) {
   if (!g || !srcs || nsrc <= 0 || !dist) {
@@ -334,6 +360,52 @@ extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int
   MG_TRY(sssp_run(g, srcs, nsrc, out, o, stats));
   if (!o.device_output) {
     MG_TRY(copy_out(g, dist, out, sizeof(int32_t) * g->n, 0));
+    MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
+  return MG_OK;
+}
+
+// nsrc independent single-source runs in one device run (no reference
+// counterpart; the reference loops the engine per source,
+// Algorithms/BFS/bfs.cu:442-456). Instance i relaxes items i << s | v, with
+// 2^s >= n; the distance rows are then packed to nsrc x n.
+extern "C" mg_status mg_sssp_batch(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist,
+                                   const mg_opts *opts, mg_stats *stats) {
+  if (!g || !srcs || nsrc <= 0 || !dist) {
+    mg_set_error("mg_sssp_batch: null argument or nsrc <= 0");
+    return MG_ERR_ARG;
+  }
+  mg_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.directed = 1;
+  if (opts) o = *opts;
+  MG_TRY(graph_enter(g));
+  MG_TRY(sssp_check(g, srcs, nsrc, o, "mg_sssp_batch"));
+  const int64_t n = g->n;
+  int shift = 0;
+  while ((int64_t(1) << shift) < n) shift++;
+  const int64_t stride = int64_t(1) << shift;
+  if (n == 0 || (int64_t)nsrc * stride > (int64_t)INT_MAX) {
+    mg_set_error("mg_sssp_batch: %d instances of %lld (padded to %lld) vertices exceed 2^31 frontier items; "
+                 "split the sources", nsrc, (long long)n, (long long)stride);
+    return MG_ERR_ARG;
+  }
+  const int64_t nitems = (int64_t)nsrc * stride;
+  std::vector<int32_t> seeds(nsrc);
+  for (int32_t i = 0; i < nsrc; i++) seeds[i] = (int32_t)(((int64_t)i << shift) | srcs[i]);
+  // Distances are computed into a padded buffer unless the rows are already dense
+  // and the output is on the device.
+  const bool direct = stride == n && o.device_output;
+  int32_t *work = dist;
+  if (!direct) {
+    MG_TRY(ws_reserve(g->ws_out, sizeof(int32_t) * (size_t)nitems + 256));
+    work = (int32_t *)g->ws_out.ptr;
+  }
+  MG_TRY(sssp_core(g, seeds.data(), nsrc, work, nitems, (int32_t)(stride - 1), o, stats));
+  if (!direct) {
+    MG_CUDA_TRY(cudaMemcpy2DAsync(dist, sizeof(int32_t) * n, work, sizeof(int32_t) * stride, sizeof(int32_t) * n,
+                                  nsrc, o.device_output ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  g->stream));
     MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
   }
   return MG_OK;
