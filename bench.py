@@ -53,6 +53,10 @@ def parse():
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-versus-looped section")
+    p.add_argument("--batched-scale", type=int, default=20)
+    p.add_argument("--no-extra", action="store_true",
+                   help="skip the lattice (BFS/SSSP) and weighted PageRank forward + adjoint sections")
     p.add_argument("--host-loop", action="store_true",
                    help="drive iterations from the host instead of a CUDA-graph WHILE node (for profilers "
                         "that cannot see kernels inside conditional graphs)")
@@ -91,7 +95,7 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -121,6 +125,147 @@ class Clocks:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def batched_section(scale, torch, mg):
+    """Batched workload against looping the plain engine once per instance, on
+    the same GPU: 64 BFS and 64 SSSP sources (half top-1% degree, half median
+    degree), 256 personalised PageRank vectors (supports of U{1..32} vertices)
+    on R-MAT `scale` ef16 symmetrised with weights U{1..255}, and a ragged batch
+    of 32 R-MAT graphs of scale U{10..18} (ef 8), one BFS from vertex 0 each.
+    Device time from the engine's CUDA events; TEPS edges per instance as in the
+    plain runs (PPR: m x iterations per vector)."""
+    h = mg.gen_rmat(scale, 16, SEED + 7, symmetrize=True, weights="int", p0=1, p1=255)
+    n = h.n
+    g = mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True)
+    srcs = mg.mixed_degree_sources(h.row_offsets, 64, SEED + 8)
+    out = torch.empty(64 * n, dtype=torch.int32, device="cuda")
+    one = torch.empty(n, dtype=torch.int32, device="cuda")
+    res = {}
+
+    def pair(name, batched, looped, reps=2):
+        for _ in range(reps):
+            eb, tb = batched()
+        el, tl = looped()
+        res[name] = {"batched_gteps": eb / tb / 1e6, "looped_gteps": el / tl / 1e6, "batched_ms": tb,
+                     "looped_ms": tl, "speedup_gteps": (eb / tb) / (el / tl), "speedup_time": tl / tb}
+        return eb, tb, el, tl
+
+    def bfs_b():
+        _, st = g.bfs_batch(srcs, out=out)
+        return st["edges_traversed"], st["kernel_ms"]
+
+    def bfs_l():
+        e = t = 0.0
+        for s_ in srcs:
+            _, st = g.bfs([int(s_)], out=one)
+            e += st["edges_traversed"]
+            t += st["kernel_ms"]
+        return e, t
+
+    def sssp_b():
+        _, st = g.sssp_batch(srcs, out=out)
+        return st["edges_traversed"], st["kernel_ms"]
+
+    def sssp_l():
+        e = t = 0.0
+        for s_ in srcs:
+            _, st = g.sssp([int(s_)], out=one)
+            e += st["edges_traversed"]
+            t += st["kernel_ms"]
+        return e, t
+
+    tele = torch.from_numpy(mg.sparse_teleports(n, 256, SEED + 9).reshape(-1)).cuda()
+    pout = torch.empty(256 * n, dtype=torch.float32, device="cuda")
+    pone = torch.empty(n, dtype=torch.float32, device="cuda")
+
+    def ppr_b():
+        _, st = g.pagerank(teleport=tele, nvec=256, out=pout, mode="normalized", alpha=ALPHA, tol=PR_TOL,
+                           max_iter=PR_MAX_IT)
+        return st["edges_traversed"], st["kernel_ms"]
+
+    def ppr_l():
+        e = t = 0.0
+        for k in range(256):
+            _, st = g.pagerank(teleport=tele[k * n:(k + 1) * n], out=pone, mode="normalized", alpha=ALPHA,
+                               tol=PR_TOL, max_iter=PR_MAX_IT)
+            e += st["edges_traversed"]
+            t += st["kernel_ms"]
+        return e, t
+
+    tot = [0.0, 0.0, 0.0, 0.0]
+    for name, b, l_ in (("bfs_64", bfs_b, bfs_l), ("sssp_64", sssp_b, sssp_l), ("ppr_256", ppr_b, ppr_l)):
+        r = pair(name, b, l_)
+        tot = [x + y for x, y in zip(tot, r)]
+    g.close()
+    rng = np.random.default_rng(SEED + 10)
+    members = [mg.gen_rmat(int(sc), 8, SEED + 100 + i, symmetrize=True) for i, sc in enumerate(rng.integers(10, 19, 32))]
+    gr = mg.Graph.ragged(members, symmetric=True)
+    singles = [mg.Graph(m_.row_offsets, m_.col_idx, symmetric=True) for m_ in members]
+
+    def rag_b():
+        _, st = gr.bfs_ragged(np.zeros(32, dtype=np.int32))
+        return st["edges_traversed"], st["kernel_ms"]
+
+    def rag_l():
+        e = t = 0.0
+        for gm in singles:
+            _, st = gm.bfs([0])
+            e += st["edges_traversed"]
+            t += st["kernel_ms"]
+        return e, t
+
+    r = pair("ragged_bfs_32", rag_b, rag_l)
+    tot = [x + y for x, y in zip(tot, r)]
+    gr.close()
+    for gm in singles:
+        gm.close()
+    res["aggregate"] = {"batched_gteps": tot[0] / tot[1] / 1e6, "looped_gteps": tot[2] / tot[3] / 1e6,
+                        "speedup_gteps": (tot[0] / tot[1]) / (tot[2] / tot[3])}
+    res["config"] = (f"R-MAT s{scale} ef16 sym (n={n}, m={h.m}), weights U{{1..255}}; 64 BFS + 64 SSSP sources "
+                     "(32 top-1% degree, 32 median); 256 PPR vectors (support U{1..32}); 32 ragged R-MAT graphs "
+                     "scale U{10..18} ef8, BFS from 0; looped = one plain engine call per instance")
+    return res
+
+
+def lattice_section(torch, mg, side=4096):
+    """High-diameter workload: side x side 4-neighbour lattice (id = r * side + c)
+    plus 0.1% uniform long-range pairs, every edge both ways, weights U{1..1000};
+    BFS and SSSP from the corner vertex 0 (device time, CUDA events)."""
+    h = mg.gen_lattice(side, side, 0.001, SEED + 11, weights="int", p0=1, p1=1000)
+    g = mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True)
+    out = torch.empty(h.n, dtype=torch.int32, device="cuda")
+    res = {"config": f"lattice {side}x{side} + 0.1% long-range (n={h.n}, m={h.m}), weights U{{1..1000}}, src 0"}
+    for name, fn in (("bfs", g.bfs), ("sssp", g.sssp)):
+        for _ in range(2):
+            _, st = fn([0], out=out)
+        res[name] = {"gteps": st["edges_traversed"] / st["kernel_ms"] / 1e6, "ms": st["kernel_ms"],
+                     "iterations": st["iterations"], "launches": st["launches"]}
+    g.close()
+    return res
+
+
+def adjoint_section(torch, mg, scale=24):
+    """Weighted PageRank forward + adjoint: R-MAT `scale` ef16 directed, weights
+    lognormal(0, 1) (normalised by their row sums), alpha 0.85, forward to L1 <
+    1e-6; backward of L = w . x with w ~ N(0, 1) to relative tolerance 1e-7."""
+    h = mg.gen_rmat(scale, 16, SEED + 12, symmetrize=False, weights="lognormal", p0=0, p1=1)
+    n, m = h.n, h.m
+    g = mg.Graph(h.row_offsets, h.col_idx, h.weights_f32)
+    x = torch.empty(n, dtype=torch.float32, device="cuda")
+    wv = torch.from_numpy(np.random.default_rng(SEED + 13).standard_normal(n).astype(np.float32)).cuda()
+    gw = torch.empty(m, dtype=torch.float32, device="cuda")
+    gt = torch.empty(n, dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        _, sf = g.pagerank(mode="normalized", weighted=True, alpha=ALPHA, tol=PR_TOL, max_iter=200, out=x)
+        _, _, sb = g.pagerank_backward(x, wv, weighted=True, alpha=ALPHA, tol=1e-7, max_iter=200,
+                                       out_weights=gw, out_teleport=gt)
+    g.close()
+    return {"config": f"R-MAT s{scale} ef16 directed (n={n}, m={m}), lognormal(0,1) weights, alpha {ALPHA}",
+            "forward": {"ms": sf["kernel_ms"], "iterations": sf["iterations"],
+                        "gteps": m * sf["iterations"] / sf["kernel_ms"] / 1e6},
+            "backward": {"ms": sb["kernel_ms"], "iterations": sb["iterations"],
+                         "gteps": m * sb["iterations"] / sb["kernel_ms"] / 1e6}}
 
 
 def cpu_reference_run(h, src):
@@ -280,8 +425,9 @@ def run_ours(args):
         sssp_edges += st["edges_traversed"]
         sssp_ms += t
 
-    # Roofline of the dominant kernel: solve_binned_kernel, one launch per PageRank
-    # iteration (degree-binned CSC gather + row update + residual). Algorithmic
+    # Roofline of the dominant kernel: solve_binned_hub_kernel, one launch per
+    # PageRank iteration (degree-binned CSC gather with the shared-memory column
+    # cache + row update + residual). Algorithmic
     # bytes per launch = offsets 4(n+1) + indices 4m + read x 4n + write x 4n +
     # write x/s 4n. Its duration is the PageRank call's device time divided by the
     # iterations (the call also holds two init kernels, so this slightly
@@ -293,7 +439,7 @@ def run_ours(args):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        t = tj.get("solve_binned_kernel", {})
+        t = tj.get("solve_binned_hub_kernel", {})
         if t.get("scale") == args.scale:
             traffic = t.get("dram_bytes_per_launch")
     except Exception:
@@ -336,7 +482,7 @@ def run_ours(args):
                    "scale": args.scale, "edge_factor": args.edge_factor, "n": n, "m": m,
                    "l2": "256 MiB buffer written between steps; graph (CSR 537 MB) larger than L2",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "solve_binned_kernel (one PageRank iteration)",
+        "roofline": {"bound": "hbm", "kernel": "solve_binned_hub_kernel (one PageRank iteration)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": pr_bytes_iter},
@@ -364,6 +510,17 @@ def run_ours(args):
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
     g.close()
+    if not args.no_batched:
+        try:
+            line["batched"] = batched_section(args.batched_scale, torch, mg)
+        except Exception as e:
+            line["batched"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if not args.no_extra:
+        for key, fn in (("lattice", lattice_section), ("pagerank_adjoint", adjoint_section)):
+            try:
+                line[key] = fn(torch, mg)
+            except Exception as e:
+                line[key] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -73,7 +73,10 @@ typedef struct mg_opts {
   int32_t threshold;     /* reference "threshold": accepted for compatibility; strategy is chosen on the device */
   int32_t use_graph;     /* 1 (default when 0): run the iteration loop as a CUDA graph with a device-side while node;
                             -1: host-driven loop (one frontier-size read per iteration) */
-  int32_t reserved[4];
+  int32_t delta;         /* SSSP only: > 0 runs the near-far schedule with this bucket width (int32 weights,
+                            iter_num unbounded); <= 0 (default) plain frontier Bellman-Ford, whose rounds are
+                            the reference's, so an iteration cap keeps its meaning */
+  int32_t reserved[3];
 } mg_opts;
 
 /* Counters returned by every compute call (may be NULL). */
@@ -101,8 +104,10 @@ typedef struct mg_pr_opts {
   int32_t compensated;   /* 1: two-sum compensated FP32 accumulation [1]; -1 plain FP32 sums */
   int32_t device_output; /* 1: ranks/teleport/gradient arrays are device pointers */
   int32_t use_graph;     /* as mg_opts.use_graph */
-  int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps [default],
-                            1 merge-path tiles staged in shared memory by TMA bulk copies */
+  int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps, with the
+                              most-gathered columns cached in shared memory in the forward
+                              solve [default]; 1 merge-path tiles staged in shared memory by
+                              TMA bulk copies; 2 degree-binned without the column cache */
   int32_t reserved[2];
 } mg_pr_opts;
 

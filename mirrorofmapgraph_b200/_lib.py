@@ -32,7 +32,7 @@ MG_BFS_NOALLOC_MAX_SOURCES = 1024
 class MgOpts(C.Structure):
     _fields_ = [("directed", C.c_int32), ("iter_num", C.c_int32), ("direction", C.c_int32),
                 ("device_output", C.c_int32), ("queue_sizing", C.c_double), ("threshold", C.c_int32),
-                ("use_graph", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("use_graph", C.c_int32), ("delta", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class MgStats(C.Structure):

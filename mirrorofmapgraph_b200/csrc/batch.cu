@@ -105,7 +105,7 @@ __device__ __forceinline__ void ms_write_depths(int32_t *depth, int64_t n, int64
 
 // Top-down expansion of the union frontier into the accumulators.
 __global__ void __launch_bounds__(MS_NT) ms_push_kernel(MsArgs a) {
-  __shared__ ExpandSmem<MS_NT> sm;
+  __shared__ ExpandSmem<MS_NT, uint64_t> sm;
   __shared__ int64_t s_sum[MS_NT / 32 + 1];
   if (ms_skip(a, 0)) return;
   DevCtl *c = a.ctl;
@@ -118,16 +118,20 @@ __global__ void __launch_bounds__(MS_NT) ms_push_kernel(MsArgs a) {
   const int32_t *ci = a.ci, *ri = a.ri;
   int64_t insp = 0, nexp = 0;
   const BigList big{a.big_v, &c->big_len};
-  auto visit_to = [&](int32_t sv, int32_t w) {
-    const uint64_t add = __ldg(fcur + sv) & ~__ldg(seen + w);
+  auto visit_to = [&](uint64_t f, int32_t w) {
+    const uint64_t add = f & ~__ldg(seen + w);
     if (add) atomicOr(acc + w, (unsigned long long)add);
   };
   for (int64_t tile = (int64_t)blockIdx.x * MS_NT; tile < nin; tile += (int64_t)gridDim.x * MS_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
     nexp += v >= 0;
-    expand_tile<MS_NT, MS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) { visit_to(sv, ci[k]); }, &big);
-    if (a.both) expand_tile<MS_NT, MS_CTA_TH>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) { visit_to(sv, ri[k]); });
+    const uint64_t f = v >= 0 ? __ldg(fcur + v) : 0;  // the sender's frontier mask, once per vertex
+    expand_tile_p<MS_NT, MS_CTA_TH>(sm, a.ro, v, f, insp,
+                                    [&](int32_t, uint64_t fv, int32_t k) { visit_to(fv, ci[k]); }, &big);
+    if (a.both)
+      expand_tile_p<MS_NT, MS_CTA_TH>(sm, a.co, v, f, insp,
+                                      [&](int32_t, uint64_t fv, int32_t k) { visit_to(fv, ri[k]); });
   }
   const int64_t bins = block_sum<MS_NT>(insp, s_sum);
   const int64_t bexp = block_sum<MS_NT>(nexp, s_sum);

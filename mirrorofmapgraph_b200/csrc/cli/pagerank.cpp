@@ -23,8 +23,10 @@ int main(int argc, char **argv) {
   o.directed = (int32_t)cfg.getInt("directed");
   const int64_t it = cfg.getInt("iter_num");
   o.max_iter = it >= INT32_MAX ? 0 : (int32_t)it;
-  o.alpha = cfg.getDouble("alpha");
-  o.tol = cfg.getDouble("pr_tol");
+  if (o.mode == MG_PR_NORMALIZED) {  // REFCOMPAT keeps the reference's 0.01 delta frontier
+    o.alpha = cfg.getDouble("alpha");
+    o.tol = cfg.getDouble("pr_tol");
+  }
   std::vector<float> rank(h.n);
   mg_stats st;
   mgcli::check(mg_pagerank(g, nullptr, 1, rank.data(), &o, &st), "mg_pagerank");

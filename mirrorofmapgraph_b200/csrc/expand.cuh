@@ -18,26 +18,33 @@
 
 namespace mg {
 
-template <int NT>
+// P: the type of a per-vertex payload handed to visit() beside the vertex (for
+// example the vertex's distance or frontier mask, read once per vertex instead of
+// once per edge).
+template <int NT, typename P = int32_t>
 struct ExpandSmem {
   int32_t scan[NT];
   int32_t beg[NT];
   int32_t vtx[NT];
+  P pay[NT];
   int32_t red[NT / 32 + 1];
   int32_t cta[4];
+  P cpay;
 };
 
 struct BigList;
 __device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t deg);
 
+// visit(v, payload, k) for every edge k of the tile's vertices; each thread brings
+// its vertex v (or -1) and that vertex's payload.
 //
 // `vmask` maps a frontier item to the vertex whose offsets it uses (item & vmask);
 // -1 (every bit) is the identity. Batched runs pack an instance number into the
 // item's high bits and pass the low-bit mask.
-template <int NT, int CTA_TH, typename Visit>
-__device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *__restrict__ off, int32_t v,
-                                            int64_t &insp, Visit &&visit, const BigList *big = nullptr,
-                                            int32_t vmask = -1) {
+template <int NT, int CTA_TH, typename P, typename Visit>
+__device__ __forceinline__ void expand_tile_p(ExpandSmem<NT, P> &sm, const int32_t *__restrict__ off, int32_t v,
+                                              P pay, int64_t &insp, Visit &&visit, const BigList *big = nullptr,
+                                              int32_t vmask = -1) {
   const int tid = threadIdx.x, lane = lane_id();
   int32_t beg = 0, deg = 0;
   if (v >= 0) {
@@ -55,11 +62,13 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
       sm.cta[1] = beg;
       sm.cta[2] = beg + deg;
       sm.cta[3] = v;
+      sm.cpay = pay;
       deg = 0;
     }
     __syncthreads();
     const int32_t b = sm.cta[1], e = sm.cta[2], cv = sm.cta[3];
-    for (int32_t k = b + tid; k < e; k += NT) visit(cv, k);
+    const P cp = sm.cpay;
+    for (int32_t k = b + tid; k < e; k += NT) visit(cv, cp, k);
   }
   // Warp bin.
   for (;;) {
@@ -68,8 +77,9 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
     const int l = __ffs(wm) - 1;
     const int32_t b = __shfl_sync(FULL, beg, l), e = __shfl_sync(FULL, beg + deg, l);
     const int32_t wv = __shfl_sync(FULL, v, l);
+    const P wp = __shfl_sync(FULL, pay, l);
     if (lane == l) deg = 0;
-    for (int32_t k = b + lane; k < e; k += 32) visit(wv, k);
+    for (int32_t k = b + lane; k < e; k += 32) visit(wv, wp, k);
   }
   // Thread bin.
   int32_t total;
@@ -77,6 +87,7 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
   sm.scan[tid] = ex;
   sm.beg[tid] = beg;
   sm.vtx[tid] = v;
+  sm.pay[tid] = pay;
   __syncthreads();
   for (int32_t k = tid; k < total; k += NT) {
     int lo = 0, hi = NT;
@@ -85,9 +96,18 @@ __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *_
       if (sm.scan[mid] <= k) lo = mid;
       else hi = mid;
     }
-    visit(sm.vtx[lo], sm.beg[lo] + (k - sm.scan[lo]));
+    visit(sm.vtx[lo], sm.pay[lo], sm.beg[lo] + (k - sm.scan[lo]));
   }
   __syncthreads();
+}
+
+// expand_tile_p without a payload: visit(v, k).
+template <int NT, int CTA_TH, typename Visit>
+__device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *__restrict__ off, int32_t v,
+                                            int64_t &insp, Visit &&visit, const BigList *big = nullptr,
+                                            int32_t vmask = -1) {
+  expand_tile_p<NT, CTA_TH>(sm, off, v, (int32_t)0, insp, [&](int32_t sv, int32_t, int32_t k) { visit(sv, k); },
+                            big, vmask);
 }
 
 template <typename T>

@@ -54,6 +54,15 @@ struct DevCtl {
   int32_t overflow;          // set by a kernel whose frontier append ran past capacity
   int32_t body_iters;        // WHILE-body executions so far (loop guard)
   int32_t big_len;           // vertices deferred to the grid-strided bin this level
+  // SSSP near-far: vertices at distance >= thr wait in a far pile (ping-pong
+  // far_cur) until the near frontier runs dry; then the pile is split at a new
+  // threshold (split set between the relaxation and split kernels).
+  int64_t thr;
+  int32_t far_len[2];
+  int32_t far_cur;
+  int32_t split;
+  int32_t far_min;
+  int32_t splits;
 };
 
 // Padding of the device graph arrays. Offsets arrays hold n + 1 + MG_OFF_PAD
@@ -86,6 +95,7 @@ struct mg_graph {
   // cached checks of the edge values
   bool weights_checked = false;
   int32_t min_weight = 0;
+  double mean_weight = 0.0;
   // ragged batch
   std::vector<int64_t> vbase;
   // workspaces: ws_main per-run state, ws_aux graph build scratch, ws_out staged

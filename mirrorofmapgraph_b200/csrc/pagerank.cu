@@ -22,6 +22,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -39,10 +40,23 @@ struct GatherPlan {
   int32_t *tx = nullptr, *ty = nullptr;
 };
 
+// Shared-memory cache of the most gathered columns (forward gather over the
+// CSC): the K vertices of largest out-degree get slots 0..K-1; cidx is the CSC
+// index array with each cached column replaced by (slot | 0x80000000), so the
+// gather reads those values from shared memory.
+struct HubCache {
+  int32_t *cidx = nullptr;  // m + 8 entries
+  int32_t *slot = nullptr;  // n: slot of a vertex, -1 if not cached
+  int32_t *hv = nullptr;    // K: vertex of a slot
+  int32_t K = 0;
+  bool ok = false;
+};
+
 struct PlanSet {
   GatherPlan csc, csr;
   BinPlan bcsc, bcsr;
   bool bcsc_ok = false, bcsr_ok = false;
+  HubCache hubs;
 };
 
 }  // namespace mg
@@ -64,6 +78,8 @@ void pr_release_plans(mg_graph *g) {
                     (void *)b->hcontrib})
       if (q) cudaFree(q);
   }
+  for (void *q : {(void *)ps->hubs.cidx, (void *)ps->hubs.slot, (void *)ps->hubs.hv})
+    if (q) cudaFree(q);
   delete ps;
   g->plan_csc = nullptr;
 }
@@ -141,6 +157,11 @@ static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
   return MG_OK;
 }
 
+// Column cache of the forward gather (built once per graph): the vertices of
+// largest out-degree, at most `cap` of them, with every vertex of degree >= T
+// for the smallest T that fits.
+static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out);
+
 static mg::PrbArgs prb_args_of(const mg_graph *g, const mg::BinPlan &bp, bool csr, const float *wts) {
   mg::PrbArgs p;
   p.off = csr ? g->ro : g->co;
@@ -191,6 +212,9 @@ struct SolveArgs {
   int32_t adjoint;
   double *part1, *part2;      // per-CTA FP64 partials of the two kernels
   int32_t grid1, grid2;
+  const int32_t *hslot;       // shared-memory column cache: slot of each vertex (nullptr: no cache)
+  float *gh0, *gh1;           // cached columns' gathered values, ping-pong with g0/g1
+  int32_t nhub;               // cached columns
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
@@ -209,6 +233,7 @@ struct RowUpdate {
   float *vnew, *gnew;
   double scal;  // forward: dangling mass d of the current iterate; adjoint: t.lambda
   double resid = 0.0, red2 = 0.0;
+  float *ghnew = nullptr;  // forward with the column cache: its copy of gnew
 
   __device__ __forceinline__ void apply(int32_t r, Comp v, const RowIn &in) {
     const double acc = (double)v.hi + (double)v.lo;
@@ -216,10 +241,13 @@ struct RowUpdate {
     double nv;
     if (!a->adjoint) {
       nv = a->alpha * (acc + scal * in.t) + (1.0 - a->alpha) * in.t;
-      if (s > 0.0) gnew[r] = (float)(nv / s);
-      else {
-        gnew[r] = 0.f;
-        red2 += nv;
+      float gv = 0.f;
+      if (s > 0.0) gv = (float)(nv / s);
+      else red2 += nv;
+      gnew[r] = gv;
+      if (ghnew) {
+        const int32_t sl = __ldg(a->hslot + r);
+        if (sl >= 0) ghnew[sl] = gv;
       }
     } else {
       nv = (double)in.w + a->alpha * (s > 0.0 ? acc / s : scal);
@@ -296,6 +324,7 @@ __global__ void __launch_bounds__(PRG_NT) solve_gather_kernel(SolveArgs a) {
 
 // Last CTA of an iteration: fixed-order FP64 reduction of the per-CTA partials
 // (and of the hub contributions), then the convergence decision.
+template <int NT = PRG_NT>
 __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *hcontrib, int64_t nheavy,
                                     double *s_red) {
   DevCtl *c = a.ctl;
@@ -312,8 +341,8 @@ __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *h
     r += __ldcg(hcontrib + 2 * i);
     d += __ldcg(hcontrib + 2 * i + 1);
   }
-  r = block_sum<PRG_NT>(r, s_red);
-  d = block_sum<PRG_NT>(d, s_red);
+  r = block_sum<NT>(r, s_red);
+  d = block_sum<NT>(d, s_red);
   if (threadIdx.x == 0) {
     const int lvl = c->level + 1;
     c->level = lvl;
@@ -356,6 +385,111 @@ __global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) solve_binned_kernel(So
     a.part1[2 * blockIdx.x + 1] = d;
   }
   if (last_block(&c->blocks_done)) solve_iteration_end(a, cur, p.hcontrib, p.nheavy, s_red);
+}
+
+// One whole iteration of the degree-binned solver with the column cache: every
+// CTA first copies the cached columns' gathered values into shared memory.
+#ifndef PRB_HUB_THREADS
+#define PRB_HUB_THREADS 768
+#endif
+#ifndef PRB_HUB_MINB
+#define PRB_HUB_MINB 2
+#endif
+// Columns cached per CTA: the rest of the SM's shared memory stays L1 for the
+// uncached gathers (20480 columns = 80 KB per CTA measured best on R-MAT s22).
+#ifndef PRB_HUB_CAP
+#define PRB_HUB_CAP 20480
+#endif
+constexpr int PRB_HUB_NT = PRB_HUB_THREADS;
+
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_kernel(SolveArgs a, PrbArgs p) {
+  extern __shared__ __align__(16) float s_hub[];
+  __shared__ double s_red[PRB_HUB_NT / 32 + 1];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *vold = cur ? a.v1 : a.v0;
+  const float *__restrict__ gold = cur ? a.g1 : a.g0;
+  const float *ghold = cur ? a.gh1 : a.gh0;
+  float *vnew = cur ? a.v0 : a.v1, *gnew = cur ? a.g0 : a.g1, *ghnew = cur ? a.gh0 : a.gh1;
+  const int32_t nh4 = a.nhub >> 2;
+  for (int32_t i = threadIdx.x; i < nh4; i += PRB_HUB_NT)
+    reinterpret_cast<float4 *>(s_hub)[i] = __ldcg(reinterpret_cast<const float4 *>(ghold) + i);
+  for (int32_t i = 4 * nh4 + threadIdx.x; i < a.nhub; i += PRB_HUB_NT) s_hub[i] = __ldcg(ghold + i);
+  __syncthreads();
+  const double scal = vload(&c->dprev[1]);
+  RowUpdate up{&a, vold, vnew, gnew, scal};
+  up.ghnew = ghnew;
+  auto hub = [&](int64_t h, int32_t row, Comp v) {
+    RowUpdate hu{&a, vold, vnew, gnew, scal};
+    hu.ghnew = ghnew;
+    hu(row, v);
+    p.hcontrib[2 * h] = hu.resid;
+    p.hcontrib[2 * h + 1] = hu.red2;
+    __threadfence();
+  };
+  prb_run<WEIGHTED>(p, [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); }, up,
+                    hub);
+  const double r = block_sum<PRB_HUB_NT>(up.resid, s_red);
+  const double d = block_sum<PRB_HUB_NT>(up.red2, s_red);
+  if (threadIdx.x == 0) {
+    a.part1[2 * blockIdx.x] = r;
+    a.part1[2 * blockIdx.x + 1] = d;
+  }
+  if (last_block(&c->blocks_done)) solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.nheavy, s_red);
+}
+
+// Column-cache set-up kernels.
+// Out-degree histogram (bins 0..65535, the last one collecting every larger
+// degree): small degrees are counted in shared memory first, since most vertices
+// share a handful of small-degree bins.
+constexpr int HUB_SMEM_BINS = 4096;
+
+__global__ void __launch_bounds__(256) hub_hist_kernel(const int32_t *__restrict__ ro, int64_t n, unsigned *hist) {
+  __shared__ unsigned sh[HUB_SMEM_BINS];
+  for (int i = threadIdx.x; i < HUB_SMEM_BINS; i += 256) sh[i] = 0;
+  __syncthreads();
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = min(ro[v + 1] - ro[v], 65535);
+    if (d < HUB_SMEM_BINS) atomicAdd(sh + d, 1u);
+    else atomicAdd(hist + d, 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < HUB_SMEM_BINS; i += 256)
+    if (sh[i]) atomicAdd(hist + i, sh[i]);
+}
+
+__global__ void hub_slot_kernel(const int32_t *__restrict__ ro, int64_t n, int32_t thr, int32_t cap, int32_t *slot,
+                                int32_t *hv, unsigned *count) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    int32_t sl = -1;
+    if (ro[v + 1] - ro[v] >= thr) {
+      const unsigned t = atomicAdd(count, 1u);
+      if ((int32_t)t < cap) {
+        sl = (int32_t)t;
+        hv[sl] = (int32_t)v;
+      }
+    }
+    slot[v] = sl;
+  }
+}
+
+__global__ void hub_remap_kernel(const int32_t *__restrict__ ri, int64_t m, const int32_t *__restrict__ slot,
+                                 int32_t *cidx) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m + 8; k += (int64_t)gridDim.x * blockDim.x) {
+    if (k >= m) {
+      cidx[k] = 0;
+      continue;
+    }
+    const int32_t c = ri[k];
+    const int32_t sl = slot[c];
+    cidx[k] = sl >= 0 ? (int32_t)((uint32_t)sl | 0x80000000u) : c;
+  }
+}
+
+__global__ void hub_fill_kernel(const int32_t *__restrict__ hv, int32_t K, const float *__restrict__ g, float *gh) {
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) gh[i] = g[hv[i]];
 }
 
 struct RowSumStore {
@@ -493,7 +627,18 @@ struct SolvePlan {
   mg::PrbArgs p;        // degree-binned variant (default)
   bool weighted;
   bool use_tma;
+  bool use_hub;         // degree-binned with the shared-memory column cache
+  int32_t hub_bytes;    // its dynamic shared memory
 };
+
+template <bool W>
+static int hub_occupancy(int32_t bytes) {
+  int occ = 0;
+  cudaFuncSetAttribute(mg::solve_binned_hub_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::solve_binned_hub_kernel<W>, mg::PRB_HUB_NT, bytes);
+  cudaGetLastError();
+  return std::max(1, std::min(occ, PRB_HUB_MINB));
+}
 
 template <bool W>
 static int binned_occupancy() {
@@ -503,17 +648,69 @@ static int binned_occupancy() {
   return std::max(1, std::min(occ, 8));
 }
 
+static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
+  using namespace mg;
+  HubCache &hc = plans_of(g)->hubs;
+  if (!hc.ok) {
+    const int64_t n = g->n, m = g->m;
+    cudaStream_t s = g->stream;
+    unsigned *hist = nullptr;
+    MG_CUDA_TRY(cudaMallocAsync((void **)&hist, sizeof(unsigned) * (65536 + 1), s));
+    MG_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(unsigned) * (65536 + 1), s));
+    hub_hist_kernel<<<g->num_sms * 4, 256, 0, s>>>(g->ro, n, hist);
+    std::vector<unsigned> h(65536);
+    MG_CUDA_TRY(cudaMemcpyAsync(h.data(), hist, sizeof(unsigned) * 65536, cudaMemcpyDeviceToHost, s));
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t cum = 0;
+    int32_t thr = 65536;
+    for (int32_t d = 65535; d >= 1; d--) {
+      if (cum + h[d] > cap) break;
+      cum += h[d];
+      thr = d;
+    }
+    MG_CUDA_TRY(cudaMalloc((void **)&hc.slot, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&hc.hv, sizeof(int32_t) * std::max<int64_t>(cap, 1)));
+    MG_CUDA_TRY(cudaMalloc((void **)&hc.cidx, sizeof(int32_t) * (m + 8)));
+    unsigned *count = hist + 65536;
+    hub_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(g->ro, n, thr, cap, hc.slot, hc.hv, count);
+    hub_remap_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ri, m, hc.slot, hc.cidx);
+    unsigned k = 0;
+    MG_CUDA_TRY(cudaMemcpyAsync(&k, count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    MG_CUDA_TRY(cudaFreeAsync(hist, s));
+    hc.K = (int32_t)std::min<unsigned>(k, (unsigned)cap);
+    hc.ok = true;
+  }
+  *out = &hc;
+  return MG_OK;
+}
+
+// Capacity of the column cache: half of an SM's shared memory per CTA (two CTAs
+// of PRB_HUB_NT threads per SM), less the kernel's own static shared memory.
+static int32_t hub_cache_capacity(mg_graph *g) {
+  int per_sm = 0, per_block = 0;
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, g->device);
+  cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, g->device);
+  cudaGetLastError();
+  const int bytes = std::min(per_sm / PRB_HUB_MINB - 2048, per_block - 1024);
+  return std::min(PRB_HUB_CAP, std::max(0, bytes / 4) & ~63);
+}
+
 // Carves the solver's buffers out of ws_main (every per-vertex array padded to
 // n + 8 entries for the widened tile copies), copies the teleport vector and the
 // adjoint right-hand side into padded buffers, computes the row sums s_u and picks
 // the gather variant.
 static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const float *tele_src,
-                             const float *wvec_src, bool use_tma, SolvePlan &sp) {
+                             const float *wvec_src, int variant, SolvePlan &sp) {
   using namespace mg;
+  const bool use_tma = variant == 1;
+  const bool use_hub = variant == 0 && !adjoint && g->n > 0;
   GatherPlan *plan = nullptr;
   BinPlan *bins = nullptr, *rbins = nullptr;
+  HubCache *hubs = nullptr;
   if (use_tma) MG_TRY(get_plan(g, adjoint, &plan));
   else MG_TRY(get_bin_plan(g, adjoint, &bins));
+  if (use_hub) MG_TRY(get_hub_cache(g, hub_cache_capacity(g), &hubs));
   if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
   const size_t np = (size_t)n + 8;
@@ -528,9 +725,12 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
   a.ri_wvec = adjoint ? nr++ : -1;
   int occ = 0;
   sp.use_tma = use_tma;
+  sp.use_hub = use_hub;
+  sp.hub_bytes = use_hub ? (int32_t)(sizeof(float) * hubs->K) : 0;
   sp.weighted = weighted;
   sp.gather = nullptr;
   if (use_tma) sp.gather = gather_variant(weighted, nr, &occ);
+  else if (use_hub) occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
   else occ = weighted ? binned_occupancy<true>() : binned_occupancy<false>();
   const int g1 = g->num_sms * std::max(1, std::min(occ, 8));
   const int g2 = use_tma ? std::max(1, (nt + PRG_NT - 1) / PRG_NT) : 0;
@@ -540,7 +740,9 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
                                    sizeof(float) * np, sizeof(float) * np, sizeof(float) * np,
                                    sizeof(int32_t) * (size_t)nt, sizeof(int32_t) * (size_t)nt,
                                    sizeof(Comp) * (size_t)nt, sizeof(Comp) * (size_t)nt,
-                                   sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp});
+                                   sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp,
+                                   sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0),
+                                   sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0)});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   a.v0 = cv.take<float>(np);
@@ -556,6 +758,12 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
   a.head_val = cv.take<Comp>(nt);
   a.part1 = cv.take<double>(2 * (size_t)gp);
   a.part2 = cv.take<double>(2 * (size_t)gp);
+  if (use_hub) {
+    a.gh0 = cv.take<float>((size_t)hubs->K + 8);
+    a.gh1 = cv.take<float>((size_t)hubs->K + 8);
+    a.hslot = hubs->slot;
+    a.nhub = hubs->K;
+  }
   a.n = n;
   a.srow = srow;
   a.tele = tele_src ? tele : nullptr;
@@ -583,6 +791,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
     a.ntiles = plan->ntiles;
   } else {
     sp.p = prb_args_of(g, *bins, adjoint, a.wts);
+    if (use_hub) sp.p.idx = hubs->cidx;
   }
   MG_CUDA_TRY(cudaGetLastError());
   return MG_OK;
@@ -598,12 +807,16 @@ static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) 
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
   solve_init_kernel<<<ginit, 256, 0, s>>>(a);
   solve_init_reduce_kernel<<<1, 256, 0, s>>>(a, ginit);
+  if (sp.use_hub) {
+    const HubCache &hc = plans_of(g)->hubs;
+    hub_fill_kernel<<<g->num_sms, 256, 0, s>>>(hc.hv, hc.K, a.g0, a.gh0);
+  }
   MG_CUDA_TRY(cudaGetLastError());
   struct Sig {
     SolveArgs a;
     GatherLaunch gl;
     PrbArgs p;
-    int w, tma;
+    int w, tma, hub;
   } sig;
   std::memset(&sig, 0, sizeof(sig));
   sig.a = a;
@@ -611,17 +824,22 @@ static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) 
   sig.p = sp.p;
   sig.w = sp.weighted;
   sig.tma = sp.use_tma;
+  sig.hub = sp.use_hub;
   const int g1 = a.grid1, g2 = a.grid2;
   const GatherLaunch gl = sp.gather;
   const PrbArgs p = sp.p;
-  const bool tma = sp.use_tma, w = sp.weighted;
-  LoopBody body = [a, gl, p, g1, g2, tma, w](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+  const bool tma = sp.use_tma, w = sp.weighted, hub = sp.use_hub;
+  const int32_t hb = sp.hub_bytes;
+  LoopBody body = [a, gl, p, g1, g2, tma, w, hub, hb](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
     SolveArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
     if (tma) {
       gl(g1, st, b);
       solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
+    } else if (hub) {
+      if (w) solve_binned_hub_kernel<true><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
+      else solve_binned_hub_kernel<false><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
     } else if (w) {
       solve_binned_kernel<true><<<g1, PRB_NT, 0, st>>>(b, p);
     } else {
@@ -929,7 +1147,7 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     return MG_ERR_ARG;
   }
   SolvePlan sp;
-  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, o.gather_kernel == 1, sp));
+  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, o.gather_kernel, sp));
   SolveArgs &a = sp.a;
   a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -960,7 +1178,7 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     // fill + row sums + init + init reduce, then per iteration the gather (merge-path:
     // gather + fix-up), plus the loop guard when the loop runs as a graph
     const int64_t per_it = o.gather_kernel == 1 ? 2 : 1;
-    stats->launches = 4 + (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
+    stats->launches = 4 + (sp.use_hub ? 1 : 0) + (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
   }
   return MG_OK;
 }
@@ -1316,7 +1534,7 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
   }
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
   SolvePlan sp;
-  MG_TRY(solve_setup(g, true, weighted, t_dev, w_dev, o.gather_kernel == 1, sp));
+  MG_TRY(solve_setup(g, true, weighted, t_dev, w_dev, o.gather_kernel == 1 ? 1 : 0, sp));
   SolveArgs &a = sp.a;
   a.tn = n > 0 ? 1.0 / (double)n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;

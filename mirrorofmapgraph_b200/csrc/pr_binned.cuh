@@ -38,7 +38,30 @@ constexpr int PRB_BINS = 7;
 #ifndef PRB_UNROLL
 #define PRB_UNROLL 8
 #endif
-constexpr int32_t PRB_HEAVY = 2048;
+// Index (and weight) streams are read once per iteration: loads marked
+// evict-first (ld.global.cs) keep them from displacing the gathered vector in
+// L1 and L2. PRB_STREAM_LOADS=0 uses plain read-only loads instead.
+#ifndef PRB_STREAM_LOADS
+#define PRB_STREAM_LOADS 1
+#endif
+template <typename T>
+__device__ __forceinline__ T prb_stream(const T *p) {
+#if PRB_STREAM_LOADS
+  return __ldcs(p);
+#else
+  return __ldg(p);
+#endif
+}
+#ifndef PRB_HEAVY_EDGES
+#define PRB_HEAVY_EDGES 2048
+#endif
+// Assignment order of a persistent warp: 1 walks the plan from the hub chunks and
+// the heaviest bins down to the lightest (longest items first shortens the
+// tail); 0 walks bins 0..6 in order.
+#ifndef PRB_HEAVY_FIRST
+#define PRB_HEAVY_FIRST 1
+#endif
+constexpr int32_t PRB_HEAVY = PRB_HEAVY_EDGES;
 constexpr int32_t PRB_CHUNK = 2048;
 
 // Plan of one adjacency.
@@ -171,7 +194,7 @@ struct PrbArgs {
 template <bool WEIGHTED>
 __device__ __forceinline__ void prb_add(Comp &acc, float g, const float *__restrict__ wts, int32_t k) {
   if (WEIGHTED) {
-    const float a = __ldg(wts + k);
+    const float a = prb_stream(wts + k);
     const float p = a * g;
     two_sum_add(acc, p);
     acc.lo += __fmaf_rn(a, g, -p);
@@ -205,12 +228,12 @@ __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int3
     int32_t c[PRB_UNROLL];
     float x[PRB_UNROLL];
 #pragma unroll
-    for (int j = 0; j < PRB_UNROLL; j++) c[j] = k + 32 * j < e ? __ldg(p.idx + k + 32 * j) : -1;
+    for (int j = 0; j < PRB_UNROLL; j++) c[j] = k + 32 * j < e ? prb_stream(p.idx + k + 32 * j) : 0;
 #pragma unroll
-    for (int j = 0; j < PRB_UNROLL; j++) x[j] = c[j] >= 0 ? gather(c[j]) : 0.f;
+    for (int j = 0; j < PRB_UNROLL; j++) x[j] = k + 32 * j < e ? gather(c[j]) : 0.f;
 #pragma unroll
     for (int j = 0; j < PRB_UNROLL; j++)
-      if (c[j] >= 0) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
+      if (k + 32 * j < e) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
   }
   group_comp_reduce<32>(acc);
   return acc;
@@ -255,7 +278,7 @@ __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa
         k_of[j] = b + gl < e ? b + gl : -1;
       }
 #pragma unroll
-      for (int j = 0; j < BATCH; j++) c_of[j] = k_of[j] >= 0 ? __ldg(p.idx + k_of[j]) : 0;
+      for (int j = 0; j < BATCH; j++) c_of[j] = k_of[j] >= 0 ? prb_stream(p.idx + k_of[j]) : 0;
 #pragma unroll
       for (int j = 0; j < BATCH; j++) v_of[j] = k_of[j] >= 0 ? gather(c_of[j]) : 0.f;
 #pragma unroll
@@ -280,7 +303,8 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t total = p.wstart[PRB_BINS];
   const int lane = threadIdx.x & 31;
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += nwarps) {
+  for (int64_t wi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total; wi += nwarps) {
+    const int64_t w = PRB_HEAVY_FIRST ? total - 1 - wi : wi;
     int bin = 0;
 #pragma unroll
     for (int q = 1; q < PRB_BINS; q++)

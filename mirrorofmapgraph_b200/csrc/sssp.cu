@@ -40,6 +40,9 @@ struct SsspArgs {
   int32_t *big_v;  // grid-strided bin (BIG_CAP entries)
   int32_t vmask;   // item -> vertex mask: -1 for one instance; batched runs keep the
                    // instance number in the bits above it (item = instance << s | v)
+  int32_t delta;   // near-far bucket width (0: plain frontier Bellman-Ford)
+  int32_t *far0, *far1;  // far piles (ping-pong)
+  uint32_t *infar;       // bit per item: in the current far pile
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
@@ -54,12 +57,17 @@ struct RelaxCtx {
   int32_t vmask;
   int64_t reach_deg;  // out-degrees of vertices reached for the first time
   int64_t updates;
+  // near-far: improvements to a distance >= thr go to the far pile instead
+  int32_t delta;
+  int64_t thr;
+  uint32_t *infar;
+  int32_t *far_out, *far_len_out;
 };
 
-__device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t w) {
-  const int32_t dv = vload(x.dist + v);
+// Relaxes edge (v, u) of weight w, dv = dist[v] as read when v was expanded.
+__device__ __forceinline__ void relax_d(RelaxCtx &x, int32_t dv, int32_t u, int32_t w) {
   const int64_t nd64 = (int64_t)dv + (int64_t)w;
-  bool push = false;
+  bool push = false, far = false;
   if (nd64 < (int64_t)vload(x.dist + u)) {
     const int32_t nd = (int32_t)nd64;
     const int32_t old = atomicMin(x.dist + u, nd);
@@ -67,10 +75,22 @@ __device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t
       x.updates++;
       if (old == INT_MAX) x.reach_deg += x.ro[(u & x.vmask) + 1] - x.ro[u & x.vmask];
       const uint32_t bit = 1u << (u & 31);
-      push = !(atomicOr(x.inq_next + (u >> 5), bit) & bit);
+      if (x.delta <= 0 || (int64_t)nd < x.thr) push = !(atomicOr(x.inq_next + (u >> 5), bit) & bit);
+      else far = !(atomicOr(x.infar + (u >> 5), bit) & bit);
     }
   }
   warp_append(push, u, x.qout, x.qlen_out, x.qcap, x.overflow);
+  if (x.delta > 0) warp_append(far, u, x.far_out, x.far_len_out, x.qcap, x.overflow);
+}
+
+__device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t w) {
+  relax_d(x, vload(x.dist + v), u, w);
+}
+
+__device__ __forceinline__ RelaxCtx relax_ctx(const SsspArgs &a, DevCtl *c, int cur) {
+  const int fc = a.delta > 0 ? vload(&c->far_cur) : 0;
+  return RelaxCtx{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap,
+                  a.vmask, 0, 0, a.delta, vload(&c->thr), a.infar, fc ? a.far1 : a.far0, &c->far_len[fc]};
 }
 
 __device__ void sssp_level_end(const SsspArgs &a) {
@@ -86,7 +106,12 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   c->blocks_done = 0;
   c->big_len = 0;
   const bool over = vload(&c->overflow) != 0;
-  const bool done = nf == 0 || lvl >= c->iter_cap || over;
+  // near-far: an empty near frontier with vertices waiting in the far pile is a
+  // split (the far kernels refill the near frontier), not the end
+  const int32_t nfar = a.delta > 0 ? vload(&c->far_len[vload(&c->far_cur)]) : 0;
+  const bool split = nf == 0 && nfar > 0 && !over;
+  const bool done = (nf == 0 && !split) || lvl >= c->iter_cap || over;
+  c->split = (split && !done) ? 1 : 0;
   if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
   __threadfence();
   c->done = done ? 1 : 0;
@@ -102,11 +127,10 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
     return;
   }
   const int cur = vload(&c->cur);
-  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t nin = vload(&c->qlen[cur]);  // relaxations below read dist[v] once per vertex
   const int32_t *qin = cur ? a.q1 : a.q0;
   uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
-  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, a.vmask,
-             0, 0};
+  RelaxCtx x = relax_ctx(a, c, cur);
   const int32_t hi = ~a.vmask;  // instance bits of an item
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
@@ -120,12 +144,13 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
       inq_cur[v >> 5] = 0u;
       nexp++;
     }
-    expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, insp, [&](int32_t sv, int32_t k) {
-      relax(x, sv, (sv & hi) | ci[k], w ? w[k] : 1);
+    const int32_t dv = v >= 0 ? vload(a.dist + v) : 0;
+    expand_tile_p<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, dv, insp, [&](int32_t sv, int32_t d, int32_t k) {
+      relax_d(x, d, (sv & hi) | ci[k], w ? w[k] : 1);
     }, &big, a.vmask);
     if (a.both)
-      expand_tile<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, insp, [&](int32_t sv, int32_t k) {
-        relax(x, sv, (sv & hi) | ri[k], cw ? cw[k] : 1);
+      expand_tile_p<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, dv, insp, [&](int32_t sv, int32_t d, int32_t k) {
+        relax_d(x, d, (sv & hi) | ri[k], cw ? cw[k] : 1);
       }, nullptr, a.vmask);
   }
   const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
@@ -150,8 +175,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
     return;
   }
   const int cur = vload(&c->cur);
-  RelaxCtx x{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, a.vmask,
-             0, 0};
+  RelaxCtx x = relax_ctx(a, c, cur);
   const int32_t hi = ~a.vmask;  // instance bits of an item
   const int32_t *ci = a.ci, *w = a.w;
   expand_big<SSSP_NT>(sm, a.ro, BigList{a.big_v, &c->big_len},
@@ -165,13 +189,101 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
   if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
 }
 
-__global__ void sssp_clear_kernel(int32_t *dist, uint32_t *b0, uint32_t *b1, int64_t n) {
+// Near-far split, pass 1: the smallest distance still waiting at or above the
+// threshold (entries below it are stale: their vertex was improved into the near
+// frontier since).
+__global__ void __launch_bounds__(SSSP_NT) sssp_far_min_kernel(SsspArgs a) {
+  DevCtl *c = a.ctl;
+  if (vload(&c->done) || !vload(&c->split)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0 && vload(&c->done)) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int fc = vload(&c->far_cur);
+  const int32_t len = min(vload(&c->far_len[fc]), a.qcap);
+  const int32_t *far = fc ? a.far1 : a.far0;
+  const int64_t thr = vload(&c->thr);
+  int32_t mn = INT_MAX;
+  for (int32_t i = blockIdx.x * SSSP_NT + threadIdx.x; i < len; i += gridDim.x * SSSP_NT) {
+    const int32_t d = vload(a.dist + far[i]);
+    if ((int64_t)d >= thr) mn = min(mn, d);
+  }
+  mn = __reduce_min_sync(FULL, mn);
+  if (lane_id() == 0 && mn != INT_MAX) atomicMin(&c->far_min, mn);
+}
+
+// Pass 2: new threshold max(thr, far_min) + delta; waiting vertices below it
+// join the near frontier, the rest move to the other far pile, stale entries are
+// dropped. The last CTA switches the piles.
+__global__ void __launch_bounds__(SSSP_NT) sssp_far_split_kernel(SsspArgs a) {
+  DevCtl *c = a.ctl;
+  if (vload(&c->done) || !vload(&c->split)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0 && vload(&c->done)) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int fc = vload(&c->far_cur);
+  const int32_t len = min(vload(&c->far_len[fc]), a.qcap);
+  const int32_t *far = fc ? a.far1 : a.far0;
+  int32_t *far_keep = fc ? a.far0 : a.far1;
+  const int64_t thr = vload(&c->thr);
+  const int32_t fmin = vload(&c->far_min);
+  const int64_t thr_new = (fmin == INT_MAX ? thr : max(thr, (int64_t)fmin)) + a.delta;
+  int32_t *qnear = cur ? a.q1 : a.q0;
+  uint32_t *inq_near = cur ? a.inq1 : a.inq0;
+  const int32_t ntile = (len + SSSP_NT - 1) / SSSP_NT;
+  for (int32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int32_t i = t * SSSP_NT + threadIdx.x;
+    bool to_near = false, keep = false;
+    int32_t u = 0;
+    if (i < len) {
+      u = far[i];
+      const int64_t d = vload(a.dist + u);
+      const uint32_t bit = 1u << (u & 31);
+      if (d < thr_new) {
+        atomicAnd(a.infar + (u >> 5), ~bit);
+        if (d >= thr) to_near = !(atomicOr(inq_near + (u >> 5), bit) & bit);
+      } else {
+        keep = true;
+      }
+    }
+    warp_append(to_near, u, qnear, &c->qlen[cur], a.qcap, &c->overflow);
+    warp_append(keep, u, far_keep, &c->far_len[fc ^ 1], a.qcap, &c->overflow);
+  }
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->blocks_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  c->blocks_done = 0;
+  c->thr = thr_new;
+  c->far_len[fc] = 0;
+  c->far_cur = fc ^ 1;
+  c->far_min = INT_MAX;
+  c->splits += 1;
+  const bool over = vload(&c->overflow) != 0;
+  const int32_t nn = vload(&c->qlen[cur]);
+  const int32_t nk = vload(&c->far_len[fc ^ 1]);
+  // Nothing moved but vertices still wait: split again at the next pass.
+  c->split = (nn == 0 && nk > 0 && !over) ? 1 : 0;
+  const bool done = (nn == 0 && nk == 0) || over;
+  if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+  __threadfence();
+  c->done = done ? 1 : 0;
+  if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+}
+
+__global__ void sssp_clear_kernel(int32_t *dist, uint32_t *b0, uint32_t *b1, uint32_t *b2, int64_t n) {
   const int64_t nw = (n + 31) >> 5;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     dist[i] = INT_MAX;
     if (i < nw) {
       b0[i] = 0;
       b1[i] = 0;
+      if (b2) b2[i] = 0;
     }
   }
 }
@@ -195,17 +307,28 @@ __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, 
   if (threadIdx.x == 0) {
     c->visited_deg = t;
     c->iter_cap = iter_cap;
+    c->thr = a.delta > 0 ? (int64_t)a.delta : INT64_MAX;
+    c->far_min = INT_MAX;
     c->done = c->overflow ? 1 : 0;
     if (c->overflow) c->status = MG_ERR_QUEUE_OVERFLOW;
   }
 }
 
+// Minimum and sum of the int32 edge weights (out[0] min, out[1..2] the sum as
+// an unsigned 64-bit count of non-negative values).
 __global__ void min_i32_kernel(const int32_t *__restrict__ v, int64_t m, int *__restrict__ out) {
   int mn = INT_MAX;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+  unsigned long long sum = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
     mn = min(mn, v[i]);
+    sum += v[i] > 0 ? (unsigned long long)v[i] : 0ull;
+  }
   mn = __reduce_min_sync(FULL, mn);
-  if (lane_id() == 0 && mn != INT_MAX) atomicMin(out, mn);
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
+  if (lane_id() == 0) {
+    if (mn != INT_MAX) atomicMin(out, mn);
+    if (sum) atomicAdd(reinterpret_cast<unsigned long long *>(out + 2), sum);
+  }
 }
 
 }  // namespace mg
@@ -214,13 +337,16 @@ __global__ void min_i32_kernel(const int32_t *__restrict__ v, int64_t m, int *__
 static mg_status check_weights_nonnegative(mg_graph *g) {
   if (g->vtype != MG_DTYPE_I32 || g->m == 0 || g->weights_checked) return MG_OK;
   int *d = reinterpret_cast<int *>(reinterpret_cast<char *>(g->ctl) + sizeof(DevCtl));
-  int h = INT_MAX;
-  MG_CUDA_TRY(cudaMemcpyAsync(d, &h, sizeof(int), cudaMemcpyHostToDevice, g->stream));
+  int h[4] = {INT_MAX, 0, 0, 0};
+  MG_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
   mg::min_i32_kernel<<<g->num_sms * 4, 256, 0, g->stream>>>((const int32_t *)g->vals, g->m, d);
-  MG_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+  MG_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
   MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  unsigned long long sum = 0;
+  std::memcpy(&sum, h + 2, sizeof(sum));
   g->weights_checked = true;
-  g->min_weight = h;
+  g->min_weight = h[0];
+  g->mean_weight = (double)sum / (double)g->m;
   return MG_OK;
 }
 
@@ -262,9 +388,17 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)nitems) : nitems;
   const int32_t qcap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(qcap64, nitems));
   const int64_t nwords = (nitems + 31) / 32;
+  // Near-far bucket width, when asked for (delta > 0) and no iteration cap is set
+  // (the cap counts the reference's relaxation rounds). Plain frontier
+  // Bellman-Ford otherwise: on R-MAT graphs it is the faster of the two (fewer,
+  // wider rounds), see the SSSP section of the design notes.
+  const int32_t delta = (o.iter_num <= 0 && o.delta > 0 && g->vtype == MG_DTYPE_I32) ? o.delta : -1;
+  const size_t far_items = delta > 0 ? (size_t)qcap : 0;
   const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
-                                   sizeof(int32_t) * (size_t)nseed, sizeof(int32_t) * (size_t)BIG_CAP});
+                                   sizeof(int32_t) * (size_t)nseed, sizeof(int32_t) * (size_t)BIG_CAP,
+                                   sizeof(int32_t) * far_items, sizeof(int32_t) * far_items,
+                                   sizeof(uint32_t) * (delta > 0 ? (size_t)nwords : 0)});
   MG_TRY(ws_reserve(g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   SsspArgs a;
@@ -274,6 +408,10 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   a.q1 = cv.take<int32_t>(qcap);
   int32_t *dsrc = cv.take<int32_t>(nseed);
   a.big_v = cv.take<int32_t>(BIG_CAP);
+  a.delta = delta > 0 ? delta : 0;
+  a.far0 = delta > 0 ? cv.take<int32_t>(far_items) : nullptr;
+  a.far1 = delta > 0 ? cv.take<int32_t>(far_items) : nullptr;
+  a.infar = delta > 0 ? cv.take<uint32_t>(nwords) : nullptr;
   a.ro = g->ro;
   a.ci = g->ci;
   a.w = g->vtype == MG_DTYPE_I32 ? (const int32_t *)g->vals : nullptr;
@@ -289,12 +427,15 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   a.h = 0;
   a.use_cond = 0;
   cudaStream_t s = g->stream;
-  // Bellman-Ford rounds of every instance are bounded by its vertex count.
-  const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
+  // Bellman-Ford rounds of every instance are bounded by its vertex count; the
+  // near-far schedule adds rounds that find nothing new (a bucket's last round),
+  // so its bound is looser.
+  const int64_t rounds = delta > 0 ? std::min<int64_t>(4 * n + 64, INT_MAX - 64) : n + 1;
+  const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)rounds;
   MG_CUDA_TRY(cudaMemcpyAsync(dsrc, seeds, sizeof(int32_t) * nseed, cudaMemcpyHostToDevice, s));
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
-  sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, nitems);
+  sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, a.infar, nitems);
   sssp_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nseed, iter_cap);
   MG_CUDA_TRY(cudaGetLastError());
   const int grid = g->num_sms * 4;
@@ -311,8 +452,13 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
     b.use_cond = use_cond;
     sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
     sssp_relax_big_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    if (b.delta > 0) {
+      sssp_far_min_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+      sssp_far_split_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    }
   };
-  MG_TRY(run_loop(g, vmask == -1 ? SLOT_SSSP : SLOT_BSSSP, &sig, sizeof(sig), o.use_graph >= 0, body, n + 2));
+  MG_TRY(run_loop(g, vmask == -1 ? SLOT_SSSP : SLOT_BSSSP, &sig, sizeof(sig), o.use_graph >= 0, body,
+                  (int64_t)iter_cap + 2));
   MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
   MG_TRY(fetch_ctl(g));
   const DevCtl &hc = *g->ctl_host;
@@ -325,7 +471,9 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
-    stats->launches = 2 + (o.use_graph >= 0 ? 3 * (int64_t)hc.body_iters : 2 * (int64_t)hc.level);
+    const int64_t per = a.delta > 0 ? 4 : 2;
+    stats->launches = 2 + (o.use_graph >= 0 ? (per + 1) * (int64_t)hc.body_iters : per * (int64_t)hc.level);
+    stats->status_detail = a.delta > 0 ? a.delta : 0;
   }
   if (hc.status != 0) {
     mg_set_error("mg_sssp: device status %d (queue capacity %d)", hc.status, qcap);

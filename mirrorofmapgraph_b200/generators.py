@@ -113,3 +113,27 @@ def csr_to_csc(g: HostCsr):
     _check(lib.mg_host_csr_to_csc(g.n, g.m, ro.ctypes.data, ci.ctypes.data, co.ctypes.data, ri.ctypes.data,
                                   perm.ctypes.data), "mg_host_csr_to_csc")
     return co, ri[:g.m], perm[:g.m]
+
+
+def mixed_degree_sources(row_offsets, k: int, seed: int) -> np.ndarray:
+    """k seeded sources: half drawn from the top-1% out-degree vertices, half from
+    the vertices of median (non-zero) out-degree -- the batched workload's mix."""
+    deg = np.diff(np.asarray(row_offsets, dtype=np.int64))
+    rng = np.random.default_rng(seed)
+    order = np.argsort(-deg, kind="stable")
+    top = order[: max(1, len(order) // 100)]
+    med = np.flatnonzero(deg == np.median(deg[deg > 0]))
+    if med.size == 0:
+        med = np.flatnonzero(deg > 0)
+    return np.concatenate([rng.choice(top, k // 2), rng.choice(med, k - k // 2)]).astype(np.int32)
+
+
+def sparse_teleports(n: int, nvec: int, seed: int) -> np.ndarray:
+    """nvec personalised teleport vectors (nvec x n float32): each has a seeded
+    support of U{1..32} vertices with uniform mass on it."""
+    rng = np.random.default_rng(seed)
+    tele = np.zeros((nvec, n), dtype=np.float32)
+    for k in range(nvec):
+        sup = rng.choice(n, size=rng.integers(1, 33), replace=False)
+        tele[k, sup] = 1.0 / sup.size
+    return tele

@@ -54,7 +54,7 @@ def _len(x) -> int:
 
 
 def _opts(directed=1, iter_num=0, direction="auto", device_output=False, queue_sizing=0.0, threshold=0,
-          use_graph=True) -> L.MgOpts:
+          use_graph=True, delta=0) -> L.MgOpts:
     o = L.MgOpts()
     o.directed = int(directed)
     o.iter_num = int(iter_num) if iter_num else 0
@@ -63,6 +63,7 @@ def _opts(directed=1, iter_num=0, direction="auto", device_output=False, queue_s
     o.queue_sizing = float(queue_sizing)
     o.threshold = int(threshold)
     o.use_graph = 0 if use_graph else -1
+    o.delta = int(delta)
     return o
 
 
@@ -247,7 +248,7 @@ class Graph:
     def _pr_opts(mode="refcompat", directed=1, max_iter=0, weighted=False, alpha=0.85, tol=None,
                  compensated=True, device_output=False, use_graph=True, gather="binned") -> L.MgPrOpts:
         o = L.MgPrOpts()
-        o.gather_kernel = {"binned": 0, "tma": 1}[gather]
+        o.gather_kernel = {"binned": 0, "tma": 1, "plain": 2}[gather]
         o.mode = {"refcompat": L.MG_PR_REFCOMPAT, "normalized": L.MG_PR_NORMALIZED}[mode]
         o.directed = int(directed)
         o.max_iter = int(max_iter)

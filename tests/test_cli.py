@@ -8,6 +8,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import oracle
 from mirrorofmapgraph_b200 import _build
 
 INT_MAX = 2**31 - 1
@@ -28,6 +29,16 @@ def _write_mtx(path, d):
         for r in range(n):
             for k in range(ro[r], ro[r + 1]):
                 f.write(f"{r + 1} {ci[k] + 1} {vals[k]}\n")
+
+
+def _check_pagerank(x, d):
+    # The reference's own pass test against CPUPR (relative L2 below its tol 0.1,
+    # Algorithms/PageRank/PageRank.cu:316-321; CPUPR sweeps in place, so it is not a
+    # tighter reference), then the FP64 restatement of the engine's schedule.
+    ref = np.array(d["cpupr"])
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 0.1
+    x64, _ = oracle.pr_refcompat(np.array(d["row_offsets"]), np.array(d["col_idx"]), 1)
+    assert np.abs(x - x64).max() < 1.5e-5  # engine vs FP64 (as the library tests), six printed decimals
 
 
 def _run(exe, *args):
@@ -75,8 +86,7 @@ def test_drivers_match_reference_cpu_results(bins, mtx_fixtures, tmp_path, name)
     r = _run(bins["pagerank"], "-g", g, "-o", out)
     assert r.returncode == 0, r.stderr
     x = _read(out, np.float64)
-    ref = np.array(d["cpupr"])
-    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-3
+    _check_pagerank(x, d)
     if "cpubfs_undirected" in d:
         r = _run(bins["bfs"], "-g", g, "-o", out, "-p", "directed=0")
         assert r.returncode == 0, r.stderr
@@ -129,5 +139,4 @@ def test_cpp_shim_results(shim_driver, mtx_fixtures, tmp_path, name):
     r = _run(shim_driver, "pagerank", g, "0")
     assert r.returncode == 0, r.stderr
     x = np.array([float(v) for v in r.stdout.split()])
-    ref = np.array(d["cpupr"])
-    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-3
+    _check_pagerank(x, d)

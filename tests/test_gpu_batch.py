@@ -11,15 +11,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _c4_sources(ro, k, seed):
-    """Half of the sources from the top-1% degree vertices, half from median-degree ones."""
-    deg = np.diff(ro)
-    rng = np.random.default_rng(seed)
-    order = np.argsort(-deg, kind="stable")
-    top = order[: max(1, len(order) // 100)]
-    med = np.flatnonzero(deg == np.median(deg[deg > 0]))
-    if med.size == 0:
-        med = np.flatnonzero(deg > 0)
-    return np.concatenate([rng.choice(top, k // 2), rng.choice(med, k - k // 2)]).astype(np.int32)
+    return mg.mixed_degree_sources(ro, k, seed)
 
 
 @pytest.fixture(scope="module")
@@ -139,13 +131,7 @@ def test_sssp_batch_power_of_two_device_output(rmat14):
 
 
 def _sparse_teleports(n, nvec, seed):
-    """C4 personalised teleports: support of U{1..32} vertices, uniform mass on it."""
-    rng = np.random.default_rng(seed)
-    tele = np.zeros((nvec, n), dtype=np.float32)
-    for k in range(nvec):
-        sup = rng.choice(n, size=rng.integers(1, 33), replace=False)
-        tele[k, sup] = 1.0 / sup.size
-    return tele
+    return mg.sparse_teleports(n, nvec, seed)
 
 
 PR_L1_TOL = 1e-6  # FP32 engine vs FP64 oracle, same iteration count

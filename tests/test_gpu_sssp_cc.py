@@ -155,3 +155,40 @@ def test_api_mirrors_reference_driver(mtx_fixtures):
         enactor.EnactIterativeSearch(csr_problem, ro, 1, 1, srcs, cfg.getParameter("iter_num"),
                                      cfg.getParameter("threshold"))
         assert csr_problem.ExtractResults().tolist() == ref_sssp_to_engine(d[key]).tolist()
+
+
+@pytest.mark.parametrize("delta", [-1, 0, 1, 7, 300, 1 << 24])
+def test_sssp_near_far_bucket_widths(delta):
+    # near-far (delta > 0) and plain Bellman-Ford (delta <= 0) reach the same
+    # unique distances, in both loop drivers, on
+    # weighted R-MAT, a directed ER graph read both ways and a lattice
+    h = mg.gen_rmat(13, 16, 77, symmetrize=True, weights="int", p0=1, p1=255)
+    with mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True) as g:
+        for s in (0, 5, h.n - 1):
+            ref = oracle.sssp(h.row_offsets, h.col_idx, h.weights_i32, [s])
+            for loop in LOOPS:
+                d, st = g.sssp([s], delta=delta, **loop)
+                assert (d == ref).all()
+            dist_b, _ = g.sssp_batch([s, 1, 2], delta=delta)
+            assert (dist_b[0] == ref).all()
+    e = mg.gen_er(3000, 12000, 6, weights="int", p0=0, p1=40)
+    with mg.Graph(e.row_offsets, e.col_idx, e.weights_i32) as g:
+        for directed in (1, 0):
+            d, _ = g.sssp([0, 9], delta=delta, directed=directed)
+            assert (d == oracle.sssp(e.row_offsets, e.col_idx, e.weights_i32, [0, 9], directed)).all()
+    lat = mg.gen_lattice(64, 80, 0.001, 2, weights="int", p0=1, p1=1000)
+    with mg.Graph(lat.row_offsets, lat.col_idx, lat.weights_i32, symmetric=True) as g:
+        d, st = g.sssp([0], delta=delta)
+        assert (d == oracle.sssp(lat.row_offsets, lat.col_idx, lat.weights_i32, [0])).all()
+        if delta > 0:
+            assert st["status_detail"] == delta
+
+
+def test_sssp_iteration_cap_keeps_reference_rounds():
+    # with iter_num set the schedule is the reference's rounds even when a bucket
+    # width is asked for
+    h = mg.gen_er(500, 3000, 8, weights="int", p0=1, p1=9)
+    with mg.Graph(h.row_offsets, h.col_idx, h.weights_i32) as g:
+        a, _ = g.sssp([0], iter_num=2, delta=5)
+        b, _ = g.sssp([0], iter_num=2, delta=-1)
+        assert (a == b).all()
