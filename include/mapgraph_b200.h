@@ -73,9 +73,10 @@ typedef struct mg_opts {
   int32_t threshold;     /* reference "threshold": accepted for compatibility; strategy is chosen on the device */
   int32_t use_graph;     /* 1 (default when 0): run the iteration loop as a CUDA graph with a device-side while node;
                             -1: host-driven loop (one frontier-size read per iteration) */
-  int32_t delta;         /* SSSP only: > 0 runs the near-far schedule with this bucket width (int32 weights,
-                            iter_num unbounded); <= 0 (default) plain frontier Bellman-Ford, whose rounds are
-                            the reference's, so an iteration cap keeps its meaning */
+  int32_t delta;         /* SSSP only (int32 weights, iter_num unbounded): > 0 runs the near-far schedule with
+                            this bucket width; 0 (default) chooses near-far with 8 x the mean weight on sparse
+                            graphs (mean out-degree <= 8) and plain frontier Bellman-Ford otherwise; < 0 always
+                            plain Bellman-Ford, whose rounds are the reference's (an iteration cap keeps it) */
   int32_t reserved[3];
 } mg_opts;
 
@@ -183,6 +184,14 @@ mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_stats *stat
  * the dangling mass are reduced in FP64. */
 mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nvec, float *ranks,
                       const mg_pr_opts *opts, mg_stats *stats);
+
+/* BFS predecessors from a depth array (mg_bfs output), replacing the reference's
+ * pred_extract (Algorithms/BFS/predextract.cuh:246-373, called at
+ * Algorithms/BFS/bfs.cu:463-468): pred[v] = the largest in-neighbour u with
+ * depth[v] - depth[u] == 1, else -1 (sources get their largest unreached
+ * in-neighbour, as in the reference). depth and pred are host arrays unless
+ * opts->device_output is set; other options are ignored. */
+mg_status mg_bfs_predecessors(mg_graph *g, const int32_t *depth, int32_t *pred, const mg_opts *opts);
 
 /* ---- batching (no reference counterpart: the reference loops the engine once
  * per source, Algorithms/BFS/bfs.cu:442-456) ---------------------------------

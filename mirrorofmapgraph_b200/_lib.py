@@ -73,6 +73,7 @@ SIGNATURES = {
     "mg_graph_device_arrays": (C.c_int, [_P] + [C.POINTER(_P)] * 6),
     "mg_bfs": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_bfs_noalloc": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
+    "mg_bfs_predecessors": (C.c_int, [_P, _P, _P, C.POINTER(MgOpts)]),
     "mg_sssp": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_cc": (C.c_int, [_P, _P, C.POINTER(MgOpts), C.POINTER(MgStats)]),
     "mg_pagerank": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(MgPrOpts), C.POINTER(MgStats)]),

@@ -565,3 +565,81 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   }
   return MG_OK;
 }
+
+// ---- predecessors of a BFS result ------------------------------------------
+// The reference's pred_extract (Algorithms/BFS/predextract.cuh:246-373): over the
+// in-edges of every vertex v, the candidate of edge (u, v) is u when
+// label[v] - label[u] == 1 and -1 otherwise (gather_edge, :143-155), reduced by max
+// (ReduceFunctor, :211-219). Unreached vertices get -1; a source (label 0) gets
+// its largest unreached in-neighbour, as in the reference, where the comment calls
+// that value arbitrary (Algorithms/BFS/bfs.cu:461). Vertices without in-edges get
+// -1. Each lane takes one vertex; in-degrees above 32 are scanned by the warp.
+namespace mg {
+
+__global__ void __launch_bounds__(256) bfs_pred_kernel(const int32_t *__restrict__ co, const int32_t *__restrict__ ri,
+                                                       const int32_t *__restrict__ label, int64_t n,
+                                                       int32_t *__restrict__ pred) {
+  const int lane = lane_id();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t v = base + threadIdx.x;
+    const bool in = v < n;
+    const int32_t lv = in ? label[v] : -1;
+    const int32_t beg = in ? co[v] : 0, end = in ? co[v + 1] : 0;
+    const bool scan = in && lv != -1;  // unreached vertices never match (label -2 does not exist)
+    int32_t best = -1;
+    const bool small = end - beg <= 32;
+    if (scan && small)
+      for (int32_t e = beg; e < end; e++) {
+        const int32_t u = ri[e];
+        if (lv - label[u] == 1) best = max(best, u);
+      }
+    unsigned pend = __ballot_sync(FULL, scan && !small);
+    while (pend) {
+      const int l = __ffs(pend) - 1;
+      pend &= pend - 1;
+      const int32_t b = __shfl_sync(FULL, beg, l), en = __shfl_sync(FULL, end, l), lbl = __shfl_sync(FULL, lv, l);
+      int32_t m = -1;
+      for (int32_t e = b + lane; e < en; e += 32) {
+        const int32_t u = ri[e];
+        if (lbl - label[u] == 1) m = max(m, u);
+      }
+      m = __reduce_max_sync(FULL, m);
+      if (lane == l) best = m;
+    }
+    if (in) pred[v] = best;
+  }
+}
+
+}  // namespace mg
+
+extern "C" mg_status mg_bfs_predecessors(mg_graph *g, const int32_t *depth, int32_t *pred, const mg_opts *opts) {
+  using namespace mg;
+  if (!g || !depth || !pred) {
+    mg_set_error("mg_bfs_predecessors: null argument");
+    return MG_ERR_ARG;
+  }
+  const int dev_io = opts ? opts->device_output : 0;
+  if (!g->has_csc) {
+    mg_set_error("mg_bfs_predecessors: the gather over in-edges needs the CSC (graph created with MG_GRAPH_NO_CSC)");
+    return MG_ERR_UNSUPPORTED;
+  }
+  MG_TRY(graph_enter(g));
+  const int64_t n = g->n;
+  cudaStream_t s = g->stream;
+  const int32_t *dlabel = depth;
+  int32_t *dpred = pred;
+  if (!dev_io) {
+    MG_TRY(ws_reserve(g->ws_out, Carve::need({sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n})));
+    Carve cv(g->ws_out.ptr);
+    int32_t *l = cv.take<int32_t>(n);
+    dpred = cv.take<int32_t>(n);
+    MG_CUDA_TRY(cudaMemcpyAsync(l, depth, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    dlabel = l;
+  }
+  if (n > 0) bfs_pred_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->co, g->ri, dlabel, n, dpred);
+  MG_CUDA_TRY(cudaGetLastError());
+  if (!dev_io) MG_CUDA_TRY(cudaMemcpyAsync(pred, dpred, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  return MG_OK;
+}

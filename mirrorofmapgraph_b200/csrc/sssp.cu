@@ -388,11 +388,20 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)nitems) : nitems;
   const int32_t qcap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(qcap64, nitems));
   const int64_t nwords = (nitems + 31) / 32;
-  // Near-far bucket width, when asked for (delta > 0) and no iteration cap is set
-  // (the cap counts the reference's relaxation rounds). Plain frontier
-  // Bellman-Ford otherwise: on R-MAT graphs it is the faster of the two (fewer,
-  // wider rounds), see the SSSP section of the design notes.
-  const int32_t delta = (o.iter_num <= 0 && o.delta > 0 && g->vtype == MG_DTYPE_I32) ? o.delta : -1;
+  // Schedule. Near-far with bucket width delta when asked for (delta > 0), or by
+  // default on sparse graphs (mean out-degree <= 8, e.g. lattices), where plain
+  // frontier Bellman-Ford re-relaxes every edge many times over its long paths:
+  // there delta = 8 x the mean weight. Plain Bellman-Ford on denser graphs (R-MAT:
+  // fewer, wider rounds win) and whenever an iteration cap is set (the cap counts
+  // the reference's relaxation rounds) or delta < 0.
+  int32_t delta = -1;
+  if (o.iter_num <= 0 && g->vtype == MG_DTYPE_I32) {
+    if (o.delta > 0) {
+      delta = o.delta;
+    } else if (o.delta == 0 && n > 0 && (double)g->m <= 8.0 * (double)n) {
+      delta = (int32_t)std::max(1.0, std::min(1e9, std::round(8.0 * g->mean_weight)));
+    }
+  }
   const size_t far_items = delta > 0 ? (size_t)qcap : 0;
   const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,

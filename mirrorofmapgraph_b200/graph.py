@@ -201,6 +201,17 @@ class Graph:
         _check(self._lib.mg_bfs(self._h, sp, ns, rp, C.byref(o), C.byref(st)), "mg_bfs")
         return res, st.as_dict()
 
+    def bfs_predecessors(self, depth, out=None):
+        """Predecessors from a depth array (the reference's pred_extract): the largest
+        in-neighbour one level closer, -1 where none."""
+        d_p, d_dev, keep = _ptr(depth, np.int32)
+        res, rp, dev = self._out(out, self.n, np.int32)
+        if d_dev != dev:
+            raise ValueError("depth and out must both be host or both be device arrays")
+        o = _opts(device_output=dev)
+        _check(self._lib.mg_bfs_predecessors(self._h, d_p, rp, C.byref(o)), "mg_bfs_predecessors")
+        return res
+
     def sssp(self, srcs, out=None, **kw):
         """struct sssp: shortest distance from the nearest source (INT_MAX unreached)."""
         s, sp, ns = self._srcs(srcs)

@@ -319,3 +319,19 @@ class Ref:
         finally:
             lib.mgref_graph_free(h)
         return ro, ci, vals, co, ri
+
+
+def bfs_pred(ro, ci, depth, csc=None):
+    """BFS predecessors as the reference's pred_extract computes them
+    (Algorithms/BFS/predextract.cuh:246-373): over every in-edge (u, v) the
+    candidate is u when depth[v] - depth[u] == 1, else -1 (gather_edge, :143-155),
+    reduced by max (ReduceFunctor, :211-219); -1 for vertices without in-edges."""
+    co, ri, _ = csc if csc is not None else csc_of(ro, ci)
+    n = len(ro) - 1
+    depth = np.asarray(depth, dtype=np.int64)
+    ri = np.asarray(ri, dtype=np.int64)
+    dst = np.repeat(np.arange(n), np.diff(np.asarray(co, dtype=np.int64)))
+    cand = np.where(depth[dst] - depth[ri] == 1, ri, -1)
+    pred = np.full(n, -1, dtype=np.int64)
+    np.maximum.at(pred, dst, cand)
+    return pred.astype(np.int32)

@@ -196,3 +196,24 @@ def _copy_device_ptr(dst_tensor, src_ptr):
     rc = cudart.cudaMemcpy(C.c_void_p(dst_tensor.data_ptr()), C.c_void_p(src_ptr), nbytes, 3)
     assert rc == 0
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("kind", ["rmat", "er"])
+def test_bfs_predecessors_match_reference_rule(kind):
+    torch = pytest.importorskip("torch")
+    h = (mg.gen_rmat(12, 16, 31, symmetrize=False) if kind == "rmat" else mg.gen_er(5000, 20000, 3))
+    with mg.Graph(h.row_offsets, h.col_idx) as g:
+        depth, _ = g.bfs([1])
+        pred = g.bfs_predecessors(depth)
+        ref = oracle.bfs_pred(h.row_offsets, h.col_idx, depth)
+        np.testing.assert_array_equal(pred, ref)
+        # every reached non-source vertex points one level up, along an edge
+        rows = np.repeat(np.arange(h.n), np.diff(h.row_offsets))
+        edges = set(zip(rows.tolist(), h.col_idx.tolist()))
+        for v in np.flatnonzero(depth > 0)[:500]:
+            u = pred[v]
+            assert depth[u] == depth[v] - 1 and (int(u), int(v)) in edges
+        dd = torch.from_numpy(depth).cuda()
+        dp = torch.empty(h.n, dtype=torch.int32, device="cuda")
+        g.bfs_predecessors(dd, out=dp)
+        np.testing.assert_array_equal(dp.cpu().numpy(), ref)

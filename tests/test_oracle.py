@@ -156,3 +156,12 @@ def test_adjoint_matches_finite_differences():
         lp = oracle.pr_loss(ro, ci, a, w, x, teleport=tp)
         lm = oracle.pr_loss(ro, ci, a, w, x, teleport=tm)
         assert abs((lp - lm) / (2 * h) - gt[i]) <= 1e-4 * max(1.0, abs(gt[i]))
+
+
+def test_bfs_pred_rule_on_a_path():
+    # 0 -> 1 -> 2, 3 -> 2, 4 isolated: pred(1) = 0, pred(2) = 1 (3 is unreached),
+    # the source takes its largest unreached in-neighbour (none here: -1)
+    ro = np.array([0, 1, 2, 2, 3, 3], dtype=np.int32)
+    ci = np.array([1, 2, 2], dtype=np.int32)
+    depth = np.array([0, 1, 2, -1, -1], dtype=np.int32)
+    assert oracle.bfs_pred(ro, ci, depth).tolist() == [-1, 0, 1, -1, -1]
