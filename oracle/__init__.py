@@ -14,6 +14,9 @@ Two layers:
   ingest, compiled from the reference tree when it is present. It pins the
   restatement; tests/golden/ holds vectors recorded from it so the pin also holds
   where the reference tree is absent.
+* ``_ref/gas_ref_tuned`` and ``_ref/gas_ref_generic``: the reference's own bundled
+  vertex programs (Algorithms/*/*.h, unchanged) compiled against this
+  repository's compat GASengine headers, to check that they run on the engine.
 """
 from __future__ import annotations
 
@@ -42,8 +45,14 @@ def build(force: bool = False) -> None:
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
         subprocess.run(["gcc", "-O2", "-shared", "-fPIC", "-o", LIB, src, "-lm"], check=True)
     if os.path.isdir(REFERENCE_DIR):
-        deps = [os.path.join(HERE, "ref_wrap.cpp"), os.path.join(HERE, "build_ref.sh")]
-        if force or not os.path.exists(REF_LIB) or os.path.getmtime(REF_LIB) < max(map(os.path.getmtime, deps)):
+        root = os.path.dirname(HERE)
+        deps = [os.path.join(HERE, "ref_wrap.cpp"), os.path.join(HERE, "build_ref.sh"),
+                os.path.join(root, "tests", "cpp", "gas_ref_programs.cu"),
+                os.path.join(root, "include", "compat", "GASengine", "csr_problem.cuh"),
+                os.path.join(root, "include", "compat", "GASengine", "enactor_vertex_centric.cuh")]
+        outs = [REF_LIB] + [os.path.join(HERE, "_ref", f"gas_ref_{m}") for m in ("tuned", "generic")]
+        newest = max(map(os.path.getmtime, [d for d in deps if os.path.exists(d)]))
+        if force or any(not os.path.exists(o) or os.path.getmtime(o) < newest for o in outs):
             subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True, capture_output=True)
 
 

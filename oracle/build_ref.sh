@@ -38,3 +38,20 @@ g++ -O3 -std=c++14 -shared -fPIC -w \
     "$HERE/ref_wrap.cpp" -o "$OUT/libmgref.so" \
     -L"$CUDA/lib64" -lcudart_static -ldl -lrt -lpthread
 echo "built $OUT/libmgref.so"
+
+# MapGraph's own bundled vertex programs (Algorithms/*/*.h, unchanged) compiled
+# against the compat GASengine headers of this repository and linked with the
+# engine library: oracle/_ref/gas_ref_tuned dispatches them to the tuned entry
+# points, oracle/_ref/gas_ref_generic runs them on the generic kernels.
+ROOT="$(cd "$HERE/.." && pwd)"
+LIBDIR="$ROOT/mirrorofmapgraph_b200/lib"
+if [ -x "$CUDA/bin/nvcc" ] && [ -f "$LIBDIR/libmapgraph_b200.so" ]; then
+  for mode in tuned generic; do
+    flag=""
+    [ "$mode" = generic ] && flag="-DMG_GAS_GENERIC_ONLY"
+    "$CUDA/bin/nvcc" -gencode arch=compute_100a,code=sm_100a -std=c++17 -O2 -w -Xcompiler -fpermissive $flag \
+        -I"$ROOT/include/compat" -I"$ROOT/include" -I"$REF" "$ROOT/tests/cpp/gas_ref_programs.cu" \
+        -o "$OUT/gas_ref_$mode" -L"$LIBDIR" -lmapgraph_b200 -Xlinker -rpath -Xlinker '$ORIGIN/../../mirrorofmapgraph_b200/lib'
+  done
+  echo "built $OUT/gas_ref_tuned $OUT/gas_ref_generic"
+fi
