@@ -109,7 +109,11 @@ typedef struct mg_pr_opts {
                               most-gathered columns cached in shared memory in the forward
                               solve [default]; 1 merge-path tiles staged in shared memory by
                               TMA bulk copies; 2 degree-binned without the column cache */
-  int32_t reserved[2];
+  int32_t autotune;      /* NORMALIZED forward with gather_kernel 0: 1 makes the first such solve on a graph
+                            time the gather variants on it (column caches of 8K, 16K, 20K and the largest
+                            that fits, and no cache; 4 iterations each) and keep the fastest for every later
+                            solve; stats->status_detail reports the choice (cache columns, 0 for none) [0] */
+  int32_t reserved[1];
 } mg_pr_opts;
 
 /* ---- status ------------------------------------------------------------- */

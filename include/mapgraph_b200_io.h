@@ -61,6 +61,17 @@ mg_status mg_gen_lattice(int32_t rows, int32_t cols, double longrange_frac, uint
  * (stable sort by row). Returns MG_ERR_ARG for a malformed or truncated file. */
 mg_status mg_read_market(const char *path, int32_t undirected, mg_host_csr *out);
 
+/* Writes a host CSR as a Matrix Market file (1-based "row col [value]" lines in
+ * CSR order; values: 0 none ("pattern"), 1 the int32 weights, 2 the float
+ * weights). Reading it back with mg_read_market(path, 0, ...) gives the same CSR. */
+mg_status mg_write_market(const char *path, const mg_host_csr *g, int32_t values);
+
+/* Binary CSR cache (no reference counterpart: the reference re-parses the text
+ * file on every run): mg_save_csr writes the arrays of a host CSR, mg_load_csr
+ * reads them back (release with mg_host_csr_free). Native byte order. */
+mg_status mg_save_csr(const char *path, const mg_host_csr *g);
+mg_status mg_load_csr(const char *path, mg_host_csr *out);
+
 /* Host CSR -> CSC (stable: within a column, edges in CSR order, as the
  * reference's std::stable_sort by column, csr_graph.cuh:128-153). perm[k] is the
  * CSR edge id of CSC slot k. Arrays are caller-allocated (n+1, m, m). */

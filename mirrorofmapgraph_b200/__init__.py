@@ -19,10 +19,10 @@ from __future__ import annotations
 
 from .graph import Graph, MapGraphError, device_count, version  # noqa: F401
 from .generators import (HostCsr, gen_er, gen_lattice, gen_rmat, read_market, csr_to_csc,  # noqa: F401
-                         mixed_degree_sources, sparse_teleports)
+                         mixed_degree_sources, sparse_teleports, write_market, save_csr, load_csr)
 from .api import Config, CsrProblem, EnactorVertexCentric, bfs, sssp, cc, pagerank  # noqa: F401
 
 __all__ = [
     "Graph", "MapGraphError", "device_count", "version", "HostCsr", "gen_er", "gen_rmat", "gen_lattice",
-    "read_market", "csr_to_csc", "mixed_degree_sources", "sparse_teleports", "Config", "CsrProblem", "EnactorVertexCentric", "bfs", "sssp", "cc", "pagerank",
+    "read_market", "csr_to_csc", "mixed_degree_sources", "sparse_teleports", "write_market", "save_csr", "load_csr", "Config", "CsrProblem", "EnactorVertexCentric", "bfs", "sssp", "cc", "pagerank",
 ]

@@ -48,7 +48,7 @@ class MgPrOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("directed", C.c_int32), ("max_iter", C.c_int32), ("weighted", C.c_int32),
                 ("alpha", C.c_double), ("tol", C.c_double), ("compensated", C.c_int32),
                 ("device_output", C.c_int32), ("use_graph", C.c_int32), ("gather_kernel", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("autotune", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class MgHostCsr(C.Structure):
@@ -92,6 +92,9 @@ SIGNATURES = {
     "mg_gen_lattice": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.c_int32, C.c_double, C.c_double,
                                  C.POINTER(MgHostCsr)]),
     "mg_read_market": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(MgHostCsr)]),
+    "mg_write_market": (C.c_int, [C.c_char_p, C.POINTER(MgHostCsr), C.c_int32]),
+    "mg_save_csr": (C.c_int, [C.c_char_p, C.POINTER(MgHostCsr)]),
+    "mg_load_csr": (C.c_int, [C.c_char_p, C.POINTER(MgHostCsr)]),
     "mg_host_csr_to_csc": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
 }
 

@@ -315,6 +315,37 @@ mg_status mg_gen_lattice(int32_t rows, int32_t cols, double longrange_frac, uint
   return coo_to_csr(n, coo, wkind, true, out);
 }
 
+namespace {
+
+// One Matrix Market entry line: "row col [value]" with sscanf("%lld %lld %lf")
+// semantics (leading blanks skipped, a missing or unparsable value means 1.0).
+// Returns the number of fields read (2 or 3), or fewer on a malformed line.
+int parse_entry(const char *p, const char *eol, long long *r, long long *c, double *v) {
+  char *q = nullptr;
+  std::string tmp;  // strtoll/strtod stop at the first character they do not take
+  *r = std::strtoll(p, &q, 10);
+  if (q == p || q > eol) return 0;
+  const char *p2 = q;
+  *c = std::strtoll(p2, &q, 10);
+  if (q == p2 || q > eol) return 1;
+  const char *p3 = q;
+  const double x = std::strtod(p3, &q);
+  if (q == p3 || q > eol) return 2;
+  *v = x;
+  return 3;
+}
+
+bool blank_line(const char *p, const char *eol) {
+  while (p < eol && (*p == ' ' || *p == '\t' || *p == '\r')) p++;
+  return p == eol;
+}
+
+}  // namespace
+
+// Parallel reader: the header is parsed first; the body is cut into chunks at
+// line boundaries, each thread counts its entry lines, and after a prefix sum
+// every thread parses its lines into their file positions, so the result equals
+// a line-by-line read (rows then keep file order, as the reference's stable sort).
 mg_status mg_read_market(const char *path, int32_t undirected, mg_host_csr *out) {
   if (!path || !out) {
     mg_set_error("mg_read_market: null argument");
@@ -342,81 +373,128 @@ mg_status mg_read_market(const char *path, int32_t undirected, mg_host_csr *out)
   close(fd);
   buf[got] = '\0';
   const char *p = buf.data(), *end = buf.data() + got;
-  int64_t n = -1, declared = 0, read_edges = 0;
-  Coo coo;
-  std::vector<double> vals;
+  // Problem line: the first line that is neither blank nor a '%' comment.
+  int64_t n = -1, declared = 0;
   while (p < end) {
-    // Blank lines are skipped like the reference's fscanf("%[^\n]\n").
     const char *eol = (const char *)std::memchr(p, '\n', (size_t)(end - p));
     if (!eol) eol = end;
-    const char *q = p;
-    while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) q++;
-    if (q == eol) { p = eol + 1; continue; }
-    if (*p == '%') { p = eol + 1; continue; }
-    std::string line(p, eol);
-    p = eol + 1;
-    if (n < 0) {
-      long long rx, cy, ne;
-      if (std::sscanf(line.c_str(), "%lld %lld %lld", &rx, &cy, &ne) != 3) {
-        mg_set_error("mg_read_market: invalid problem description");
-        return MG_ERR_ARG;
-      }
-      if (rx != cy) {
-        mg_set_error("mg_read_market: not square (%lld, %lld)", rx, cy);
-        return MG_ERR_ARG;
-      }
-      if (rx < 0 || rx > INT32_MAX - 1 || ne < 0 || ne * (undirected ? 2 : 1) > INT32_MAX) {
-        mg_set_error("mg_read_market: sizes exceed int32");
-        return MG_ERR_ARG;
-      }
-      n = rx;
-      declared = ne;
-      coo.src.reserve(ne * (undirected ? 2 : 1));
-      coo.dst.reserve(ne * (undirected ? 2 : 1));
-      vals.reserve(ne * (undirected ? 2 : 1));
+    if (blank_line(p, eol) || *p == '%') {
+      p = eol + 1;
       continue;
     }
-    if (read_edges >= declared) {
-      mg_set_error("mg_read_market: more than %lld entries", (long long)declared);
+    long long rx, cy, ne;
+    std::string line(p, eol);
+    p = eol + 1;
+    if (std::sscanf(line.c_str(), "%lld %lld %lld", &rx, &cy, &ne) != 3) {
+      mg_set_error("mg_read_market: invalid problem description");
       return MG_ERR_ARG;
     }
-    long long r, c;
-    double v = 1.0;
-    int nr = std::sscanf(line.c_str(), "%lld %lld %lf", &r, &c, &v);
-    if (nr != 2 && nr != 3) {
-      mg_set_error("mg_read_market: badly formed entry %lld", (long long)read_edges);
+    if (rx != cy) {
+      mg_set_error("mg_read_market: not square (%lld, %lld)", rx, cy);
       return MG_ERR_ARG;
     }
-    if (r < 1 || r > n || c < 1 || c > n) {
-      mg_set_error("mg_read_market: entry %lld out of range", (long long)read_edges);
+    if (rx < 0 || rx > INT32_MAX - 1 || ne < 0 || ne * (undirected ? 2 : 1) > INT32_MAX) {
+      mg_set_error("mg_read_market: sizes exceed int32");
       return MG_ERR_ARG;
     }
-    coo.src.push_back((int32_t)(r - 1));
-    coo.dst.push_back((int32_t)(c - 1));
-    vals.push_back(v);
-    if (undirected) {
-      coo.src.push_back((int32_t)(c - 1));
-      coo.dst.push_back((int32_t)(r - 1));
-      vals.push_back(v);
-    }
-    read_edges++;
+    n = rx;
+    declared = ne;
+    break;
   }
   if (n < 0) {
     mg_set_error("mg_read_market: no graph found");
     return MG_ERR_ARG;
   }
-  if (read_edges != declared) {
-    mg_set_error("mg_read_market: only %lld/%lld entries read", (long long)read_edges, (long long)declared);
+  const char *body = std::min(p, end);
+  const size_t blen = (size_t)(end - body);
+  const int nth = std::max(1, omp_get_max_threads());
+  const int nchunk = (int)std::min<size_t>((size_t)nth * 8, std::max<size_t>(1, blen / 4096 + 1));
+  std::vector<const char *> cb(nchunk + 1);
+  cb[0] = body;
+  for (int i = 1; i < nchunk; i++) {
+    const char *c = body + blen * (size_t)i / (size_t)nchunk;
+    c = std::max(c, cb[i - 1]);
+    const char *nl = c < end ? (const char *)std::memchr(c, '\n', (size_t)(end - c)) : nullptr;
+    cb[i] = nl ? nl + 1 : end;
+  }
+  cb[nchunk] = end;
+  std::vector<int64_t> cnt(nchunk + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < nchunk; i++) {
+    int64_t k = 0;
+    for (const char *q = cb[i]; q < cb[i + 1];) {
+      const char *eol = (const char *)std::memchr(q, '\n', (size_t)(cb[i + 1] - q));
+      if (!eol) eol = cb[i + 1];
+      if (!blank_line(q, eol) && *q != '%') k++;
+      q = eol + 1;
+    }
+    cnt[i + 1] = k;
+  }
+  for (int i = 0; i < nchunk; i++) cnt[i + 1] += cnt[i];
+  const int64_t entries = cnt[nchunk];
+  if (entries > declared) {
+    mg_set_error("mg_read_market: more than %lld entries", (long long)declared);
+    return MG_ERR_ARG;
+  }
+  if (entries < declared) {
+    mg_set_error("mg_read_market: only %lld/%lld entries read", (long long)entries, (long long)declared);
+    return MG_ERR_ARG;
+  }
+  const int64_t dup = undirected ? 2 : 1;
+  Coo coo;
+  coo.src.resize((size_t)(entries * dup));
+  coo.dst.resize((size_t)(entries * dup));
+  std::vector<double> vals((size_t)(entries * dup));
+  std::atomic<int64_t> bad{INT64_MAX};
+  std::atomic<int> bad_kind{0};
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < nchunk; i++) {
+    int64_t k = cnt[i];
+    for (const char *q = cb[i]; q < cb[i + 1];) {
+      const char *eol = (const char *)std::memchr(q, '\n', (size_t)(cb[i + 1] - q));
+      if (!eol) eol = cb[i + 1];
+      if (blank_line(q, eol) || *q == '%') {
+        q = eol + 1;
+        continue;
+      }
+      long long r = 0, c = 0;
+      double v = 1.0;
+      const int nr = parse_entry(q, eol, &r, &c, &v);
+      int kind = 0;
+      if (nr != 2 && nr != 3) kind = 1;
+      else if (r < 1 || r > n || c < 1 || c > n) kind = 2;
+      if (kind) {
+        int64_t prev = bad.load();
+        while (k < prev && !bad.compare_exchange_weak(prev, k)) {
+        }
+        if (k <= bad.load()) bad_kind.store(kind);
+      } else {
+        const size_t at = (size_t)(k * dup);
+        coo.src[at] = (int32_t)(r - 1);
+        coo.dst[at] = (int32_t)(c - 1);
+        vals[at] = v;
+        if (undirected) {
+          coo.src[at + 1] = (int32_t)(c - 1);
+          coo.dst[at + 1] = (int32_t)(r - 1);
+          vals[at + 1] = v;
+        }
+      }
+      k++;
+      q = eol + 1;
+    }
+  }
+  if (bad.load() != INT64_MAX) {
+    if (bad_kind.load() == 1) mg_set_error("mg_read_market: badly formed entry %lld", (long long)bad.load());
+    else mg_set_error("mg_read_market: entry %lld out of range", (long long)bad.load());
     return MG_ERR_ARG;
   }
   const size_t mm = coo.src.size();
   coo.wi.resize(mm);
-  for (size_t e = 0; e < mm; e++) coo.wi[e] = (int32_t)vals[e];
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < (int64_t)mm; e++) coo.wi[e] = (int32_t)vals[e];
   mg_status st2 = coo_to_csr(n, coo, MG_W_UNIFORM_INT, false, out);
   if (st2 != MG_OK) return st2;
   // Float view of the same values (the PageRank program reads Value = float).
-  std::vector<float> vf(mm);
-  for (size_t e = 0; e < mm; e++) vf[e] = (float)vals[e];
   out->weights_f32 = (float *)std::malloc(sizeof(float) * std::max<size_t>(mm, 1));
   if (!out->weights_f32) {
     mg_host_csr_free(out);
@@ -425,7 +503,131 @@ mg_status mg_read_market(const char *path, int32_t undirected, mg_host_csr *out)
   // Re-run the stable row placement for the float values.
   std::vector<int64_t> cur((size_t)n + 1);
   for (int64_t v = 0; v <= n; v++) cur[v] = out->row_offsets[v];
-  for (size_t e = 0; e < mm; e++) out->weights_f32[cur[coo.src[e]]++] = vf[e];
+  for (size_t e = 0; e < mm; e++) out->weights_f32[cur[coo.src[e]]++] = (float)vals[e];
+  return MG_OK;
+}
+
+mg_status mg_write_market(const char *path, const mg_host_csr *g, int32_t values) {
+  if (!path || !g || g->n < 0 || g->m < 0 || !g->row_offsets || (g->m > 0 && !g->col_idx)) {
+    mg_set_error("mg_write_market: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  const bool vi = values == 1 && g->weights_i32, vf = values == 2 && g->weights_f32;
+  if (values != 0 && !vi && !vf) {
+    mg_set_error("mg_write_market: the graph has no %s weights", values == 1 ? "int32" : "float");
+    return MG_ERR_ARG;
+  }
+  FILE *f = std::fopen(path, "wb");
+  if (!f) {
+    mg_set_error("mg_write_market: cannot open %s: %s", path, std::strerror(errno));
+    return MG_ERR_ARG;
+  }
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate %s general\n%lld %lld %lld\n",
+               vf ? "real" : (vi ? "integer" : "pattern"), (long long)g->n, (long long)g->n, (long long)g->m);
+  // Rows are formatted in parallel blocks, then written in order.
+  const int64_t n = g->n;
+  const int64_t block = 1 << 16;
+  const int64_t nblk = (n + block - 1) / block;
+  bool ok = true;
+  for (int64_t b0 = 0; b0 < nblk && ok; b0 += 64) {
+    const int64_t b1 = std::min<int64_t>(nblk, b0 + 64);
+    std::vector<std::string> text((size_t)(b1 - b0));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t b = b0; b < b1; b++) {
+      std::string &t = text[(size_t)(b - b0)];
+      char line[96];
+      for (int64_t v = b * block; v < std::min(n, (b + 1) * block); v++) {
+        for (int64_t k = g->row_offsets[v]; k < g->row_offsets[v + 1]; k++) {
+          int len;
+          if (vi) len = std::snprintf(line, sizeof(line), "%lld %d %d\n", (long long)v + 1, g->col_idx[k] + 1, g->weights_i32[k]);
+          else if (vf) len = std::snprintf(line, sizeof(line), "%lld %d %.9g\n", (long long)v + 1, g->col_idx[k] + 1, (double)g->weights_f32[k]);
+          else len = std::snprintf(line, sizeof(line), "%lld %d\n", (long long)v + 1, g->col_idx[k] + 1);
+          t.append(line, (size_t)len);
+        }
+      }
+    }
+    for (const std::string &t : text)
+      if (!t.empty() && std::fwrite(t.data(), 1, t.size(), f) != t.size()) ok = false;
+  }
+  if (std::fclose(f) != 0) ok = false;
+  if (!ok) {
+    mg_set_error("mg_write_market: write to %s failed", path);
+    return MG_ERR_ARG;
+  }
+  return MG_OK;
+}
+
+// Binary CSR cache: "MGB200C1", int64 n, int64 m, int32 flags (1: int32
+// weights, 2: float weights), int32 0, then row_offsets (n + 1), col_idx (m),
+// weights_i32 (m, if flagged), weights_f32 (m, if flagged); native byte order.
+static const char kCsrMagic[8] = {'M', 'G', 'B', '2', '0', '0', 'C', '1'};
+
+mg_status mg_save_csr(const char *path, const mg_host_csr *g) {
+  if (!path || !g || g->n < 0 || g->m < 0 || !g->row_offsets || (g->m > 0 && !g->col_idx)) {
+    mg_set_error("mg_save_csr: invalid arguments");
+    return MG_ERR_ARG;
+  }
+  FILE *f = std::fopen(path, "wb");
+  if (!f) {
+    mg_set_error("mg_save_csr: cannot open %s: %s", path, std::strerror(errno));
+    return MG_ERR_ARG;
+  }
+  const int32_t flags = (g->weights_i32 ? 1 : 0) | (g->weights_f32 ? 2 : 0), zero = 0;
+  const int64_t n = g->n, m = g->m;
+  bool ok = std::fwrite(kCsrMagic, 1, 8, f) == 8 && std::fwrite(&n, 8, 1, f) == 1 && std::fwrite(&m, 8, 1, f) == 1 &&
+            std::fwrite(&flags, 4, 1, f) == 1 && std::fwrite(&zero, 4, 1, f) == 1;
+  ok = ok && std::fwrite(g->row_offsets, 4, (size_t)n + 1, f) == (size_t)n + 1;
+  ok = ok && std::fwrite(g->col_idx, 4, (size_t)m, f) == (size_t)m;
+  if (g->weights_i32) ok = ok && std::fwrite(g->weights_i32, 4, (size_t)m, f) == (size_t)m;
+  if (g->weights_f32) ok = ok && std::fwrite(g->weights_f32, 4, (size_t)m, f) == (size_t)m;
+  if (std::fclose(f) != 0) ok = false;
+  if (!ok) {
+    mg_set_error("mg_save_csr: write to %s failed", path);
+    return MG_ERR_ARG;
+  }
+  return MG_OK;
+}
+
+mg_status mg_load_csr(const char *path, mg_host_csr *out) {
+  if (!path || !out) {
+    mg_set_error("mg_load_csr: null argument");
+    return MG_ERR_ARG;
+  }
+  std::memset(out, 0, sizeof(*out));
+  FILE *f = std::fopen(path, "rb");
+  if (!f) {
+    mg_set_error("mg_load_csr: cannot open %s: %s", path, std::strerror(errno));
+    return MG_ERR_ARG;
+  }
+  char magic[8];
+  int64_t n = 0, m = 0;
+  int32_t flags = 0, zero = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCsrMagic, 8) == 0 &&
+            std::fread(&n, 8, 1, f) == 1 && std::fread(&m, 8, 1, f) == 1 && std::fread(&flags, 4, 1, f) == 1 &&
+            std::fread(&zero, 4, 1, f) == 1 && n >= 0 && n <= INT32_MAX - 1 && m >= 0 && m <= INT32_MAX;
+  if (!ok) {
+    std::fclose(f);
+    mg_set_error("mg_load_csr: %s is not a mapgraph_b200 CSR file", path);
+    return MG_ERR_ARG;
+  }
+  out->n = n;
+  out->m = m;
+  out->row_offsets = (int32_t *)std::malloc(4 * ((size_t)n + 1));
+  out->col_idx = (int32_t *)std::malloc(4 * std::max<size_t>((size_t)m, 1));
+  if (flags & 1) out->weights_i32 = (int32_t *)std::malloc(4 * std::max<size_t>((size_t)m, 1));
+  if (flags & 2) out->weights_f32 = (float *)std::malloc(4 * std::max<size_t>((size_t)m, 1));
+  ok = out->row_offsets && out->col_idx && (!(flags & 1) || out->weights_i32) && (!(flags & 2) || out->weights_f32);
+  ok = ok && std::fread(out->row_offsets, 4, (size_t)n + 1, f) == (size_t)n + 1;
+  ok = ok && std::fread(out->col_idx, 4, (size_t)m, f) == (size_t)m;
+  if (flags & 1) ok = ok && std::fread(out->weights_i32, 4, (size_t)m, f) == (size_t)m;
+  if (flags & 2) ok = ok && std::fread(out->weights_f32, 4, (size_t)m, f) == (size_t)m;
+  std::fclose(f);
+  if (ok && (out->row_offsets[0] != 0 || out->row_offsets[n] != m)) ok = false;
+  if (!ok) {
+    mg_host_csr_free(out);
+    mg_set_error("mg_load_csr: %s is truncated or inconsistent", path);
+    return MG_ERR_ARG;
+  }
   return MG_OK;
 }
 

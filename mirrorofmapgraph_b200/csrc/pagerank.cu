@@ -49,6 +49,7 @@ struct HubCache {
   int32_t *slot = nullptr;  // n: slot of a vertex, -1 if not cached
   int32_t *hv = nullptr;    // K: vertex of a slot
   int32_t K = 0;
+  int32_t cap = 0;          // capacity it was built for
   bool ok = false;
 };
 
@@ -57,6 +58,7 @@ struct PlanSet {
   BinPlan bcsc, bcsr;
   bool bcsc_ok = false, bcsr_ok = false;
   HubCache hubs;
+  int32_t tuned_cap = -1;  // autotuned column-cache capacity (-1 not tuned, 0 no cache)
 };
 
 }  // namespace mg
@@ -651,6 +653,11 @@ static int binned_occupancy() {
 static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
   using namespace mg;
   HubCache &hc = plans_of(g)->hubs;
+  if (hc.ok && hc.cap != cap) {  // rebuilt for another capacity
+    for (void *q : {(void *)hc.cidx, (void *)hc.slot, (void *)hc.hv})
+      if (q) cudaFree(q);
+    hc = HubCache();
+  }
   if (!hc.ok) {
     const int64_t n = g->n, m = g->m;
     cudaStream_t s = g->stream;
@@ -679,6 +686,7 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
     MG_CUDA_TRY(cudaStreamSynchronize(s));
     MG_CUDA_TRY(cudaFreeAsync(hist, s));
     hc.K = (int32_t)std::min<unsigned>(k, (unsigned)cap);
+    hc.cap = cap;
     hc.ok = true;
   }
   *out = &hc;
@@ -687,21 +695,23 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
 
 // Capacity of the column cache: half of an SM's shared memory per CTA (two CTAs
 // of PRB_HUB_NT threads per SM), less the kernel's own static shared memory.
-static int32_t hub_cache_capacity(mg_graph *g) {
+static int32_t hub_cache_limit(mg_graph *g) {
   int per_sm = 0, per_block = 0;
   cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, g->device);
   cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, g->device);
   cudaGetLastError();
   const int bytes = std::min(per_sm / PRB_HUB_MINB - 2048, per_block - 1024);
-  return std::min(PRB_HUB_CAP, std::max(0, bytes / 4) & ~63);
+  return std::max(0, bytes / 4) & ~63;
 }
+
+static int32_t hub_cache_capacity(mg_graph *g) { return std::min(PRB_HUB_CAP, hub_cache_limit(g)); }
 
 // Carves the solver's buffers out of ws_main (every per-vertex array padded to
 // n + 8 entries for the widened tile copies), copies the teleport vector and the
 // adjoint right-hand side into padded buffers, computes the row sums s_u and picks
 // the gather variant.
 static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const float *tele_src,
-                             const float *wvec_src, int variant, SolvePlan &sp) {
+                             const float *wvec_src, int variant, SolvePlan &sp, int32_t hub_cap = -1) {
   using namespace mg;
   const bool use_tma = variant == 1;
   const bool use_hub = variant == 0 && !adjoint && g->n > 0;
@@ -710,7 +720,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
   HubCache *hubs = nullptr;
   if (use_tma) MG_TRY(get_plan(g, adjoint, &plan));
   else MG_TRY(get_bin_plan(g, adjoint, &bins));
-  if (use_hub) MG_TRY(get_hub_cache(g, hub_cache_capacity(g), &hubs));
+  if (use_hub) MG_TRY(get_hub_cache(g, hub_cap > 0 ? hub_cap : hub_cache_capacity(g), &hubs));
   if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
   const size_t np = (size_t)n + 8;
@@ -1134,6 +1144,48 @@ static mg_status pagerank_refcompat(mg_graph *g, float *ranks, const mg_pr_opts 
 }
 
 // NORMALIZED, one vector.
+// Gather autotuner (mg_pr_opts.autotune): times the forward solve's gather
+// variants on this graph -- the column cache at several capacities and the binned
+// kernel without a cache -- over four iterations each (second of two runs, so the
+// executable graph is cached) and keeps the fastest for the graph's later solves.
+// Results do not depend on the choice beyond rounding.
+static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opts &o) {
+  using namespace mg;
+  const bool weighted = o.weighted != 0;
+  const int32_t limit = hub_cache_limit(g);
+  std::vector<int32_t> caps;
+  for (int32_t c : {8192, 16384, 20480, limit})
+    if (c > 0 && c <= limit && std::find(caps.begin(), caps.end(), c) == caps.end()) caps.push_back(c);
+  caps.push_back(0);  // no cache
+  float best = 0.f;
+  int32_t best_cap = 0;
+  for (size_t i = 0; i < caps.size(); i++) {
+    const int32_t c = caps[i];
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; rep++) {
+      SolvePlan sp;
+      MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, c > 0 ? 0 : 2, sp, c > 0 ? c : -1));
+      SolveArgs &a = sp.a;
+      a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
+      a.alpha = o.alpha > 0 ? o.alpha : 0.85;
+      a.tol = 1e-300;  // run all four iterations
+      a.max_iter = 4;
+      a.adjoint = 0;
+      MG_CUDA_TRY(cudaEventRecord(g->ev0, g->stream));
+      MG_TRY(solve_run(g, sp, 0, SLOT_PR));
+      MG_CUDA_TRY(cudaEventRecord(g->ev1, g->stream));
+      MG_CUDA_TRY(cudaEventSynchronize(g->ev1));
+      MG_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    }
+    if (i == 0 || ms < best) {
+      best = ms;
+      best_cap = c;
+    }
+  }
+  plans_of(g)->tuned_cap = best_cap;
+  return MG_OK;
+}
+
 static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *ranks_out, int out_is_device,
                                      const mg_pr_opts &o, mg_stats *stats) {
   using namespace mg;
@@ -1146,8 +1198,14 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     mg_set_error("mg_pagerank: weighted mode needs float edge values");
     return MG_ERR_ARG;
   }
+  PlanSet *ps = plans_of(g);
+  if (o.gather_kernel == 0 && o.autotune && ps->tuned_cap < 0) MG_TRY(pr_autotune(g, tele_dev, o));
+  int variant = o.gather_kernel;
+  int32_t cap = -1;
+  if (variant == 0 && ps->tuned_cap == 0) variant = 2;
+  else if (variant == 0 && ps->tuned_cap > 0) cap = ps->tuned_cap;
   SolvePlan sp;
-  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, o.gather_kernel, sp));
+  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, variant, sp, cap));
   SolveArgs &a = sp.a;
   a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -1178,6 +1236,7 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     // fill + row sums + init + init reduce, then per iteration the gather (merge-path:
     // gather + fix-up), plus the loop guard when the loop runs as a graph
     const int64_t per_it = o.gather_kernel == 1 ? 2 : 1;
+    stats->status_detail = sp.use_hub ? (int32_t)(sp.hub_bytes / sizeof(float)) : 0;
     stats->launches = 4 + (sp.use_hub ? 1 : 0) + (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
   }
   return MG_OK;

@@ -102,6 +102,42 @@ def read_market(path: str, undirected: bool = False) -> HostCsr:
     return _take(h)
 
 
+def _view(g: HostCsr):
+    """An MgHostCsr over the arrays of g (kept alive by the returned tuple)."""
+    keep = [np.ascontiguousarray(g.row_offsets, dtype=np.int32), np.ascontiguousarray(g.col_idx, dtype=np.int32)]
+    h = L.MgHostCsr()
+    h.n, h.m = g.n, g.m
+    h.row_offsets = keep[0].ctypes.data_as(C.POINTER(C.c_int32))
+    h.col_idx = keep[1].ctypes.data_as(C.POINTER(C.c_int32))
+    if g.weights_i32 is not None:
+        keep.append(np.ascontiguousarray(g.weights_i32, dtype=np.int32))
+        h.weights_i32 = keep[-1].ctypes.data_as(C.POINTER(C.c_int32))
+    if g.weights_f32 is not None:
+        keep.append(np.ascontiguousarray(g.weights_f32, dtype=np.float32))
+        h.weights_f32 = keep[-1].ctypes.data_as(C.POINTER(C.c_float))
+    return h, keep
+
+
+def write_market(path: str, g: HostCsr, values: str | None = None) -> None:
+    """Writes g as a Matrix Market file (values None, "int" or "float")."""
+    h, keep = _view(g)
+    kind = {None: 0, "int": 1, "float": 2}[values]
+    _check(L.load().mg_write_market(path.encode(), C.byref(h), kind), "mg_write_market")
+
+
+def save_csr(path: str, g: HostCsr) -> None:
+    """Binary CSR cache of g (mg_save_csr)."""
+    h, keep = _view(g)
+    _check(L.load().mg_save_csr(path.encode(), C.byref(h)), "mg_save_csr")
+
+
+def load_csr(path: str) -> HostCsr:
+    """Reads a binary CSR cache written by save_csr (mg_load_csr)."""
+    h = L.MgHostCsr()
+    _check(L.load().mg_load_csr(path.encode(), C.byref(h)), "mg_load_csr")
+    return _take(h)
+
+
 def csr_to_csc(g: HostCsr):
     """Stable host transpose: (col_offsets, row_idx, perm) with perm[k] the CSR edge of CSC slot k."""
     lib = L.load()

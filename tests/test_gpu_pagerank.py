@@ -202,3 +202,15 @@ def test_hub_column_cache_partial(weighted):
     xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, w, 0.85, 0.0, st["iterations"])
     assert np.abs(x - xr).sum() <= L1_TOL
     assert np.abs(x - xb).sum() <= L1_TOL
+
+
+def test_gather_autotune_picks_and_keeps_a_variant():
+    h = mg.gen_rmat(15, 16, 9, symmetrize=True)
+    with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+        x, st = g.pagerank(mode="normalized", autotune=True)
+        choice = st["status_detail"]  # cached columns of the chosen variant, 0 for none
+        assert 0 <= choice <= h.n
+        x2, st2 = g.pagerank(mode="normalized", autotune=True)  # tuned once per graph
+        assert st2["status_detail"] == choice and (x == x2).all()
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+        assert np.abs(x - xr).sum() <= L1_TOL

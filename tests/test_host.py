@@ -170,3 +170,54 @@ def test_program_selectors_mirror_reference():
     assert mg.sssp.INIT_VALUE == 2**31 - 1 and mg.sssp.applyOverEdges() == "APPLY_FRONTIER"
     assert mg.cc.srcVertex() == "ALL"
     assert mg.pagerank.gatherOverEdges() == "GATHER_IN_EDGES" and not mg.pagerank.allow_duplicates
+
+
+def _same(a, b, weights=("weights_i32", "weights_f32")):
+    assert (a.row_offsets == b.row_offsets).all() and (a.col_idx == b.col_idx).all()
+    for w in weights:
+        x, y = getattr(a, w), getattr(b, w)
+        assert (x is None) == (y is None) and (x is None or (x == y).all())
+
+
+def test_market_write_read_round_trip(tmp_path):
+    g = mg.gen_rmat(13, 8, 5, weights="int", p0=1, p1=1000)
+    p = str(tmp_path / "g.mtx")
+    mg.write_market(p, g, values="int")
+    h = mg.read_market(p)
+    _same(g, h, weights=("weights_i32",))
+    assert np.allclose(h.weights_f32, g.weights_i32)
+    mg.write_market(p, g)  # pattern: unit values
+    assert (mg.read_market(p).weights_i32 == 1).all()
+
+
+def test_parallel_reader_matches_line_order_with_comments_and_blanks(tmp_path):
+    # entries in random order with comments and blank lines between them: rows must
+    # keep file order (the reference's stable sort) and values parse as doubles
+    rng = np.random.default_rng(3)
+    n, m = 500, 20000
+    r = rng.integers(1, n + 1, m)
+    c = rng.integers(1, n + 1, m)
+    v = rng.integers(-5, 100, m)
+    lines = ["%%MatrixMarket matrix coordinate integer general", "% comment", "", f"{n} {n} {m}"]
+    for i in range(m):
+        lines.append(f"{r[i]} {c[i]} {v[i]}.0" if i % 3 else f"  {r[i]}\t{c[i]} {v[i]}")
+        if i % 997 == 0:
+            lines += ["% in-between comment", "   "]
+    p = tmp_path / "x.mtx"
+    p.write_text("\n".join(lines))
+    g = mg.read_market(str(p))
+    order = np.argsort(r - 1, kind="stable")
+    assert (g.col_idx == (c - 1)[order]).all() and (g.weights_i32 == v[order]).all()
+    gu = mg.read_market(str(p), undirected=True)
+    assert gu.m == 2 * m
+
+
+def test_binary_csr_cache_round_trip_and_rejects_garbage(tmp_path):
+    g = mg.gen_rmat(12, 8, 6, weights="lognormal", p0=0, p1=1)
+    p = str(tmp_path / "g.csr")
+    mg.save_csr(p, g)
+    _same(g, mg.load_csr(p))
+    q = tmp_path / "bad.csr"
+    q.write_bytes(b"not a csr file at all")
+    with pytest.raises(RuntimeError):
+        mg.load_csr(str(q))
