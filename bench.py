@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-versus-looped section")
     p.add_argument("--batched-scale", type=int, default=20)
+    p.add_argument("--pr-gather", default="auto", choices=["auto", "binned", "cached"],
+                   help="PageRank gather: autotuned per graph (default) or forced (for profiling one kernel)")
     p.add_argument("--no-extra", action="store_true",
                    help="skip the lattice (BFS/SSSP) and weighted PageRank forward + adjoint sections")
     p.add_argument("--host-loop", action="store_true",
@@ -286,40 +288,78 @@ def cpu_sample_graph():
     return mg.gen_rmat(CPU_SAMPLE_SCALE, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
 
 
+def _ref_worker(path, src, steps, warmup, barrier, out):
+    """One reference process: loads the sample graph, runs the warm-up passes,
+    waits for the others, then times `steps` passes of CPUBFS + CPUCC + CPUPR."""
+    import mirrorofmapgraph_b200 as mg
+    h = mg.load_csr(path)
+    for _ in range(warmup):
+        cpu_reference_run(h, src)
+    barrier.wait()
+    t0 = time.time()
+    per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
+    for _ in range(steps):
+        r = cpu_reference_run(h, src)
+        for k in per:
+            per[k][0] += r[k][0]
+            per[k][1] += r[k][1]
+    out.put((t0, time.time(), per))
+
+
 def run_reference(args):
+    """The reference's own CPU implementation of the path (CPUBFS, CPUCC, CPUPR,
+    compiled from the reference tree into oracle/_ref). The functions are serial,
+    so all host cores are used by running one independent copy per core (up to
+    32), each from its own source, on the bounded sample graph; the value is all
+    copies' TEPS edges over the wall time from the common start to the last finish."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     t_all = time.time()
     try:
+        import multiprocessing as mp
+        import tempfile
         import oracle
+        import mirrorofmapgraph_b200 as mg
         if not oracle.have_ref():
             raise RuntimeError("oracle/_ref/libmgref.so missing (reference CPU path not built)")
         h = cpu_sample_graph()
-        srcs = sources(h, max(1, args.steps), SEED + 1)
-        for i in range(args.warmup):
-            cpu_reference_run(h, srcs[i % len(srcs)])
-        edges = secs = 0.0
-        per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
-        for i in range(args.steps):
-            r = cpu_reference_run(h, srcs[i % len(srcs)])
-            for k in per:
-                per[k][0] += r[k][0]
-                per[k][1] += r[k][1]
-                edges += r[k][0]
-                secs += r[k][1]
-        value = edges / secs / 1e9
+        try:
+            ncores = len(os.sched_getaffinity(0))
+        except Exception:
+            ncores = os.cpu_count() or 1
+        procs = max(1, min(32, ncores))
+        srcs = sources(h, procs, SEED + 1)
+        tmpdir = tempfile.mkdtemp(prefix="mg_ref_")
+        path = os.path.join(tmpdir, "sample.csr")
+        mg.save_csr(path, h)
+        ctx = mp.get_context("spawn")
+        barrier, out = ctx.Barrier(procs), ctx.Queue()
+        ps = [ctx.Process(target=_ref_worker, args=(path, srcs[i], args.steps, args.warmup, barrier, out))
+              for i in range(procs)]
+        for p_ in ps:
+            p_.start()
+        res = [out.get() for _ in ps]
+        for p_ in ps:
+            p_.join()
+        os.remove(path)
+        os.rmdir(tmpdir)
+        wall = max(r[1] for r in res) - min(r[0] for r in res)
+        per = {k: [sum(r[2][k][0] for r in res), sum(r[2][k][1] for r in res)] for k in ("bfs", "cc", "pagerank")}
+        edges = sum(v[0] for v in per.values())
+        value = edges / wall / 1e9
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32",
             "data": "synthetic (seeded R-MAT)",
             "config": {"workload": f"rmat_s{CPU_SAMPLE_SCALE}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
                                    "CPUBFS + CPUCC + CPUPR", "scale": CPU_SAMPLE_SCALE, "n": h.n, "m": h.m},
-            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": 1, "kind": "reference",
-                             "sample": f"reference CPUBFS/CPUCC/CPUPR (serial) on R-MAT scale {CPU_SAMPLE_SCALE} "
-                                       f"per step; CPUPR alone takes ~35 s at scale 22"},
-            "per_algorithm": {k: {"gteps": v[0] / v[1] / 1e9 if v[1] else None, "seconds": v[1]}
+            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs, "kind": "reference",
+                             "sample": f"{procs} concurrent copies of the reference's serial CPUBFS/CPUCC/CPUPR, "
+                                       f"each {args.steps} step(s) on R-MAT scale {CPU_SAMPLE_SCALE} from its own "
+                                       f"source (CPUPR alone takes ~35 s at scale 22)"},
+            "per_algorithm": {k: {"gteps_per_core": v[0] / v[1] / 1e9 if v[1] else None, "core_seconds": v[1]}
                               for k, v in per.items()},
             "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": time.time() - t_all,
@@ -369,14 +409,18 @@ def run_ours(args):
 
     ug = not args.host_loop
 
+    pr_kw = dict(autotune=True) if args.pr_gather == "auto" else dict(gather=args.pr_gather)
+
     def step(i):
         with torch.cuda.stream(stream):
             flush.zero_()
         s = srcs[i % len(srcs)]
         (_, st_b), tb = timed(lambda: g.bfs([s], out=depth, use_graph=ug))
         (_, st_c), tc = timed(lambda: g.cc(out=label))
+        # autotune: the first (warm-up) solve times the gather variants on this GPU
+        # and graph and keeps the fastest (mg_pr_opts.autotune)
         (_, st_p), tp = timed(lambda: g.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT,
-                                                 out=rank_v, use_graph=ug))
+                                                 out=rank_v, use_graph=ug, **pr_kw))
         return {"bfs": (st_b["edges_traversed"], tb, st_b), "cc": (m, tc, st_c),
                 "pagerank": (m * st_p["iterations"], tp, st_p)}
 
@@ -390,8 +434,10 @@ def run_ours(args):
     per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
     launches = 0
     pr_iters = 0
+    pr_cache = 0
     pr_ms = 0.0
     bfs_stats = []
+    cc_stats = []
     for i in range(args.steps):
         r = step(args.warmup + i)
         for k in per:
@@ -399,8 +445,10 @@ def run_ours(args):
             per[k][1] += r[k][1]
             launches += r[k][2]["launches"]
         pr_iters += r["pagerank"][2]["iterations"]
+        pr_cache = r["pagerank"][2]["status_detail"]
         pr_ms += r["pagerank"][1]
         bfs_stats.append(r["bfs"][2])
+        cc_stats.append(r["cc"][2])
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     if dist:
@@ -417,21 +465,24 @@ def run_ours(args):
     value = edges / (ms * 1e-3) / 1e9
 
     # SSSP, reported per algorithm (not in the headline; see the module docstring).
-    sssp_edges = sssp_ms = 0.0
+    sssp_edges = sssp_ms = sssp_bytes = 0.0
     for i in range(min(3, args.steps)):
         with torch.cuda.stream(stream):
             flush.zero_()
         (_, st), t = timed(lambda: g.sssp([srcs[i]], out=dist_v, use_graph=ug))
         sssp_edges += st["edges_traversed"]
         sssp_ms += t
+        sssp_bytes += st["bytes_compulsory"]
 
-    # Roofline of the dominant kernel: solve_binned_hub_kernel, one launch per
-    # PageRank iteration (degree-binned CSC gather with the shared-memory column
-    # cache + row update + residual). Algorithmic
+    # Roofline of the dominant kernel: one launch per PageRank iteration of the
+    # gather the autotuner kept -- solve_binned_kernel (degree-binned CSC gather +
+    # row update + residual) or solve_binned_hub_kernel (the same with a column
+    # cache in shared memory). Algorithmic
     # bytes per launch = offsets 4(n+1) + indices 4m + read x 4n + write x 4n +
     # write x/s 4n. Its duration is the PageRank call's device time divided by the
     # iterations (the call also holds two init kernels, so this slightly
     # understates the kernel's own rate).
+    pr_kernel = "solve_binned_hub_kernel" if pr_cache > 0 else "solve_binned_kernel"
     pr_bytes_iter = 4 * (n + 1) + 4 * m + 12 * n
     pr_s_iter = (pr_ms / max(pr_iters, 1)) * 1e-3
     achieved = pr_bytes_iter / pr_s_iter / 1e9
@@ -439,7 +490,7 @@ def run_ours(args):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        t = tj.get("solve_binned_hub_kernel", {})
+        t = tj.get(pr_kernel, {})
         if t.get("scale") == args.scale:
             traffic = t.get("dram_bytes_per_launch")
     except Exception:
@@ -447,27 +498,36 @@ def run_ours(args):
     per_alg = {k: {"gteps": v[0] / (v[1] * 1e-3) / 1e9, "ms_per_run": v[1] / args.steps} for k, v in per.items()}
     per_alg["sssp"] = {"gteps": sssp_edges / (sssp_ms * 1e-3) / 1e9 if sssp_ms else None,
                        "ms_per_run": sssp_ms / max(1, min(3, args.steps)), "in_headline": False}
-    # compulsory-byte roofline fractions per algorithm (stats.bytes_compulsory / time)
-    for k, key in (("bfs", "bfs"),):
-        bc = sum(s["bytes_compulsory"] for s in bfs_stats)
+    # compulsory-byte roofline fractions per algorithm: the programs' own count of
+    # compulsory DRAM bytes (mg_stats.bytes_compulsory) over their device time
+    for k, sts in (("bfs", bfs_stats), ("cc", cc_stats)):
+        bc = sum(s_["bytes_compulsory"] for s_ in sts)
         per_alg[k]["hbm_frac"] = bc / (per[k][1] * 1e-3) / 1e9 / peak
+    if sssp_ms:
+        per_alg["sssp"]["hbm_frac"] = sssp_bytes / (sssp_ms * 1e-3) / 1e9 / peak
     per_alg["pagerank"]["hbm_frac"] = achieved / peak
 
     # End to end through the public API with host buffers: upload from pinned host
-    # memory, run the three programs with host outputs, read them back, release.
+    # memory, run the three programs with outputs in pinned host buffers (read back
+    # by each call), release the graph. One untimed pass first.
     ro_pin = torch.from_numpy(h.row_offsets).pin_memory()
     ci_pin = torch.from_numpy(h.col_idx).pin_memory()
+    depth_pin = torch.empty(n, dtype=torch.int32).pin_memory()
+    label_pin = torch.empty(n, dtype=torch.int32).pin_memory()
+    rank_pin = torch.empty(n, dtype=torch.float32).pin_memory()
     e2e_edges = 0.0
     e2e_s = 0.0
     h2d = (n + 1) * 4 + m * 4
     d2h = 3 * n * 4
-    for i in range(args.e2e_steps):
+    for i in range(-1, args.e2e_steps) if args.e2e_steps > 0 else ():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         with mg.Graph(ro_pin, ci_pin, symmetric=True) as ge:
-            d, sb = ge.bfs([srcs[i % len(srcs)]])
-            _, sc = ge.cc()
-            _, sp = ge.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT)
+            _, sb = ge.bfs([srcs[i % len(srcs)]], out=depth_pin)
+            _, sc = ge.cc(out=label_pin)
+            _, sp = ge.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT, out=rank_pin)
+        if i < 0:
+            continue
         e2e_s += time.perf_counter() - t0
         e2e_edges += sb["edges_traversed"] + m + m * sp["iterations"]
     e2e = e2e_edges / e2e_s / 1e9 * (world if world > 1 else 1) if e2e_s > 0 else None
@@ -482,7 +542,8 @@ def run_ours(args):
                    "scale": args.scale, "edge_factor": args.edge_factor, "n": n, "m": m,
                    "l2": "256 MiB buffer written between steps; graph (CSR 537 MB) larger than L2",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "solve_binned_hub_kernel (one PageRank iteration)",
+        "roofline": {"bound": "hbm", "kernel": f"{pr_kernel} (one PageRank iteration"
+                     + (f", {pr_cache} cached columns)" if pr_cache else ")"),
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": pr_bytes_iter},

@@ -105,14 +105,13 @@ typedef struct mg_pr_opts {
   int32_t compensated;   /* 1: two-sum compensated FP32 accumulation [1]; -1 plain FP32 sums */
   int32_t device_output; /* 1: ranks/teleport/gradient arrays are device pointers */
   int32_t use_graph;     /* as mg_opts.use_graph */
-  int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps, with the
-                              most-gathered columns cached in shared memory in the forward
-                              solve [default]; 1 merge-path tiles staged in shared memory by
-                              TMA bulk copies; 2 degree-binned without the column cache */
+  int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps [default]; 1 merge-path tiles
+                            staged in shared memory by TMA bulk copies; 2 degree-binned with the most-gathered
+                            columns cached in shared memory (forward solve; the adjoint uses 0) */
   int32_t autotune;      /* NORMALIZED forward with gather_kernel 0: 1 makes the first such solve on a graph
-                            time the gather variants on it (column caches of 8K, 16K, 20K and the largest
-                            that fits, and no cache; 4 iterations each) and keep the fastest for every later
-                            solve; stats->status_detail reports the choice (cache columns, 0 for none) [0] */
+                            time the degree-binned kernel without and with column caches of 8K, 16K, 20K and
+                            the most that fits (4 iterations each) and keep the fastest for every later solve;
+                            stats->status_detail reports the choice (cache columns, 0 for none) [0] */
   int32_t reserved[1];
 } mg_pr_opts;
 
@@ -251,6 +250,55 @@ mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *
 #define MG_BFS_NOALLOC_MAX_SOURCES 1024
 mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth, const mg_opts *opts,
                          mg_stats *stats);
+
+/* ---- BFS over a 1-D vertex partition (one rank per GPU) ----------------------
+ * For graphs split over several GPUs. The reference lays out, but never runs,
+ * per-GPU vertex ranges (GASengine/csr_problem.cuh:339-365, GraphSlice per GPU;
+ * its driver loops run on GPU 0 only, enactor_vertex_centric.cuh:2398-2966).
+ * Rank r holds the out-edges and in-edges of its vertices [lo, hi) with global
+ * vertex ids and the global out-degree of all n vertices. A BFS is
+ *   mg_part_bfs_begin, then while !level.done:
+ *     mg_part_bfs_step(bits)                 this rank's discoveries, n bits
+ *     all-gather bits over the ranks         world x words, rank-major (NCCL on
+ *                                            mg_part_stream's stream, or one shared
+ *                                            buffer when the partitions share a GPU)
+ *     mg_part_bfs_merge(gathered, world)     next frontier, same on every rank
+ *   mg_part_bfs_result
+ * Every rank must pass the same sources and options; the levels, directions and
+ * depths then agree on all ranks (the merge folds the same words everywhere). */
+typedef struct mg_part mg_part;
+
+typedef struct mg_part_level {
+  int64_t frontier;       /* vertices of the frontier the next step expands */
+  int64_t frontier_edges; /* their out-edges */
+  int32_t level;          /* levels completed */
+  int32_t done;           /* 1: frontier empty or iter_num reached */
+  int32_t direction;      /* MG_DIR_PUSH or MG_DIR_PULL for the next step */
+  int32_t reserved;
+} mg_part_level;
+
+/* lo must be a multiple of 32, hi a multiple of 32 or n. out_offsets / in_offsets
+ * have hi - lo + 1 entries (row v - lo), out_idx / in_idx global ids in [0, n).
+ * With MG_GRAPH_SYMMETRIC the in-edges are the out-edges (in_* may be NULL).
+ * out_degree (n entries) may be NULL only when [lo, hi) = [0, n).
+ * MG_GRAPH_DEVICE_INPUT: the arrays are device pointers on the current device. */
+mg_status mg_part_create(int64_t n, int64_t lo, int64_t hi, const int32_t *out_offsets, const int32_t *out_idx,
+                         const int32_t *in_offsets, const int32_t *in_idx, const int32_t *out_degree,
+                         uint32_t flags, mg_part **out);
+mg_status mg_part_destroy(mg_part *p);
+/* The stream the partition's kernels run on (a cudaStream_t). */
+mg_status mg_part_stream(const mg_part *p, void **stream);
+/* Words of the n-bit bitmaps exchanged per level: (n + 31) / 32. */
+mg_status mg_part_words(const mg_part *p, int64_t *words);
+/* Resets the run and seeds the sources (opts: direction, iter_num). */
+mg_status mg_part_bfs_begin(mg_part *p, const int32_t *srcs, int32_t nsrc, const mg_opts *opts,
+                            mg_part_level *level);
+/* This rank's discoveries of the pending level into bits (device, words entries). */
+mg_status mg_part_bfs_step(mg_part *p, uint32_t *bits);
+/* Folds the world's bitmaps (device, world x words) into the next frontier. */
+mg_status mg_part_bfs_merge(mg_part *p, const uint32_t *gathered, int32_t world, mg_part_level *level);
+/* Depths of all n vertices (replicated; host or device output) and the run's counters. */
+mg_status mg_part_bfs_result(mg_part *p, int32_t *depth, int32_t device_output, mg_stats *stats);
 
 #ifdef __cplusplus
 }

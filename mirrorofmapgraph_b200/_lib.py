@@ -51,6 +51,11 @@ class MgPrOpts(C.Structure):
                 ("autotune", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
+class MgPartLevel(C.Structure):
+    _fields_ = [("frontier", C.c_int64), ("frontier_edges", C.c_int64), ("level", C.c_int32),
+                ("done", C.c_int32), ("direction", C.c_int32), ("reserved", C.c_int32)]
+
+
 class MgHostCsr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("row_offsets", C.POINTER(C.c_int32)),
                 ("col_idx", C.POINTER(C.c_int32)), ("weights_i32", C.POINTER(C.c_int32)),
@@ -96,6 +101,15 @@ SIGNATURES = {
     "mg_save_csr": (C.c_int, [C.c_char_p, C.POINTER(MgHostCsr)]),
     "mg_load_csr": (C.c_int, [C.c_char_p, C.POINTER(MgHostCsr)]),
     "mg_host_csr_to_csc": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
+    "mg_part_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, C.c_uint32,
+                                 C.POINTER(_P)]),
+    "mg_part_destroy": (C.c_int, [_P]),
+    "mg_part_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "mg_part_words": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "mg_part_bfs_begin": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgOpts), C.POINTER(MgPartLevel)]),
+    "mg_part_bfs_step": (C.c_int, [_P, _P]),
+    "mg_part_bfs_merge": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgPartLevel)]),
+    "mg_part_bfs_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
 }
 
 _lib = None

@@ -425,7 +425,7 @@ static mg_status msbfs_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32
                                    sizeof(uint64_t) * (size_t)n, sizeof(uint64_t) * (size_t)n,
                                    sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n,
                                    sizeof(int32_t) * (size_t)BIG_CAP, sizeof(int32_t) * (size_t)nsrc});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   MsArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -536,7 +536,7 @@ extern "C" mg_status mg_bfs_batch(mg_graph *g, const int32_t *srcs, int32_t nsrc
   const size_t bytes = sizeof(int32_t) * (size_t)nsrc * (size_t)g->n;
   int32_t *out = depth;
   if (!o.device_output) {
-    MG_TRY(ws_reserve(g->ws_out, bytes + 256));
+    MG_TRY(ws_reserve(g, g->ws_out, bytes + 256));
     out = (int32_t *)g->ws_out.ptr;
   }
   MG_TRY(msbfs_run(g, srcs, nsrc, out, o, stats));

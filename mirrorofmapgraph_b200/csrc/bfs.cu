@@ -68,6 +68,7 @@ __device__ void bfs_level_end(const BfsArgs &a) {
   const int64_t vdeg = vload(&c->visited_deg) + mf;
   const int lvl = vload(&c->level) + 1;
   c->visited_deg = vdeg;
+  c->mf_front = mf;
   c->level = lvl;
   c->qlen[cur] = 0;
   c->cur = cur ^ 1;
@@ -164,6 +165,122 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
     if (bmf) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)bmf);
     if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
     if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
+  }
+}
+
+// Persistent push levels for small frontiers (high-diameter graphs such as
+// lattices, where a BFS has thousands of levels of a few thousand vertices and
+// per-level launches dominate). One cooperative launch runs level after level,
+// with a grid barrier between the expansion and the level end, while the level is
+// a push level with at most PERSIST_MAX frontier vertices and PERSIST_EDGES
+// frontier out-edges; it then returns and the per-level kernels continue from the
+// same control block. Vertices of GRID_TH or more edges are deferred as in the
+// per-level push and expanded by the whole grid after a second barrier, which
+// only levels that deferred one take.
+constexpr int32_t PERSIST_MAX = 1 << 16;
+constexpr int64_t PERSIST_EDGES = 1 << 17;  // frontier out-edges
+constexpr unsigned long long PERSIST_WAIT = 1ull << 22;  // barrier polls (seconds at most) before giving up
+
+__global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
+  // The tile pass and the grid-strided pass are separated by a grid barrier.
+  __shared__ union {
+    ExpandSmem<BFS_NT> e;
+    BigSmem<BFS_NT> b;
+  } sm;
+  __shared__ int64_t s_sum[BFS_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  // Entry state, as the seed kernel or the last per-level kernel left it; every
+  // block reads the same values and then takes the same decisions level by level.
+  const int32_t l0 = vload(&c->level);
+  int32_t lvl = l0, sel = vload(&c->cur);
+  int32_t nin = vload(&c->qlen[sel]);
+  int64_t mf = vload(&c->mf_front), vdeg = vload(&c->visited_deg);
+  const int32_t iter_cap = vload(&c->iter_cap);
+  if (vload(&c->done) || vload(&c->dir) != 0 || nin > PERSIST_MAX || mf > PERSIST_EDGES) return;
+  for (;;) {
+    // Per-level counters rotate over three slots: this level appends to `out`;
+    // `zero` is the slot the next level appends to (nobody touches it now).
+    const int out = (lvl - l0 + 1) % 3, zero = (lvl - l0 + 2) % 3;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      c->pq[zero] = 0;
+      c->pm[zero] = 0;
+      c->pb[zero] = 0;
+    }
+    const int32_t *qin = sel ? a.q1 : a.q0;
+    PushCtx x{a.label, a.vis, a.ro, sel ? a.q0 : a.q1, &c->pq[out], &c->overflow, a.qcap, lvl, 0};
+    const BigList big{a.big_v, &c->pb[out]};
+    const int32_t *ci = a.ci, *ri = a.ri;
+    int64_t insp = 0, nexp = 0;
+    for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
+      const int64_t i = tile + threadIdx.x;
+      const int32_t v = i < nin ? qin[i] : -1;
+      nexp += v >= 0;
+      expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big);
+      if (a.both)
+        expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
+    }
+    const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
+    const int64_t bins = block_sum<BFS_NT>(insp, s_sum);
+    const int64_t bexp = block_sum<BFS_NT>(nexp, s_sum);
+    if (threadIdx.x == 0) {
+      if (bmf) atomicAdd((unsigned long long *)&c->pm[out], (unsigned long long)bmf);
+      if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
+      if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
+    }
+    if (!grid_barrier(&c->bar_count, &c->bar_gen, PERSIST_WAIT)) {
+      if (threadIdx.x == 0) {
+        c->status = MG_ERR_TIMEOUT;
+        c->done = 1;
+      }
+      return;
+    }
+    if (vload(&c->pb[out]) > 0) {
+      // The deferred vertices' edges, spread over the whole grid.
+      x.mf = 0;
+      expand_big<BFS_NT>(sm.b, a.ro, big, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+      const int64_t bmf2 = block_sum<BFS_NT>(x.mf, s_sum);
+      if (threadIdx.x == 0 && bmf2) atomicAdd((unsigned long long *)&c->pm[out], (unsigned long long)bmf2);
+      if (!grid_barrier(&c->bar_count, &c->bar_gen, PERSIST_WAIT)) {
+        if (threadIdx.x == 0) {
+          c->status = MG_ERR_TIMEOUT;
+          c->done = 1;
+        }
+        return;
+      }
+    }
+    // Level end (bfs_level_end's rules), computed alike in every block.
+    const int32_t nf = vload(&c->pq[out]);
+    mf = vload(&c->pm[out]);
+    vdeg += mf;
+    lvl += 1;
+    sel ^= 1;
+    const bool over = vload(&c->overflow) != 0;
+    const bool done = nf == 0 || lvl >= iter_cap || over;
+    int dir = 0;
+    if (a.mode == MG_DIR_PULL) dir = a.can_pull ? 1 : 0;
+    else if (a.mode == MG_DIR_AUTO && a.can_pull && mf > (a.m_total - vdeg) / BEAMER_ALPHA) dir = 1;
+    if (done || dir != 0 || nf > PERSIST_MAX || mf > PERSIST_EDGES) {
+      // Hand over to the per-level kernels (or finish) with their control state.
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->level = lvl;
+        c->cur = sel;
+        c->qlen[sel] = nf;
+        c->qlen[sel ^ 1] = 0;
+        c->visited_deg = vdeg;
+        c->mf_front = mf;
+        c->mf_next = 0;
+        c->blocks_done = 0;
+        c->big_len = 0;
+        c->nf_next = nf;
+        c->dir = dir;
+        if (dir == 1 && !done) c->levels_pull += 1;
+        if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+        __threadfence();
+        c->done = done ? 1 : 0;
+      }
+      return;
+    }
+    nin = nf;
   }
 }
 
@@ -282,6 +399,7 @@ __global__ void bfs_seed_kernel(BfsArgs a, const int32_t *srcs, int32_t nsrc, in
   const int64_t t = block_sum<1024>(mf, s_sum);
   if (threadIdx.x == 0) {
     c->visited_deg = t;
+    c->mf_front = t;
     c->level = 0;
     c->cur = 0;
     c->dir = dir0;
@@ -292,6 +410,17 @@ __global__ void bfs_seed_kernel(BfsArgs a, const int32_t *srcs, int32_t nsrc, in
 }
 
 }  // namespace mg
+
+// Blocks of the persistent kernel: every SM's resident share (0 when the
+// occupancy query fails).
+static int persist_grid(mg_graph *g) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::bfs_persist_kernel, mg::BFS_NT, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return occ > 0 ? g->num_sms * std::min(occ, 4) : 0;
+}
 
 extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth, const mg_opts *opts,
                             mg_stats *stats) {
@@ -329,7 +458,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   const size_t need = Carve::need({sizeof(int32_t) * (size_t)n, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
                                    sizeof(int32_t) * (size_t)nsrc, sizeof(int32_t) * (size_t)BIG_CAP});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   int32_t *label_ws = cv.take<int32_t>(n);
   uint32_t *vis = cv.take<uint32_t>(nwords);
@@ -367,6 +496,18 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   bfs_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(label, vis, n);
   bfs_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap, 0);
   MG_CUDA_TRY(cudaGetLastError());
+  // Small push levels first, in one persistent cooperative launch (all blocks
+  // resident); a device that cannot co-schedule the grid skips it.
+  const int pgrid = persist_grid(g);
+  int64_t persist_launches = 0;
+  if (pgrid > 0 && o.direction != MG_DIR_PULL) {
+    BfsArgs pa = a;
+    void *params[] = {&pa};
+    if (cudaLaunchCooperativeKernel((const void *)bfs_persist_kernel, dim3(pgrid), dim3(BFS_NT), params, 0, s) ==
+        cudaSuccess)
+      persist_launches = 1;
+    cudaGetLastError();
+  }
 
   const int grid = g->num_sms * 4;
   const bool use_graph = o.use_graph >= 0;
@@ -401,7 +542,11 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
     stats->status_detail = hc.levels_pull;
-    stats->launches = 2 + (use_graph ? 4 * (int64_t)hc.body_iters : 3 * (int64_t)hc.level);
+    stats->launches = 2 + persist_launches + (use_graph ? 4 * (int64_t)hc.body_iters : 3 * (int64_t)hc.level);
+  }
+  if (hc.status == MG_ERR_TIMEOUT) {
+    mg_set_error("mg_bfs: a grid barrier of the persistent levels timed out");
+    return MG_ERR_TIMEOUT;
   }
   if (hc.status != 0) {
     mg_set_error("mg_bfs: frontier exceeded queue capacity %d", qcap);
@@ -630,7 +775,7 @@ extern "C" mg_status mg_bfs_predecessors(mg_graph *g, const int32_t *depth, int3
   const int32_t *dlabel = depth;
   int32_t *dpred = pred;
   if (!dev_io) {
-    MG_TRY(ws_reserve(g->ws_out, Carve::need({sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n})));
+    MG_TRY(ws_reserve(g, g->ws_out, Carve::need({sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n})));
     Carve cv(g->ws_out.ptr);
     int32_t *l = cv.take<int32_t>(n);
     dpred = cv.take<int32_t>(n);

@@ -192,7 +192,7 @@ extern "C" mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_
   MG_TRY(graph_enter(g));
   const int64_t n = g->n;
   const size_t need = Carve::need({sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n, 64});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   int32_t *parent = cv.take<int32_t>(n);
   int32_t *lab_ws = cv.take<int32_t>(n);

@@ -87,6 +87,39 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
   return s_last;
 }
 
+// Grid-wide barrier for kernels whose blocks are all resident (cooperative
+// launch): arrivals are counted in *count and the last block bumps *gen. The
+// wait is bounded: after `limit` polls the block gives up and the function
+// returns false (the caller reports MG_ERR_TIMEOUT and stops), so a missing
+// block cannot hang the GPU. Every thread of every block must call it.
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned long long limit) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = *(volatile unsigned *)gen;  // read before arriving: gen moves only after every arrival
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(count, 1u) + 1 == gridDim.x) {
+      *count = 0;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      unsigned long long it = 0;
+      while (*(volatile unsigned *)gen == g) {
+        if (++it > limit) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // Warp-aggregated append of `item` to `queue` (capacity `cap`) for every active
 // lane with `pred` set; the queue length lives at *len. Lanes whose slot lands
 // past the capacity set *overflow instead of writing.

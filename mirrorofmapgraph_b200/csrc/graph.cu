@@ -31,25 +31,47 @@ void mg_set_error(const char *fmt, ...) {
   va_end(ap);
 }
 
-mg_status ws_reserve(Workspace &w, size_t bytes) {
+mg_status dev_alloc(mg_graph *g, void **p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), g->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    // Return the pool's idle blocks to the driver and try once more.
+    cudaGetLastError();
+    cudaMemPool_t pool;
+    if (cudaStreamSynchronize(g->stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+    e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), g->stream);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    mg_set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? MG_ERR_OOM : MG_ERR_CUDA;
+  }
+  return MG_OK;
+}
+
+void dev_free(mg_graph *g, void *p) {
+  if (p) cudaFreeAsync(p, g->stream);
+}
+
+mg_status ws_reserve(mg_graph *g, Workspace &w, size_t bytes) {
   if (w.bytes >= bytes) return MG_OK;
-  if (w.ptr) cudaFree(w.ptr);
+  dev_free(g, w.ptr);
   w.ptr = nullptr;
+  const size_t grown = std::max(bytes, w.bytes + w.bytes / 4);
   w.bytes = 0;
-  size_t want = std::max(bytes, w.bytes + w.bytes / 4);
-  cudaError_t e = cudaMalloc(&w.ptr, want);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    e = cudaMalloc(&w.ptr, bytes);
-    want = bytes;
+  if (dev_alloc(g, &w.ptr, grown) != MG_OK) {
+    mg_status st = dev_alloc(g, &w.ptr, bytes);
+    if (st != MG_OK) {
+      mg_set_error("workspace allocation of %zu bytes failed", bytes);
+      return st;
+    }
+    w.bytes = bytes;
+    return MG_OK;
   }
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    w.ptr = nullptr;
-    mg_set_error("workspace allocation of %zu bytes failed", bytes);
-    return MG_ERR_OOM;
-  }
-  w.bytes = want;
+  w.bytes = grown;
   return MG_OK;
 }
 
@@ -410,7 +432,7 @@ static mg_status build_csc(mg_graph *g) {
                                    sizeof(int64_t) * (size_t)ntiles, sizeof(int32_t) * 3 * (size_t)(n + 1),
                                    sizeof(int32_t) * 4, sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1),
                                    sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)});
-  MG_TRY(ws_reserve(g->ws_aux, need));
+  MG_TRY(ws_reserve(g, g->ws_aux, need));
   Carve cv(g->ws_aux.ptr);
   int32_t *cnt = cv.take<int32_t>(n + 1);
   int32_t *cursor = cv.take<int32_t>(n + 1);
@@ -440,6 +462,34 @@ static mg_status build_csc(mg_graph *g) {
   return MG_OK;
 }
 
+// Pinned host mirrors of the control blocks, recycled across graphs: pinning
+// and unpinning host memory costs a driver round trip each time.
+static std::mutex g_pinned_mu;
+static std::vector<void *> g_pinned_free;
+
+static DevCtl *pinned_ctl_get() {
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    if (!g_pinned_free.empty()) {
+      void *p = g_pinned_free.back();
+      g_pinned_free.pop_back();
+      return static_cast<DevCtl *>(p);
+    }
+  }
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, sizeof(DevCtl) + 64, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return static_cast<DevCtl *>(p);
+}
+
+static void pinned_ctl_put(DevCtl *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  g_pinned_free.push_back(p);
+}
+
 static void graph_free_device(mg_graph *g) {
   cudaStream_t s = g->stream;
   auto fr = [&](void *p) {
@@ -454,12 +504,13 @@ static void graph_free_device(mg_graph *g) {
     fr(g->perm);
     fr(g->cvals);
   }
+  fr(g->ws_main.ptr);
+  fr(g->ws_aux.ptr);
+  fr(g->ws_out.ptr);
+  fr(g->ctl);
   if (s) cudaStreamSynchronize(s);
-  if (g->ws_main.ptr) cudaFree(g->ws_main.ptr);
-  if (g->ws_aux.ptr) cudaFree(g->ws_aux.ptr);
-  if (g->ws_out.ptr) cudaFree(g->ws_out.ptr);
-  if (g->ctl) cudaFree(g->ctl);
-  if (g->ctl_host) cudaFreeHost(g->ctl_host);
+  pinned_ctl_put(g->ctl_host);
+  g->ctl_host = nullptr;
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   if (s) cudaStreamDestroy(s);
@@ -561,8 +612,12 @@ static mg_status create_impl(const int32_t *row_offsets, const int32_t *col_idx,
   CREATE_TRY(cudaMemcpyAsync(g->ro, row_offsets, sizeof(int32_t) * (n + 1), kind, s));
   if (m > 0) CREATE_TRY(cudaMemcpyAsync(g->ci, col_idx, sizeof(int32_t) * m, kind, s));
   if (vb && m > 0) CREATE_TRY(cudaMemcpyAsync(g->vals, edge_vals, vb * m, kind, s));
-  CREATE_TRY(cudaMalloc((void **)&g->ctl, sizeof(DevCtl) + 64));
-  CREATE_TRY(cudaMallocHost((void **)&g->ctl_host, sizeof(DevCtl) + 64));
+  if (dev_alloc(g, (void **)&g->ctl, sizeof(DevCtl) + 64) != MG_OK) return fail(MG_ERR_OOM);
+  g->ctl_host = pinned_ctl_get();
+  if (!g->ctl_host) {
+    mg_set_error("mg_graph_create: pinned host allocation failed");
+    return fail(MG_ERR_OOM);
+  }
   CREATE_TRY(cudaEventCreate(&g->ev0));
   CREATE_TRY(cudaEventCreate(&g->ev1));
   // Validate on the device.

@@ -63,6 +63,14 @@ struct DevCtl {
   int32_t split;
   int32_t far_min;
   int32_t splits;
+  int64_t mf_front;          // out-edges of the current frontier (BFS)
+  // persistent kernels: per-level counters in a ring of three (frontier out-edges,
+  // frontier sizes), and the grid barrier (arrivals, generation)
+  int64_t pm[3];
+  int32_t pq[3];
+  int32_t pb[3];  // deferred big vertices per level (persistent BFS)
+  uint32_t bar_count;
+  uint32_t bar_gen;
 };
 
 // Padding of the device graph arrays. Offsets arrays hold n + 1 + MG_OFF_PAD
@@ -109,8 +117,15 @@ struct mg_graph {
   void *cache = nullptr;       // cached executable loop graphs (engine.cu)
 };
 
+// Device memory of a graph's workspaces and plans, taken from the device's
+// stream-ordered pool on the graph's stream: freed blocks stay in the pool, so a
+// new graph of the same size reuses them without a driver allocation or a
+// device-wide synchronisation.
+mg_status dev_alloc(mg_graph *g, void **p, size_t bytes);
+void dev_free(mg_graph *g, void *p);
+
 // Grows a workspace to at least `bytes` (contents are not preserved).
-mg_status ws_reserve(Workspace &w, size_t bytes);
+mg_status ws_reserve(mg_graph *g, Workspace &w, size_t bytes);
 
 // Carves aligned sub-buffers out of a workspace.
 struct Carve {

@@ -72,16 +72,15 @@ void pr_release_plans(mg_graph *g) {
   if (!g->plan_csc) return;
   mg::PlanSet *ps = static_cast<mg::PlanSet *>(g->plan_csc);
   for (mg::GatherPlan *p : {&ps->csc, &ps->csr}) {
-    if (p->tx) cudaFree(p->tx);
-    if (p->ty) cudaFree(p->ty);
+    dev_free(g, p->tx);
+    dev_free(g, p->ty);
   }
   for (mg::BinPlan *b : {&ps->bcsc, &ps->bcsr}) {
     for (void *q : {(void *)b->rows, (void *)b->hrows, (void *)b->hbase, (void *)b->hcount, (void *)b->hpart,
                     (void *)b->hcontrib})
-      if (q) cudaFree(q);
+      dev_free(g, q);
   }
-  for (void *q : {(void *)ps->hubs.cidx, (void *)ps->hubs.slot, (void *)ps->hubs.hv})
-    if (q) cudaFree(q);
+  for (void *q : {(void *)ps->hubs.cidx, (void *)ps->hubs.slot, (void *)ps->hubs.hv}) dev_free(g, q);
   delete ps;
   g->plan_csc = nullptr;
 }
@@ -94,8 +93,8 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
     const int64_t items = g->n + g->m;
     const int64_t nt = (items + PRG_IPC - 1) / PRG_IPC;
     p.ntiles = (int32_t)std::max<int64_t>(nt, 1);
-    MG_CUDA_TRY(cudaMalloc((void **)&p.tx, sizeof(int32_t) * (p.ntiles + 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&p.ty, sizeof(int32_t) * (p.ntiles + 1)));
+    MG_TRY(dev_alloc(g, (void **)&p.tx, sizeof(int32_t) * (p.ntiles + 1)));
+    MG_TRY(dev_alloc(g, (void **)&p.ty, sizeof(int32_t) * (p.ntiles + 1)));
     prg_plan_kernel<<<(p.ntiles + 256) / 256, 256, 0, g->stream>>>(csr ? g->ro : g->co, g->n, g->m, p.ntiles, p.tx,
                                                                     p.ty);
     MG_CUDA_TRY(cudaGetLastError());
@@ -141,12 +140,12 @@ static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
       else w += bp.ntasks;
     }
     bp.wstart[PRB_BINS] = w;
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.rows, sizeof(int32_t) * std::max<int64_t>(acc, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.hrows, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.hbase, sizeof(int32_t) * (bp.nheavy + 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.hcount, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.hpart, sizeof(Comp) * std::max<int64_t>(bp.ntasks, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.rows, sizeof(int32_t) * std::max<int64_t>(acc, 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.hrows, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.hbase, sizeof(int32_t) * (bp.nheavy + 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.hcount, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.hpart, sizeof(Comp) * std::max<int64_t>(bp.ntasks, 1)));
+    MG_TRY(dev_alloc(g, (void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
     MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
     MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
     prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows);
@@ -392,7 +391,7 @@ __global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) solve_binned_kernel(So
 // One whole iteration of the degree-binned solver with the column cache: every
 // CTA first copies the cached columns' gathered values into shared memory.
 #ifndef PRB_HUB_THREADS
-#define PRB_HUB_THREADS 768
+#define PRB_HUB_THREADS 640
 #endif
 #ifndef PRB_HUB_MINB
 #define PRB_HUB_MINB 2
@@ -401,6 +400,12 @@ __global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) solve_binned_kernel(So
 // uncached gathers (20480 columns = 80 KB per CTA measured best on R-MAT s22).
 #ifndef PRB_HUB_CAP
 #define PRB_HUB_CAP 20480
+#endif
+// Rounds of the warp-per-row gather sized to the row's tail (prb_warp_range's
+// ADAPT) in the column-cache kernel. Measured on R-MAT s22 (us per iteration):
+// 640 threads with ADAPT 591, 768 with ADAPT 628, 768 without 599, 640 without 774.
+#ifndef PRB_HUB_ADAPT
+#define PRB_HUB_ADAPT true
 #endif
 constexpr int PRB_HUB_NT = PRB_HUB_THREADS;
 
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
     p.hcontrib[2 * h + 1] = hu.red2;
     __threadfence();
   };
-  prb_run<WEIGHTED>(p, [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); }, up,
+  prb_run<WEIGHTED, PRB_HUB_ADAPT>(p, [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); }, up,
                     hub);
   const double r = block_sum<PRB_HUB_NT>(up.resid, s_red);
   const double d = block_sum<PRB_HUB_NT>(up.red2, s_red);
@@ -654,8 +659,7 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
   using namespace mg;
   HubCache &hc = plans_of(g)->hubs;
   if (hc.ok && hc.cap != cap) {  // rebuilt for another capacity
-    for (void *q : {(void *)hc.cidx, (void *)hc.slot, (void *)hc.hv})
-      if (q) cudaFree(q);
+    for (void *q : {(void *)hc.cidx, (void *)hc.slot, (void *)hc.hv}) dev_free(g, q);
     hc = HubCache();
   }
   if (!hc.ok) {
@@ -675,9 +679,9 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
       cum += h[d];
       thr = d;
     }
-    MG_CUDA_TRY(cudaMalloc((void **)&hc.slot, sizeof(int32_t) * std::max<int64_t>(n, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&hc.hv, sizeof(int32_t) * std::max<int64_t>(cap, 1)));
-    MG_CUDA_TRY(cudaMalloc((void **)&hc.cidx, sizeof(int32_t) * (m + 8)));
+    MG_TRY(dev_alloc(g, (void **)&hc.slot, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    MG_TRY(dev_alloc(g, (void **)&hc.hv, sizeof(int32_t) * std::max<int64_t>(cap, 1)));
+    MG_TRY(dev_alloc(g, (void **)&hc.cidx, sizeof(int32_t) * (m + 8)));
     unsigned *count = hist + 65536;
     hub_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(g->ro, n, thr, cap, hc.slot, hc.hv, count);
     hub_remap_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ri, m, hc.slot, hc.cidx);
@@ -714,7 +718,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
                              const float *wvec_src, int variant, SolvePlan &sp, int32_t hub_cap = -1) {
   using namespace mg;
   const bool use_tma = variant == 1;
-  const bool use_hub = variant == 0 && !adjoint && g->n > 0;
+  const bool use_hub = variant == 2 && !adjoint && g->n > 0;
   GatherPlan *plan = nullptr;
   BinPlan *bins = nullptr, *rbins = nullptr;
   HubCache *hubs = nullptr;
@@ -753,7 +757,7 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
                                    sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp,
                                    sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0),
                                    sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0)});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   a.v0 = cv.take<float>(np);
   a.v1 = cv.take<float>(np);
@@ -1073,7 +1077,7 @@ static mg_status pagerank_refcompat(mg_graph *g, float *ranks, const mg_pr_opts 
   const int64_t nwords = (n + 31) / 32;
   const size_t need = Carve::need({4 * (size_t)n, 4 * (size_t)n, 4 * (size_t)n, (size_t)n, 4 * (size_t)nwords,
                                    4 * (size_t)nwords, 4 * (size_t)n, 4 * (size_t)n});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   RefArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -1164,7 +1168,7 @@ static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opt
     float ms = 0.f;
     for (int rep = 0; rep < 2; rep++) {
       SolvePlan sp;
-      MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, c > 0 ? 0 : 2, sp, c > 0 ? c : -1));
+      MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, c > 0 ? 2 : 0, sp, c > 0 ? c : -1));
       SolveArgs &a = sp.a;
       a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
       a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -1202,8 +1206,10 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
   if (o.gather_kernel == 0 && o.autotune && ps->tuned_cap < 0) MG_TRY(pr_autotune(g, tele_dev, o));
   int variant = o.gather_kernel;
   int32_t cap = -1;
-  if (variant == 0 && ps->tuned_cap == 0) variant = 2;
-  else if (variant == 0 && ps->tuned_cap > 0) cap = ps->tuned_cap;
+  if (variant == 0 && ps->tuned_cap > 0) {  // the autotuner chose a column cache
+    variant = 2;
+    cap = ps->tuned_cap;
+  }
   SolvePlan sp;
   MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, variant, sp, cap));
   SolveArgs &a = sp.a;
@@ -1305,7 +1311,7 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
                                    sizeof(int32_t) * (size_t)std::max<int64_t>(nheavy, 1),
                                    sizeof(double) * 2 * W * (size_t)std::max<int64_t>(nheavy, 1),
                                    out_is_device ? 0 : sizeof(float) * (size_t)kmax * n});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   PprArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -1452,7 +1458,7 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
   if (teleport) {
     if (o.device_output) tele_dev = const_cast<float *>(teleport);
     else {
-      MG_TRY(ws_reserve(g->ws_out, sizeof(float) * (size_t)n * nvec + 256));
+      MG_TRY(ws_reserve(g, g->ws_out, sizeof(float) * (size_t)n * nvec + 256));
       tele_dev = (float *)g->ws_out.ptr;
       MG_CUDA_TRY(cudaMemcpyAsync(tele_dev, teleport, sizeof(float) * n * nvec, cudaMemcpyHostToDevice, g->stream));
     }
@@ -1581,7 +1587,7 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
   // Inputs staged on the device.
   const float *x_dev = ranks, *w_dev = dL_dranks, *t_dev = teleport;
   if (!o.device_output) {
-    MG_TRY(ws_reserve(g->ws_out, Carve::need({4 * (size_t)n, 4 * (size_t)n, 4 * (size_t)n})));
+    MG_TRY(ws_reserve(g, g->ws_out, Carve::need({4 * (size_t)n, 4 * (size_t)n, 4 * (size_t)n})));
     Carve cv(g->ws_out.ptr);
     float *xs = cv.take<float>(n), *ws = cv.take<float>(n), *ts = cv.take<float>(n);
     MG_CUDA_TRY(cudaMemcpyAsync(xs, ranks, 4 * n, cudaMemcpyHostToDevice, s));
@@ -1593,7 +1599,7 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
   }
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
   SolvePlan sp;
-  MG_TRY(solve_setup(g, true, weighted, t_dev, w_dev, o.gather_kernel == 1 ? 1 : 0, sp));
+  MG_TRY(solve_setup(g, true, weighted, t_dev, w_dev, o.gather_kernel == 1 ? 1 : 0, sp));  // no cache in the adjoint
   SolveArgs &a = sp.a;
   a.tn = n > 0 ? 1.0 / (double)n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -1606,7 +1612,7 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
   const float *lam = hc.cur ? a.v1 : a.v0;
   // Per-row products and gradients (scratch in ws_aux).
   const int nparts = g->num_sms * 4;
-  MG_TRY(ws_reserve(g->ws_aux, Carve::need({8 * (size_t)n, 8 * (size_t)n, 8 * (size_t)nparts, 4 * (size_t)m,
+  MG_TRY(ws_reserve(g, g->ws_aux, Carve::need({8 * (size_t)n, 8 * (size_t)n, 8 * (size_t)nparts, 4 * (size_t)m,
                                             4 * (size_t)n})));
   Carve cv(g->ws_aux.ptr);
   double *pl = cv.take<double>(n), *coef = cv.take<double>(n), *part = cv.take<double>(nparts);

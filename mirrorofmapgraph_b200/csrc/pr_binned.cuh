@@ -217,23 +217,53 @@ __device__ __forceinline__ void group_comp_reduce(Comp &c) {
   }
 }
 
-// One warp reduces edges [b, e) of a row: 4 independent loads in flight per lane.
-template <bool WEIGHTED, typename Gather>
+// U strides of 32 edges of a row from `base` (warp-uniform); CHECK predicates
+// each slot on the row end (the last round of a row).
+template <bool WEIGHTED, int U, bool CHECK, typename Gather>
+__device__ __forceinline__ void prb_round(const PrbArgs &p, int32_t base, int32_t e, Gather &gather, Comp &acc) {
+  const int32_t k = base + (threadIdx.x & 31);
+  int32_t c[U];
+  float x[U];
+#pragma unroll
+  for (int j = 0; j < U; j++) c[j] = (!CHECK || k + 32 * j < e) ? prb_stream(p.idx + k + 32 * j) : 0;
+#pragma unroll
+  for (int j = 0; j < U; j++) x[j] = (!CHECK || k + 32 * j < e) ? gather(c[j]) : 0.f;
+#pragma unroll
+  for (int j = 0; j < U; j++)
+    if (!CHECK || k + 32 * j < e) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
+}
+
+// One warp reduces edges [b, e) of a row in rounds of PRB_UNROLL strides of 32
+// edges (all loads of a round in flight together). ADAPT: full rounds run without
+// per-slot checks and the last round is sized to what is left (8, 4, 2 or 1
+// strides), so short rows do not pay for idle slots; otherwise each lane walks
+// its own edges in full predicated rounds (fewer code paths, which suits some
+// register-tight launch shapes).
+template <bool WEIGHTED, bool ADAPT, typename Gather>
 __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int32_t e, Gather &gather) {
-  const int lane = threadIdx.x & 31;
   Comp acc{0.f, 0.f};
-  // PRB_UNROLL strides of 32 edges per round, predicated: a row of up to
-  // 32 * PRB_UNROLL edges costs one index and one gather round trip.
-  for (int32_t k = b + lane; k < e; k += 32 * PRB_UNROLL) {
-    int32_t c[PRB_UNROLL];
-    float x[PRB_UNROLL];
+  if (ADAPT) {
+    int32_t base = b;
+    for (; base + 32 * PRB_UNROLL <= e; base += 32 * PRB_UNROLL)
+      prb_round<WEIGHTED, PRB_UNROLL, false>(p, base, e, gather, acc);
+    const int32_t rem = e - base;
+    if (rem > 128) prb_round<WEIGHTED, PRB_UNROLL, true>(p, base, e, gather, acc);
+    else if (rem > 64) prb_round<WEIGHTED, 4, true>(p, base, e, gather, acc);
+    else if (rem > 32) prb_round<WEIGHTED, 2, true>(p, base, e, gather, acc);
+    else if (rem > 0) prb_round<WEIGHTED, 1, true>(p, base, e, gather, acc);
+  } else {
+    // per-lane loop: a lane stops after its last edge
+    for (int32_t k = b + (threadIdx.x & 31); k < e; k += 32 * PRB_UNROLL) {
+      int32_t c[PRB_UNROLL];
+      float x[PRB_UNROLL];
 #pragma unroll
-    for (int j = 0; j < PRB_UNROLL; j++) c[j] = k + 32 * j < e ? prb_stream(p.idx + k + 32 * j) : 0;
+      for (int j = 0; j < PRB_UNROLL; j++) c[j] = k + 32 * j < e ? prb_stream(p.idx + k + 32 * j) : 0;
 #pragma unroll
-    for (int j = 0; j < PRB_UNROLL; j++) x[j] = k + 32 * j < e ? gather(c[j]) : 0.f;
+      for (int j = 0; j < PRB_UNROLL; j++) x[j] = k + 32 * j < e ? gather(c[j]) : 0.f;
 #pragma unroll
-    for (int j = 0; j < PRB_UNROLL; j++)
-      if (k + 32 * j < e) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
+      for (int j = 0; j < PRB_UNROLL; j++)
+        if (k + 32 * j < e) prb_add<WEIGHTED>(acc, x[j], p.wts, k + 32 * j);
+    }
   }
   group_comp_reduce<32>(acc);
   return acc;
@@ -246,7 +276,7 @@ __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int3
 // waits for three memory round trips per assignment rather than three per pass.
 // The sum of slot l ends up in lane l, whose row is returned in *my_row (-1 past
 // the bin), so the row updates then run on all lanes at once.
-template <int G, bool WEIGHTED, typename Gather>
+template <int G, bool WEIGHTED, bool ADAPT, typename Gather>
 __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa, Gather &gather, int32_t *my_row) {
   constexpr int RPP = 32 / G;  // rows per pass
   const int lane = threadIdx.x & 31;
@@ -260,7 +290,7 @@ __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa
 #pragma unroll 1
     for (int q = 0; q < 32; q++) {
       const int32_t b = __shfl_sync(0xffffffffu, mb, q), e = __shfl_sync(0xffffffffu, me, q);
-      const Comp acc = prb_warp_range<WEIGHTED>(p, b, e, gather);
+      const Comp acc = prb_warp_range<WEIGHTED, ADAPT>(p, b, e, gather);
       if (lane == q) mine = acc;
     }
   } else {
@@ -298,7 +328,7 @@ __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa
 
 // Walks every assignment of the plan with a persistent grid (fixed stride).
 // finish(row, Comp) consumes a row sum; finish_hub(h, row, Comp) consumes a hub's.
-template <bool WEIGHTED, typename Gather, typename Finish, typename FinishHub>
+template <bool WEIGHTED, bool ADAPT = true, typename Gather, typename Finish, typename FinishHub>
 __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finish &&finish, FinishHub &&finish_hub) {
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t total = p.wstart[PRB_BINS];
@@ -314,12 +344,12 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
       int32_t row = -1;
       Comp acc;
       switch (bin) {
-        case 0: acc = prb_rows32<1, WEIGHTED>(p, 0, wa, gather, &row); break;
-        case 1: acc = prb_rows32<2, WEIGHTED>(p, 1, wa, gather, &row); break;
-        case 2: acc = prb_rows32<4, WEIGHTED>(p, 2, wa, gather, &row); break;
-        case 3: acc = prb_rows32<8, WEIGHTED>(p, 3, wa, gather, &row); break;
-        case 4: acc = prb_rows32<16, WEIGHTED>(p, 4, wa, gather, &row); break;
-        default: acc = prb_rows32<32, WEIGHTED>(p, 5, wa, gather, &row); break;
+        case 0: acc = prb_rows32<1, WEIGHTED, ADAPT>(p, 0, wa, gather, &row); break;
+        case 1: acc = prb_rows32<2, WEIGHTED, ADAPT>(p, 1, wa, gather, &row); break;
+        case 2: acc = prb_rows32<4, WEIGHTED, ADAPT>(p, 2, wa, gather, &row); break;
+        case 3: acc = prb_rows32<8, WEIGHTED, ADAPT>(p, 3, wa, gather, &row); break;
+        case 4: acc = prb_rows32<16, WEIGHTED, ADAPT>(p, 4, wa, gather, &row); break;
+        default: acc = prb_rows32<32, WEIGHTED, ADAPT>(p, 5, wa, gather, &row); break;
       }
       if (row >= 0) finish(row, acc);
       continue;
@@ -338,7 +368,7 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
         const int32_t rb = __ldg(p.off + row);
         const int32_t b = rb + chunk * PRB_CHUNK;
         const int32_t e = min(b + PRB_CHUNK, __ldg(p.off + row + 1));
-        const Comp acc = prb_warp_range<WEIGHTED>(p, b, e, gather);
+        const Comp acc = prb_warp_range<WEIGHTED, ADAPT>(p, b, e, gather);
         bool last = false;
         if (lane == 0) {
           p.hpart[wa] = acc;

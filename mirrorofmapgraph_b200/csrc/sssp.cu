@@ -408,7 +408,7 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
                                    sizeof(int32_t) * (size_t)nseed, sizeof(int32_t) * (size_t)BIG_CAP,
                                    sizeof(int32_t) * far_items, sizeof(int32_t) * far_items,
                                    sizeof(uint32_t) * (delta > 0 ? (size_t)nwords : 0)});
-  MG_TRY(ws_reserve(g->ws_main, need));
+  MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   SsspArgs a;
   a.inq0 = cv.take<uint32_t>(nwords);
@@ -511,7 +511,7 @@ extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int
   MG_TRY(graph_enter(g));
   int32_t *out = dist;
   if (!o.device_output) {
-    MG_TRY(ws_reserve(g->ws_out, sizeof(int32_t) * (size_t)g->n + 256));
+    MG_TRY(ws_reserve(g, g->ws_out, sizeof(int32_t) * (size_t)g->n + 256));
     out = (int32_t *)g->ws_out.ptr;
   }
   MG_TRY(sssp_run(g, srcs, nsrc, out, o, stats));
@@ -555,7 +555,7 @@ extern "C" mg_status mg_sssp_batch(mg_graph *g, const int32_t *srcs, int32_t nsr
   const bool direct = stride == n && o.device_output;
   int32_t *work = dist;
   if (!direct) {
-    MG_TRY(ws_reserve(g->ws_out, sizeof(int32_t) * (size_t)nitems + 256));
+    MG_TRY(ws_reserve(g, g->ws_out, sizeof(int32_t) * (size_t)nitems + 256));
     work = (int32_t *)g->ws_out.ptr;
   }
   MG_TRY(sssp_core(g, seeds.data(), nsrc, work, nitems, (int32_t)(stride - 1), o, stats));

@@ -261,7 +261,7 @@ class Graph:
                  autotune=False) -> L.MgPrOpts:
         o = L.MgPrOpts()
         o.autotune = 1 if autotune else 0
-        o.gather_kernel = {"binned": 0, "tma": 1, "plain": 2}[gather]
+        o.gather_kernel = {"binned": 0, "tma": 1, "cached": 2}[gather]
         o.mode = {"refcompat": L.MG_PR_REFCOMPAT, "normalized": L.MG_PR_NORMALIZED}[mode]
         o.directed = int(directed)
         o.max_iter = int(max_iter)

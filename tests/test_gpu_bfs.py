@@ -217,3 +217,54 @@ def test_bfs_predecessors_match_reference_rule(kind):
         dp = torch.empty(h.n, dtype=torch.int32, device="cuda")
         g.bfs_predecessors(dd, out=dp)
         np.testing.assert_array_equal(dp.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_bfs_long_lattice_persistent_levels(mode):
+    # a 1024 x 512 lattice without shortcuts: about 1,500 levels of small
+    # frontiers, run by the persistent cooperative kernel; directed=0 reads the
+    # same edges from both sides
+    h = mg.gen_lattice(1024, 512, 0.0, 4)
+    with mg.Graph(h.row_offsets, h.col_idx) as g:
+        depth, st = g.bfs([0], **mode)
+        ref = oracle.bfs(h.row_offsets, h.col_idx, [0])
+        np.testing.assert_array_equal(depth, ref)
+        assert st["iterations"] == ref.max() + 1
+        d2, _ = g.bfs([h.n - 1, 5], directed=0, **mode)
+        np.testing.assert_array_equal(d2, oracle.bfs(h.row_offsets, h.col_idx, [h.n - 1, 5]))
+
+
+def _csr_from_pairs(n, src, dst):
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    ro = np.zeros(n + 1, dtype=np.int32)
+    np.add.at(ro, src + 1, 1)
+    return np.cumsum(ro, dtype=np.int64).astype(np.int32), dst.astype(np.int32)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_bfs_hubs_inside_small_push_levels(mode):
+    # Hubs of 5,000-12,000 edges reached while the frontier is still small (the
+    # persistent levels): a root with 6 hub children, each hub with its own
+    # leaves, and a 300-vertex path hanging off one leaf. Hubs of >= 4096 edges
+    # go to the grid-strided pass inside the persistent kernel.
+    rng = np.random.default_rng(5)
+    hubs = np.arange(1, 7)
+    sizes = [5000, 12000, 4096, 4095, 7000, 9000]
+    src, dst, nxt = [np.zeros(6, np.int64)], [hubs], 7
+    for h_, k in zip(hubs, sizes):
+        leaves = np.arange(nxt, nxt + k)
+        nxt += k
+        src.append(np.full(k, h_)); dst.append(rng.permutation(leaves))
+    path = np.arange(nxt, nxt + 300)
+    src.append(np.concatenate([[nxt - 1], path[:-1]])); dst.append(path)
+    n = int(path[-1]) + 1
+    s = np.concatenate(src); d = np.concatenate(dst)
+    ro, ci = _csr_from_pairs(n, np.concatenate([s, d]), np.concatenate([d, s]))
+    with mg.Graph(ro, ci, symmetric=True) as g:
+        for srcs in ([0], [path[-1]], [3, path[150]]):
+            ref = oracle.bfs(ro, ci, srcs)
+            depth, st = g.bfs(srcs, **mode)
+            np.testing.assert_array_equal(depth, ref)
+            assert st["iterations"] == ref.max() + 1
+            assert st["edges_traversed"] == int((ro[1:] - ro[:-1])[ref >= 0].sum())

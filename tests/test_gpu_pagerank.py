@@ -156,7 +156,7 @@ def test_api_pagerank_program(mtx_fixtures):
     assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < cfg.getParameter("tol")
 
 
-@pytest.mark.parametrize("gather", ["binned", "tma", "plain"])
+@pytest.mark.parametrize("gather", ["binned", "tma", "cached"])
 @pytest.mark.parametrize("weighted", [False, True])
 def test_gather_kernels_agree_with_fp64(gather, weighted):
     h = mg.gen_rmat(14, 16, 61, symmetrize=False, weights="lognormal" if weighted else None, p0=0, p1=1)
@@ -178,7 +178,7 @@ def test_gather_hub_chunks_binned():
     ro = np.zeros(n + 1, dtype=np.int64)
     np.add.at(ro, src[order] + 1, 1)
     h = mg.HostCsr(np.cumsum(ro).astype(np.int32), dst[order].astype(np.int32))
-    for gather in ("binned", "tma", "plain"):
+    for gather in ("binned", "tma", "cached"):
         with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
             x, st = g.pagerank(mode="normalized", gather=gather)
         xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
@@ -194,9 +194,9 @@ def test_hub_column_cache_partial(weighted):
     assert (np.diff(h.row_offsets) > 0).sum() > 40000
     w = h.weights_f32 if weighted else None
     with mg.Graph(h.row_offsets, h.col_idx, w, symmetric=True) as g:
-        x, st = g.pagerank(mode="normalized", weighted=weighted, gather="binned")
-        xb, stb = g.pagerank(mode="normalized", weighted=weighted, gather="plain")
-        xh, _ = g.pagerank(mode="normalized", weighted=weighted, gather="binned", use_graph=False)
+        x, st = g.pagerank(mode="normalized", weighted=weighted, gather="cached")
+        xb, stb = g.pagerank(mode="normalized", weighted=weighted, gather="binned")
+        xh, _ = g.pagerank(mode="normalized", weighted=weighted, gather="cached", use_graph=False)
     assert (x == xh).all()
     assert st["iterations"] == stb["iterations"]
     xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, w, 0.85, 0.0, st["iterations"])
