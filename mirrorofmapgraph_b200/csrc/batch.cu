@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(MS_NT) ms_push_kernel(MsArgs a) {
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc);
   const int32_t *ci = a.ci, *ri = a.ri;
   int64_t insp = 0, nexp = 0;
-  const BigList big{a.big_v, &c->big_len};
+  const BigList big{a.big_v, &c->big_len, defer_threshold<MS_NT>(nin, MS_CTA_TH)};
   auto visit_to = [&](uint64_t f, int32_t w) {
     const uint64_t add = f & ~__ldg(seen + w);
     if (add) atomicOr(acc + w, (unsigned long long)add);

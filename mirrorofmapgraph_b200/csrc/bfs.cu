@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
   const int32_t *qin = cur ? a.q1 : a.q0;
   PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
   int64_t insp = 0, nexp = 0;
-  const BigList big{a.big_v, &c->big_len};
+  const BigList big{a.big_v, &c->big_len, defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
   for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
@@ -177,8 +177,14 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
 // same control block. Vertices of GRID_TH or more edges are deferred as in the
 // per-level push and expanded by the whole grid after a second barrier, which
 // only levels that deferred one take.
-constexpr int32_t PERSIST_MAX = 1 << 16;
-constexpr int64_t PERSIST_EDGES = 1 << 17;  // frontier out-edges
+#ifndef MG_PERSIST_MAX
+#define MG_PERSIST_MAX (1 << 16)
+#endif
+#ifndef MG_PERSIST_EDGES
+#define MG_PERSIST_EDGES (1 << 17)
+#endif
+constexpr int32_t PERSIST_MAX = MG_PERSIST_MAX;
+constexpr int64_t PERSIST_EDGES = MG_PERSIST_EDGES;  // frontier out-edges
 constexpr unsigned long long PERSIST_WAIT = 1ull << 22;  // barrier polls (seconds at most) before giving up
 
 __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
     }
     const int32_t *qin = sel ? a.q1 : a.q0;
     PushCtx x{a.label, a.vis, a.ro, sel ? a.q0 : a.q1, &c->pq[out], &c->overflow, a.qcap, lvl, 0};
-    const BigList big{a.big_v, &c->pb[out]};
+    const BigList big{a.big_v, &c->pb[out], defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
     const int32_t *ci = a.ci, *ri = a.ri;
     int64_t insp = 0, nexp = 0;
     for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {

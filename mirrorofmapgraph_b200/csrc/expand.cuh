@@ -123,13 +123,24 @@ constexpr int GRID_TH = 4096;
 constexpr int BIG_CAP = 4096;  // deferred vertices per level (more fall back to the CTA bin)
 
 struct BigList {
-  int32_t *v;    // deferred vertices
-  int32_t *len;  // their count (reset at the end of every level)
+  int32_t *v;            // deferred vertices
+  int32_t *len;          // their count (reset at the end of every level)
+  int32_t th = GRID_TH;  // out-degree at or above which a vertex is deferred
 };
+
+// Deferral threshold for a frontier of nin vertices expanded by this grid. When
+// the frontier fills fewer tiles than there are CTAs, the CTA bin would leave
+// most CTAs idle while a few walk heavy rows alone (a few hundred hubs of
+// thousands of edges each), so every vertex the CTA bin would take goes to the
+// grid-wide pass instead.
+template <int NT>
+__device__ __forceinline__ int32_t defer_threshold(int64_t nin, int32_t cta_th) {
+  return nin < (int64_t)gridDim.x * NT ? cta_th : GRID_TH;
+}
 
 // Returns true (and records v) when v goes to the grid bin.
 __device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t deg) {
-  if (v < 0 || deg < GRID_TH) return false;
+  if (v < 0 || deg < big.th) return false;
   const int32_t pos = atomicAdd(big.len, 1);
   if (pos >= BIG_CAP) return false;
   big.v[pos] = v;

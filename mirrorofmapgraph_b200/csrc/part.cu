@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(PART_NT) part_push_kernel(const int32_t *ro, c
   __shared__ ExpandSmem<PART_NT> sm;
   __shared__ int64_t s_sum[PART_NT / 32 + 1];
   const PartPush x{vis, bits};
-  const BigList big{big_v, &ctl->big_len};
+  const BigList big{big_v, &ctl->big_len, defer_threshold<PART_NT>(qlen, PART_CTA_TH)};
   int64_t insp = 0;
   for (int64_t tile = (int64_t)blockIdx.x * PART_NT; tile < qlen; tile += (int64_t)gridDim.x * PART_NT) {
     const int64_t i = tile + threadIdx.x;
@@ -205,20 +205,17 @@ __global__ void __launch_bounds__(PART_NT) part_merge_kernel(const uint32_t *gat
         }
       }
     }
-    // Owned vertices of the new frontier, appended warp by warp.
-    unsigned any = __ballot_sync(FULL, x != 0u && (w << 5) < hi && ((w + 1) << 5) > lo);
-    while (any) {
-      const int l = __ffs(any) - 1;
-      any &= any - 1;
-      const uint32_t xl = __shfl_sync(FULL, x, l);
-      const int64_t wl = __shfl_sync(FULL, w, l);
-      const int64_t v = (wl << 5) + lane;
-      const bool mine = ((xl >> lane) & 1u) && v >= lo && v < hi;
-      const unsigned mb = __ballot_sync(FULL, mine);
+    // Owned vertices of the new frontier (words [lo/32, ceil(hi/32)) are owned
+    // whole): one queue reservation per warp.
+    const uint32_t own = ((w << 5) >= lo && (w << 5) < hi) ? x : 0u;
+    const int32_t cnt = __popc(own);
+    const int32_t incl = warp_inclusive_scan(cnt);
+    const int32_t wtot = __shfl_sync(FULL, incl, 31);
+    if (wtot) {
       int32_t base = 0;
-      if (lane == 0) base = atomicAdd(&ctl->qlen, __popc(mb));
-      base = __shfl_sync(FULL, base, 0);
-      if (mine) q[base + __popc(mb & lanemask_lt())] = (int32_t)v;
+      if (lane == 31) base = atomicAdd(&ctl->qlen, wtot);
+      base = __shfl_sync(FULL, base, 31) + incl - cnt;
+      for (uint32_t y = own; y; y &= y - 1) q[base++] = (int32_t)((w << 5) + (__ffs(y) - 1));
     }
   }
   const int64_t bnf = block_sum<PART_NT>(nf, s_sum);
@@ -584,8 +581,7 @@ extern "C" mg_status mg_part_bfs_step(mg_part *p, uint32_t *bits) {
   MG_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * (size_t)p->nwords, s));
   if (p->dir == 0) {
     if (p->qlen > 0) {
-      const int64_t tiles = (p->qlen + PART_NT - 1) / PART_NT;
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)p->num_sms * 8));
+      const int grid = p->num_sms * 4;
       MG_CUDA_TRY(cudaMemsetAsync(&p->ctl->big_len, 0, sizeof(int32_t), s));
       part_push_kernel<<<grid, PART_NT, 0, s>>>(p->ro, p->ci, p->lo, p->q, p->qlen, p->vis, bits, p->big_v, p->ctl);
       part_push_big_kernel<<<p->num_sms * 4, PART_NT, 0, s>>>(p->ro, p->ci, p->vis, bits, p->big_v, p->ctl);

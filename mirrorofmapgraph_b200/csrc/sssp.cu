@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   const int32_t hi = ~a.vmask;  // instance bits of an item
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
-  const BigList big{a.big_v, &c->big_len};
+  const BigList big{a.big_v, &c->big_len, defer_threshold<SSSP_NT>(nin, SSSP_CTA_TH)};
   for (int64_t tile = (int64_t)blockIdx.x * SSSP_NT; tile < nin; tile += (int64_t)gridDim.x * SSSP_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
