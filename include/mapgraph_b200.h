@@ -273,8 +273,9 @@ typedef struct mg_part_level {
   int64_t frontier_edges; /* their out-edges */
   int32_t level;          /* levels completed */
   int32_t done;           /* 1: frontier empty or iter_num reached */
-  int32_t direction;      /* MG_DIR_PUSH or MG_DIR_PULL for the next step */
+  int32_t direction;      /* BFS: MG_DIR_PUSH or MG_DIR_PULL for the next step */
   int32_t reserved;
+  double residual;        /* PageRank: L1 change of the last iteration */
 } mg_part_level;
 
 /* lo must be a multiple of 32, hi a multiple of 32 or n. out_offsets / in_offsets
@@ -299,6 +300,24 @@ mg_status mg_part_bfs_step(mg_part *p, uint32_t *bits);
 mg_status mg_part_bfs_merge(mg_part *p, const uint32_t *gathered, int32_t world, mg_part_level *level);
 /* Depths of all n vertices (replicated; host or device output) and the run's counters. */
 mg_status mg_part_bfs_result(mg_part *p, int32_t *depth, int32_t device_output, mg_stats *stats);
+
+/* PageRank over the partition: MG_PR_NORMALIZED with the uniform teleport,
+ * unweighted (opts: alpha, tol, max_iter). Per iteration
+ *     mg_part_pr_step(slice)                 this rank's new ranks of [lo, hi)
+ *                                            into slice (device, hi - lo floats)
+ *     all-gather the slices, each padded to `stride` floats (>= the largest
+ *     slice), rank-major
+ *     mg_part_pr_merge(gathered, world, stride, cuts)   cuts (host, world + 1)
+ *                                            as in the partition, [0, ..., n]
+ * until level.done (L1 change below tol, or max_iter). Every rank keeps the
+ * whole iterate; the merge's sums run in a fixed order, so all ranks stop at the
+ * same iteration. */
+mg_status mg_part_pr_begin(mg_part *p, const mg_pr_opts *opts, mg_part_level *level);
+mg_status mg_part_pr_step(mg_part *p, float *slice);
+mg_status mg_part_pr_merge(mg_part *p, const float *gathered, int32_t world, int64_t stride, const int64_t *cuts,
+                           mg_part_level *level);
+/* Ranks of all n vertices (host or device output) and the run's counters. */
+mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -53,7 +53,8 @@ class MgPrOpts(C.Structure):
 
 class MgPartLevel(C.Structure):
     _fields_ = [("frontier", C.c_int64), ("frontier_edges", C.c_int64), ("level", C.c_int32),
-                ("done", C.c_int32), ("direction", C.c_int32), ("reserved", C.c_int32)]
+                ("done", C.c_int32), ("direction", C.c_int32), ("reserved", C.c_int32),
+                ("residual", C.c_double)]
 
 
 class MgHostCsr(C.Structure):
@@ -110,6 +111,10 @@ SIGNATURES = {
     "mg_part_bfs_step": (C.c_int, [_P, _P]),
     "mg_part_bfs_merge": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgPartLevel)]),
     "mg_part_bfs_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
+    "mg_part_pr_begin": (C.c_int, [_P, C.POINTER(MgPrOpts), C.POINTER(MgPartLevel)]),
+    "mg_part_pr_step": (C.c_int, [_P, _P]),
+    "mg_part_pr_merge": (C.c_int, [_P, _P, C.c_int32, C.c_int64, _P, C.POINTER(MgPartLevel)]),
+    "mg_part_pr_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
 }
 
 _lib = None

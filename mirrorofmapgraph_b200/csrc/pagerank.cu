@@ -75,11 +75,7 @@ void pr_release_plans(mg_graph *g) {
     dev_free(g, p->tx);
     dev_free(g, p->ty);
   }
-  for (mg::BinPlan *b : {&ps->bcsc, &ps->bcsr}) {
-    for (void *q : {(void *)b->rows, (void *)b->hrows, (void *)b->hbase, (void *)b->hcount, (void *)b->hpart,
-                    (void *)b->hcontrib})
-      dev_free(g, q);
-  }
+  for (mg::BinPlan *b : {&ps->bcsc, &ps->bcsr}) bin_plan_release(g->stream, *b);
   for (void *q : {(void *)ps->hubs.cidx, (void *)ps->hubs.slot, (void *)ps->hubs.hv}) dev_free(g, q);
   delete ps;
   g->plan_csc = nullptr;
@@ -103,6 +99,71 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
   return MG_OK;
 }
 
+// Degree-binned plan of any row-offset array (n + 1 entries) on stream s: the
+// CSC of a graph (forward gather), its CSR (adjoint, row sums) or the owned rows
+// of a partition slice.
+mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
+  using namespace mg;
+  auto alloc = [&](void **p, size_t bytes) -> mg_status {
+    if (cudaMallocAsync(p, std::max<size_t>(bytes, 4), s) != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      mg_set_error("PageRank plan: device allocation of %zu bytes failed", bytes);
+      return MG_ERR_OOM;
+    }
+    return MG_OK;
+  };
+  const int64_t nchunks = std::max<int64_t>(1, (n + PRB_CHUNK_ROWS - 1) / PRB_CHUNK_ROWS);
+  int64_t *counts = nullptr;
+  MG_CUDA_TRY(cudaMallocAsync((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
+  int64_t *totals = counts + nchunks * (PRB_BINS + 1);
+  int64_t *dboff = totals + (PRB_BINS + 1);
+  prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts);
+  prb_offsets_kernel<<<1, 32, 0, s>>>(counts, nchunks, totals);
+  int64_t cnt[PRB_BINS + 1];
+  MG_CUDA_TRY(cudaMemcpyAsync(cnt, totals, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  int64_t acc = 0;
+  for (int b = 0; b < PRB_BINS; b++) {
+    bp.boff[b] = acc;
+    if (b < 6) acc += cnt[b];
+  }
+  bp.boff[PRB_BINS] = acc;
+  bp.boff[6] = acc;
+  bp.nheavy = cnt[6];
+  bp.ntasks = cnt[PRB_BINS];
+  // One warp assignment per 32 rows of bins 0..5, one per hub chunk.
+  int64_t w = 0;
+  for (int b = 0; b < PRB_BINS; b++) {
+    bp.wstart[b] = w;
+    if (b < 6) w += (cnt[b] + 31) / 32;
+    else w += bp.ntasks;
+  }
+  bp.wstart[PRB_BINS] = w;
+  MG_TRY(alloc((void **)&bp.rows, sizeof(int32_t) * std::max<int64_t>(acc, 1)));
+  MG_TRY(alloc((void **)&bp.hrows, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+  MG_TRY(alloc((void **)&bp.hbase, sizeof(int32_t) * (bp.nheavy + 1)));
+  MG_TRY(alloc((void **)&bp.hcount, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
+  MG_TRY(alloc((void **)&bp.hpart, sizeof(Comp) * std::max<int64_t>(bp.ntasks, 1)));
+  MG_TRY(alloc((void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
+  MG_TRY(alloc((void **)&bp.grab, sizeof(int32_t)));
+  MG_CUDA_TRY(cudaMemsetAsync(bp.grab, 0, sizeof(int32_t), s));
+  MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
+  MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
+  prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows);
+  prb_hubs_kernel<<<1, PRB_NT, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaFreeAsync(counts, s));
+  return MG_OK;
+}
+
+void bin_plan_release(cudaStream_t s, mg::BinPlan &bp) {
+  for (void *q : {(void *)bp.rows, (void *)bp.hrows, (void *)bp.hbase, (void *)bp.hcount, (void *)bp.hpart,
+                  (void *)bp.hcontrib, (void *)bp.grab})
+    if (q) cudaFreeAsync(q, s);
+  bp = mg::BinPlan();
+}
+
 // Degree-binned plan of the CSC (forward gather) or the CSR (adjoint, row sums).
 static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
   using namespace mg;
@@ -110,48 +171,7 @@ static mg_status get_bin_plan(mg_graph *g, bool csr, mg::BinPlan **out) {
   BinPlan &bp = csr ? ps->bcsr : ps->bcsc;
   bool &ok = csr ? ps->bcsr_ok : ps->bcsc_ok;
   if (!ok) {
-    const int32_t *off = csr ? g->ro : g->co;
-    const int64_t n = g->n;
-    cudaStream_t s = g->stream;
-    const int64_t nchunks = std::max<int64_t>(1, (n + PRB_CHUNK_ROWS - 1) / PRB_CHUNK_ROWS);
-    int64_t *counts = nullptr;
-    MG_CUDA_TRY(cudaMallocAsync((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
-    int64_t *totals = counts + nchunks * (PRB_BINS + 1);
-    int64_t *dboff = totals + (PRB_BINS + 1);
-    prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts);
-    prb_offsets_kernel<<<1, 32, 0, s>>>(counts, nchunks, totals);
-    int64_t cnt[PRB_BINS + 1];
-    MG_CUDA_TRY(cudaMemcpyAsync(cnt, totals, sizeof(cnt), cudaMemcpyDeviceToHost, s));
-    MG_CUDA_TRY(cudaStreamSynchronize(s));
-    int64_t acc = 0;
-    for (int b = 0; b < PRB_BINS; b++) {
-      bp.boff[b] = acc;
-      if (b < 6) acc += cnt[b];
-    }
-    bp.boff[PRB_BINS] = acc;
-    bp.boff[6] = acc;
-    bp.nheavy = cnt[6];
-    bp.ntasks = cnt[PRB_BINS];
-    // One warp assignment per 32 rows of bins 0..5, one per hub chunk.
-    int64_t w = 0;
-    for (int b = 0; b < PRB_BINS; b++) {
-      bp.wstart[b] = w;
-      if (b < 6) w += (cnt[b] + 31) / 32;
-      else w += bp.ntasks;
-    }
-    bp.wstart[PRB_BINS] = w;
-    MG_TRY(dev_alloc(g, (void **)&bp.rows, sizeof(int32_t) * std::max<int64_t>(acc, 1)));
-    MG_TRY(dev_alloc(g, (void **)&bp.hrows, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
-    MG_TRY(dev_alloc(g, (void **)&bp.hbase, sizeof(int32_t) * (bp.nheavy + 1)));
-    MG_TRY(dev_alloc(g, (void **)&bp.hcount, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1)));
-    MG_TRY(dev_alloc(g, (void **)&bp.hpart, sizeof(Comp) * std::max<int64_t>(bp.ntasks, 1)));
-    MG_TRY(dev_alloc(g, (void **)&bp.hcontrib, sizeof(double) * 2 * std::max<int64_t>(bp.nheavy, 1)));
-    MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
-    MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
-    prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows);
-    prb_hubs_kernel<<<1, PRB_NT, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
-    MG_CUDA_TRY(cudaGetLastError());
-    MG_CUDA_TRY(cudaFreeAsync(counts, s));
+    MG_TRY(bin_plan_build(g->stream, csr ? g->ro : g->co, g->n, bp));
     ok = true;
   }
   *out = &bp;
@@ -179,6 +199,7 @@ static mg::PrbArgs prb_args_of(const mg_graph *g, const mg::BinPlan &bp, bool cs
     p.wstart[b] = bp.wstart[b];
   }
   p.nheavy = bp.nheavy;
+  p.grab = nullptr;
   return p;
 }
 
@@ -385,25 +406,33 @@ __global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) solve_binned_kernel(So
     a.part1[2 * blockIdx.x] = r;
     a.part1[2 * blockIdx.x + 1] = d;
   }
-  if (last_block(&c->blocks_done)) solve_iteration_end(a, cur, p.hcontrib, p.nheavy, s_red);
+  if (last_block(&c->blocks_done)) {
+    if (threadIdx.x == 0 && p.grab) *p.grab = 0;
+    solve_iteration_end(a, cur, p.hcontrib, p.nheavy, s_red);
+  }
 }
 
 // One whole iteration of the degree-binned solver with the column cache: every
-// CTA first copies the cached columns' gathered values into shared memory.
+// CTA first copies the cached columns' gathered values into shared memory. One
+// CTA of 1024 threads per SM, so the SM's cache is one copy. Measured on R-MAT
+// s22 with the dynamic schedule (us per iteration): 1024 threads x 1 CTA with
+// 24K / 32K / 40K / 50K columns 514 / 500 / 495 / 665 (L1 starves), 768 x 1 with
+// 40K 545, 640 x 2 with 20K 513.
 #ifndef PRB_HUB_THREADS
-#define PRB_HUB_THREADS 640
+#define PRB_HUB_THREADS 1024
 #endif
 #ifndef PRB_HUB_MINB
-#define PRB_HUB_MINB 2
+#define PRB_HUB_MINB 1
 #endif
 // Columns cached per CTA: the rest of the SM's shared memory stays L1 for the
-// uncached gathers (20480 columns = 80 KB per CTA measured best on R-MAT s22).
+// uncached gathers.
 #ifndef PRB_HUB_CAP
-#define PRB_HUB_CAP 20480
+#define PRB_HUB_CAP 40960
 #endif
 // Rounds of the warp-per-row gather sized to the row's tail (prb_warp_range's
-// ADAPT) in the column-cache kernel. Measured on R-MAT s22 (us per iteration):
-// 640 threads with ADAPT 591, 768 with ADAPT 628, 768 without 599, 640 without 774.
+// ADAPT) in the column-cache kernel. Measured on R-MAT s22 (us per iteration,
+// static schedule): 640 threads with ADAPT 591, 768 with ADAPT 628, 768 without
+// 599, 640 without 774.
 #ifndef PRB_HUB_ADAPT
 #define PRB_HUB_ADAPT true
 #endif
@@ -444,7 +473,10 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
     a.part1[2 * blockIdx.x] = r;
     a.part1[2 * blockIdx.x + 1] = d;
   }
-  if (last_block(&c->blocks_done)) solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.nheavy, s_red);
+  if (last_block(&c->blocks_done)) {
+    if (threadIdx.x == 0 && p.grab) *p.grab = 0;
+    solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.nheavy, s_red);
+  }
 }
 
 // Column-cache set-up kernels.
@@ -805,6 +837,9 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
     a.ntiles = plan->ntiles;
   } else {
     sp.p = prb_args_of(g, *bins, adjoint, a.wts);
+#if PRB_DYNAMIC
+    sp.p.grab = bins->grab;  // the solve kernels' last CTA resets it
+#endif
     if (use_hub) sp.p.idx = hubs->cidx;
   }
   MG_CUDA_TRY(cudaGetLastError());
@@ -1158,7 +1193,7 @@ static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opt
   const bool weighted = o.weighted != 0;
   const int32_t limit = hub_cache_limit(g);
   std::vector<int32_t> caps;
-  for (int32_t c : {8192, 16384, 20480, limit})
+  for (int32_t c : {20480, 32768, PRB_HUB_CAP})
     if (c > 0 && c <= limit && std::find(caps.begin(), caps.end(), c) == caps.end()) caps.push_back(c);
   caps.push_back(0);  // no cache
   float best = 0.f;
@@ -1308,7 +1343,7 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
                                    sizeof(float) * nw, sizeof(float) * ((size_t)n + 8), sizeof(double) * W,
                                    sizeof(double) * 2 * W * (size_t)gpart,
                                    sizeof(Comp) * W * (size_t)std::max<int64_t>(nchunks, 1),
-                                   sizeof(int32_t) * (size_t)std::max<int64_t>(nheavy, 1),
+                                   sizeof(int32_t) * (size_t)(std::max<int64_t>(nheavy, 1) + 1),
                                    sizeof(double) * 2 * W * (size_t)std::max<int64_t>(nheavy, 1),
                                    out_is_device ? 0 : sizeof(float) * (size_t)kmax * n});
   MG_TRY(ws_reserve(g, g->ws_main, need));
@@ -1324,7 +1359,8 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
   a.dang = cv.take<double>(W);
   a.part = cv.take<double>(2 * (size_t)W * gpart);
   a.hpart = cv.take<Comp>((size_t)W * std::max<int64_t>(nchunks, 1));
-  a.hcount = cv.take<int32_t>(std::max<int64_t>(nheavy, 1));
+  a.hcount = cv.take<int32_t>(std::max<int64_t>(nheavy, 1) + 1);
+  a.grab = a.hcount + std::max<int64_t>(nheavy, 1);
   a.hres = cv.take<double>(2 * (size_t)W * std::max<int64_t>(nheavy, 1));
   float *stage = out_is_device ? nullptr : cv.take<float>((size_t)kmax * n);
   a.off = g->co;
@@ -1346,7 +1382,7 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
   a.grid = grid;
   a.ctl = g->ctl;
   cudaStream_t s = g->stream;
-  MG_CUDA_TRY(cudaMemsetAsync(a.hcount, 0, sizeof(int32_t) * std::max<int64_t>(nheavy, 1), s));
+  MG_CUDA_TRY(cudaMemsetAsync(a.hcount, 0, sizeof(int32_t) * (std::max<int64_t>(nheavy, 1) + 1), s));
   if (!weighted) {
     outdeg_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, n, srow);
   } else {
@@ -1477,6 +1513,7 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
     total.kernel_ms += st.kernel_ms;
     total.launches += st.launches;
     total.residual = std::max(total.residual, st.residual);
+    total.status_detail = st.status_detail;  // cached columns of the gather (same for every vector)
   }
   if (stats) *stats = total;
   return MG_OK;

@@ -25,6 +25,8 @@
 #include "common.cuh"
 #include "expand.cuh"
 #include "mg_internal.h"
+#define MG_PRB_NO_PLAN_KERNELS
+#include "pr_binned.cuh"
 
 namespace mg {
 
@@ -40,6 +42,9 @@ struct PartCtl {
   int32_t qlen;             // owned vertices of the new frontier (push queue)
   int32_t big_len;          // deferred big vertices of a push step
   unsigned long long insp;  // edges read by this rank's steps (run total)
+  double resid;             // PageRank: L1 change of the last merge
+  double dang;              // PageRank: dangling mass of the current iterate
+  unsigned blocks_done;     // PageRank step: CTAs finished (the last resets the schedule)
 };
 
 __global__ void part_clear_kernel(uint32_t *vis, uint32_t *fr, int32_t *depth, int64_t nwords, int64_t n) {
@@ -252,6 +257,95 @@ __global__ void part_sum_kernel(const int32_t *v, int64_t n, unsigned long long 
   if (threadIdx.x == 0 && b) atomicAdd(sum, (unsigned long long)b);
 }
 
+// PageRank over the partition (normalised, uniform teleport t = 1/n; the rule of
+// mg_pagerank's MG_PR_NORMALIZED): x' = alpha (P^T x + d t) + (1 - alpha) t.
+// Every rank keeps x and y = x / outdeg for all n vertices; a step computes x' of
+// its own rows from y with the degree-binned gather over its in-edges, the
+// ranks all-gather the slices, and the merge (identical on every rank) forms y,
+// the L1 change and the dangling mass d with fixed-order FP64 sums, so every
+// rank takes the same stop decision.
+struct PartPrRow {
+  float *slice;
+  double alpha, tn, d;
+  __device__ __forceinline__ void operator()(int32_t r, Comp v) const {
+    const double acc = (double)v.hi + (double)v.lo;
+    slice[r] = (float)(alpha * (acc + d * tn) + (1.0 - alpha) * tn);
+  }
+};
+
+__global__ void __launch_bounds__(PRB_NT, PRB_MIN_BLOCKS) part_pr_kernel(PrbArgs p, const float *y, float *slice,
+                                                                         double alpha, double tn, PartCtl *ctl) {
+  const PartPrRow up{slice, alpha, tn, __ldcg(&ctl->dang)};
+  prb_run<false>(p, [&](int32_t col) { return __ldg(y + col); }, up,
+                 [&](int64_t, int32_t row, Comp v) { up(row, v); });
+  if (last_block(&ctl->blocks_done) && threadIdx.x == 0) {
+    *p.grab = 0;
+    ctl->blocks_done = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) part_pr_init_kernel(int64_t n, double tn, const int32_t *deg, float *x,
+                                                           float *y, double *part) {
+  __shared__ double s_red[256 / 32 + 1];
+  double d = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    x[v] = (float)tn;
+    const int32_t k = deg[v];
+    if (k > 0) {
+      y[v] = (float)(tn / k);
+    } else {
+      y[v] = 0.f;
+      d += (double)(float)tn;
+    }
+  }
+  d = block_sum<256>(d, s_red);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = 0.0;
+    part[2 * blockIdx.x + 1] = d;
+  }
+}
+
+__global__ void __launch_bounds__(256) part_pr_merge_kernel(int64_t n, const float *xo, const float *xn,
+                                                            const int32_t *deg, float *y, double *part) {
+  __shared__ double s_red[256 / 32 + 1];
+  double r = 0.0, d = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const float x = xn[v];
+    r += fabs((double)x - (double)xo[v]);
+    const int32_t k = deg[v];
+    if (k > 0) {
+      y[v] = (float)((double)x / k);
+    } else {
+      y[v] = 0.f;
+      d += (double)x;
+    }
+  }
+  r = block_sum<256>(r, s_red);
+  d = block_sum<256>(d, s_red);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = r;
+    part[2 * blockIdx.x + 1] = d;
+  }
+}
+
+// Fixed-order sum of the per-CTA partials (the same on every rank).
+__global__ void __launch_bounds__(256) part_pr_reduce_kernel(const double *part, int32_t grid, PartCtl *ctl) {
+  __shared__ double s_red[256 / 32 + 1];
+  double r = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < grid; i += 256) {
+    r += part[2 * i];
+    d += part[2 * i + 1];
+  }
+  r = block_sum<256>(r, s_red);
+  d = block_sum<256>(d, s_red);
+  if (threadIdx.x == 0) {
+    ctl->resid = r;
+    ctl->dang = d;
+  }
+}
+
 __global__ void part_outdeg_kernel(const int32_t *ro, int64_t rows, int32_t *deg) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) deg[i] = ro[i + 1] - ro[i];
@@ -272,6 +366,15 @@ struct mg_part {
   int32_t *depth = nullptr, *q = nullptr, *big_v = nullptr, *srcs = nullptr;
   int32_t src_cap = 0;
   mg::PartCtl *ctl = nullptr, *ctl_host = nullptr;
+  // PageRank state
+  mg::BinPlan prb;
+  bool prb_ok = false;
+  float *xo = nullptr, *xn = nullptr, *y = nullptr;
+  double *ppart = nullptr;
+  int32_t pgrid = 0;
+  bool pr_begun = false, pr_stepped = false, pr_done = true;
+  int32_t pr_level = 0, pr_max_iter = 50;
+  double alpha = 0.85, tol = 1e-6, tn = 0.0, resid = 0.0;
   bool begun = false, done = true, stepped = false;
   int32_t level = 0, dir = 0, mode = MG_DIR_AUTO, iter_cap = 0, qlen = 0;
   int64_t nf = 0, mf = 0, vdeg = 0, levels_pull = 0, steps = 0;
@@ -311,6 +414,11 @@ void part_free(mg_part *p) {
   fr(p->big_v);
   fr(p->srcs);
   fr(p->ctl);
+  fr(p->xo);
+  fr(p->xn);
+  fr(p->y);
+  fr(p->ppart);
+  if (p->prb_ok && p->stream) bin_plan_release(p->stream, p->prb);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->ctl_host) cudaFreeHost(p->ctl_host);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -664,6 +772,179 @@ extern "C" mg_status mg_part_bfs_result(mg_part *p, int32_t *depth, int32_t devi
     stats->kernel_ms = ms;
     stats->status_detail = (int32_t)p->levels_pull;
     stats->launches = 2 + 3 * p->steps;
+  }
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// PageRank over the partition.
+
+static void fill_pr_level(const mg_part *p, mg_part_level *lv) {
+  if (!lv) return;
+  std::memset(lv, 0, sizeof(*lv));
+  lv->level = p->pr_level;
+  lv->done = p->pr_done ? 1 : 0;
+  lv->residual = p->resid;
+}
+
+extern "C" mg_status mg_part_pr_begin(mg_part *p, const mg_pr_opts *opts, mg_part_level *level) {
+  using namespace mg;
+  if (!p) {
+    mg_set_error("mg_part_pr_begin: null argument");
+    return MG_ERR_ARG;
+  }
+  mg_pr_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.mode = MG_PR_NORMALIZED;
+  if (opts) o = *opts;
+  if (o.mode != MG_PR_NORMALIZED || o.weighted) {
+    mg_set_error("mg_part_pr_begin: the partitioned PageRank runs MG_PR_NORMALIZED, unweighted");
+    return MG_ERR_UNSUPPORTED;
+  }
+  MG_CUDA_TRY(cudaSetDevice(p->device));
+  cudaStream_t s = p->stream;
+  const int64_t rows = p->hi - p->lo;
+  if (!p->prb_ok) {
+    MG_TRY(bin_plan_build(s, p->co, rows, p->prb));
+    p->prb_ok = true;
+  }
+  p->pgrid = p->num_sms * 4;
+  const size_t vb = sizeof(float) * (size_t)(p->n + 8);
+  if (!p->xo) MG_TRY(part_alloc(p, (void **)&p->xo, vb));
+  if (!p->xn) MG_TRY(part_alloc(p, (void **)&p->xn, vb));
+  if (!p->y) MG_TRY(part_alloc(p, (void **)&p->y, vb));
+  if (!p->ppart) MG_TRY(part_alloc(p, (void **)&p->ppart, sizeof(double) * 2 * (size_t)p->pgrid));
+  p->alpha = o.alpha > 0 ? o.alpha : 0.85;
+  p->tol = o.tol > 0 ? o.tol : 1e-6;
+  p->pr_max_iter = o.max_iter > 0 ? o.max_iter : 50;
+  p->tn = 1.0 / (double)p->n;
+  MG_CUDA_TRY(cudaEventRecord(p->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(p->ctl, 0, sizeof(PartCtl), s));
+  part_pr_init_kernel<<<p->pgrid, 256, 0, s>>>(p->n, p->tn, p->deg, p->xo, p->y, p->ppart);
+  part_pr_reduce_kernel<<<1, 256, 0, s>>>(p->ppart, p->pgrid, p->ctl);
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  p->pr_level = 0;
+  p->resid = 0.0;
+  p->pr_done = false;
+  p->pr_begun = true;
+  p->pr_stepped = false;
+  fill_pr_level(p, level);
+  return MG_OK;
+}
+
+extern "C" mg_status mg_part_pr_step(mg_part *p, float *slice) {
+  using namespace mg;
+  if (!p || !slice) {
+    mg_set_error("mg_part_pr_step: null argument");
+    return MG_ERR_ARG;
+  }
+  if (!p->pr_begun || p->pr_done || p->pr_stepped) {
+    mg_set_error("mg_part_pr_step: no iteration pending (call mg_part_pr_begin, then step and merge in turn)");
+    return MG_ERR_ARG;
+  }
+  MG_CUDA_TRY(cudaSetDevice(p->device));
+  PrbArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.off = p->co;
+  a.idx = p->ri;
+  a.wts = nullptr;
+  a.rows = p->prb.rows;
+  a.hrows = p->prb.hrows;
+  a.hbase = p->prb.hbase;
+  a.hcount = p->prb.hcount;
+  a.hpart = p->prb.hpart;
+  a.hcontrib = p->prb.hcontrib;
+  a.grab = p->prb.grab;
+  for (int b = 0; b <= PRB_BINS; b++) {
+    a.boff[b] = p->prb.boff[b];
+    a.wstart[b] = p->prb.wstart[b];
+  }
+  a.nheavy = p->prb.nheavy;
+  if (p->hi > p->lo)
+    part_pr_kernel<<<p->num_sms * PRB_MIN_BLOCKS, PRB_NT, 0, p->stream>>>(a, p->y, slice, p->alpha, p->tn, p->ctl);
+  MG_CUDA_TRY(cudaGetLastError());
+  p->pr_stepped = true;
+  return MG_OK;
+}
+
+extern "C" mg_status mg_part_pr_merge(mg_part *p, const float *gathered, int32_t world, int64_t stride,
+                                      const int64_t *cuts, mg_part_level *level) {
+  using namespace mg;
+  if (!p || !gathered || !cuts || world <= 0 || stride < 0) {
+    mg_set_error("mg_part_pr_merge: null argument, world <= 0 or stride < 0");
+    return MG_ERR_ARG;
+  }
+  if (!p->pr_stepped) {
+    mg_set_error("mg_part_pr_merge: no step to merge");
+    return MG_ERR_ARG;
+  }
+  bool mine = false;
+  if (cuts[0] != 0 || cuts[world] != p->n) {
+    mg_set_error("mg_part_pr_merge: cuts must run from 0 to n");
+    return MG_ERR_ARG;
+  }
+  for (int32_t r = 0; r < world; r++) {
+    if (cuts[r + 1] < cuts[r] || cuts[r + 1] - cuts[r] > stride) {
+      mg_set_error("mg_part_pr_merge: cuts must be non-decreasing with slices of at most stride entries");
+      return MG_ERR_ARG;
+    }
+    mine = mine || (cuts[r] == p->lo && cuts[r + 1] == p->hi);
+  }
+  if (!mine) {
+    mg_set_error("mg_part_pr_merge: no slice of the cuts is this partition's [lo, hi)");
+    return MG_ERR_ARG;
+  }
+  MG_CUDA_TRY(cudaSetDevice(p->device));
+  cudaStream_t s = p->stream;
+  for (int32_t r = 0; r < world; r++) {
+    const int64_t len = cuts[r + 1] - cuts[r];
+    if (len > 0)
+      MG_CUDA_TRY(cudaMemcpyAsync(p->xn + cuts[r], gathered + (size_t)r * stride, sizeof(float) * (size_t)len,
+                                  cudaMemcpyDeviceToDevice, s));
+  }
+  part_pr_merge_kernel<<<p->pgrid, 256, 0, s>>>(p->n, p->xo, p->xn, p->deg, p->y, p->ppart);
+  part_pr_reduce_kernel<<<1, 256, 0, s>>>(p->ppart, p->pgrid, p->ctl);
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(PartCtl), cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  std::swap(p->xo, p->xn);
+  p->pr_stepped = false;
+  p->pr_level += 1;
+  p->resid = p->ctl_host->resid;
+  p->pr_done = p->resid < p->tol || p->pr_level >= p->pr_max_iter;
+  fill_pr_level(p, level);
+  return MG_OK;
+}
+
+extern "C" mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_stats *stats) {
+  using namespace mg;
+  if (!p || !ranks) {
+    mg_set_error("mg_part_pr_result: null argument");
+    return MG_ERR_ARG;
+  }
+  if (!p->pr_begun) {
+    mg_set_error("mg_part_pr_result: no run (call mg_part_pr_begin first)");
+    return MG_ERR_ARG;
+  }
+  MG_CUDA_TRY(cudaSetDevice(p->device));
+  cudaStream_t s = p->stream;
+  MG_CUDA_TRY(cudaEventRecord(p->ev1, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(ranks, p->xo, sizeof(float) * (size_t)p->n,
+                              device_output ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = p->pr_level;
+    stats->edges_traversed = p->m_total * p->pr_level;
+    stats->edges_inspected = p->m_in * p->pr_level;
+    stats->residual = p->resid;
+    stats->bytes_compulsory =
+        p->pr_level * (4 * (p->hi - p->lo + 1) + 4 * p->m_in + 4 * (p->hi - p->lo) + 16 * p->n);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+    stats->kernel_ms = ms;
+    stats->launches = 2 + 3 * (int64_t)p->pr_level;
   }
   return MG_OK;
 }

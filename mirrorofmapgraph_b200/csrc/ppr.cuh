@@ -31,6 +31,7 @@ struct PprArgs {
   const int32_t *hrows, *hbase;  // hub rows and their first chunk
   int64_t nheavy, nchunks;
   int32_t *hcount;  // arrival counters of the hubs (nheavy)
+  int32_t *grab;    // work-item counter of the dynamic schedule (reset by the last CTA)
   Comp *hpart;      // hub chunk partial sums (nchunks x W)
   double *hres;     // per-hub FP64 contributions: residual (W) then dangling (W)
   const float *srow;  // s_u (0: dangling)
@@ -205,7 +206,8 @@ __device__ void ppr_iteration_end(const PprArgs &a, int cur, double *s_max) {
 }
 
 // One iteration for every column of the group. Warp items: hub chunks first (the
-// longest items start first), then the non-hub rows; static assignment by warp.
+// longest items start first), then the non-hub rows; each warp takes the next
+// item from a shared counter, so faster SMs take more.
 template <int VPL, bool WEIGHTED>
 __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
   __shared__ double s_red[2][PPR_NT / 32][32 * VPL];
@@ -229,9 +231,8 @@ __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
     rs[j] = 0.0;
     ds[j] = 0.0;
   }
-  const int64_t nwarps = ((int64_t)gridDim.x * PPR_NT) >> 5;
   const int64_t total = a.nchunks + a.nlight;
-  for (int64_t it = ((int64_t)blockIdx.x * PPR_NT + threadIdx.x) >> 5; it < total; it += nwarps) {
+  auto item = [&](int64_t it) {
     Comp acc[VPL];
 #pragma unroll
     for (int j = 0; j < VPL; j++) acc[j] = Comp{0.f, 0.f};
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
       const int32_t row = a.rows[it - a.nchunks];
       ppr_gather<VPL, WEIGHTED>(a, go, __ldg(a.off + row), __ldg(a.off + row + 1), acc);
       ppr_update<VPL>(a, row, acc, xo, xn, gn, dj, rs, ds);
-      continue;
+      return;
     }
     // Hub chunk `it`: its hub by binary search over the chunk bases.
     int64_t lo = 0, hi = a.nheavy;
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
       last = atomicAdd(a.hcount + lo, 1) == nch - 1;
     }
     last = __shfl_sync(FULL, last, 0);
-    if (!last) continue;
+    if (!last) return;
     __threadfence();
     Comp tot[VPL];
 #pragma unroll
@@ -291,6 +292,13 @@ __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
       hc[a.W + ppr_col<VPL>(lane, j)] = hd[j];
     }
     __threadfence();
+  };
+  for (;;) {
+    int64_t it = 0;
+    if (lane == 0) it = atomicAdd(a.grab, 1);
+    it = __shfl_sync(FULL, it, 0);
+    if (it >= total) break;
+    item(it);
   }
   // Per-CTA partials, fixed order over the warps.
 #pragma unroll
@@ -314,6 +322,7 @@ __global__ void __launch_bounds__(PPR_NT) ppr_iter_kernel(PprArgs a) {
   __syncthreads();
   if (s_last) {
     __threadfence();
+    if (threadIdx.x == 0) *a.grab = 0;
     ppr_iteration_end(a, cur, s_max);
   }
 }

@@ -58,6 +58,15 @@ __device__ __forceinline__ T prb_stream(const T *p) {
 // Assignment order of a persistent warp: 1 walks the plan from the hub chunks and
 // the heaviest bins down to the lightest (longest items first shortens the
 // tail); 0 walks bins 0..6 in order.
+// Solve kernels take their work items from a shared counter (1) or by a fixed
+// grid stride (0).
+#ifndef PRB_DYNAMIC
+#define PRB_DYNAMIC 1
+#endif
+// Work items a warp takes per grab of the dynamic schedule.
+#ifndef PRB_GRAB
+#define PRB_GRAB 1
+#endif
 #ifndef PRB_HEAVY_FIRST
 #define PRB_HEAVY_FIRST 1
 #endif
@@ -72,10 +81,19 @@ struct BinPlan {
   int32_t *hcount = nullptr;    // arrival counters of the hubs (reset by the finishing warp)
   Comp *hpart = nullptr;        // partial sums of the hub chunks
   double *hcontrib = nullptr;   // per-hub FP64 contributions (residual, second reduction)
+  int32_t *grab = nullptr;      // work-item counter of the dynamic schedule (zero between launches)
   int64_t boff[PRB_BINS + 1] = {0};  // bin offsets into rows (bin 6 unused)
   int64_t nheavy = 0, ntasks = 0;
   int64_t wstart[PRB_BINS + 1] = {0};  // first warp assignment of each bin
 };
+
+}  // namespace mg
+
+// Host side (pagerank.cu): builds / releases a plan over `off` (n + 1 entries).
+mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp);
+void bin_plan_release(cudaStream_t s, mg::BinPlan &bp);
+
+namespace mg {
 
 __device__ __forceinline__ int prb_bin_of(int32_t deg) {
   if (deg <= 1) return 0;
@@ -95,6 +113,7 @@ __device__ __forceinline__ int prb_bin_of(int32_t deg) {
 constexpr int PRB_RPT = 8;
 constexpr int PRB_CHUNK_ROWS = PRB_NT * PRB_RPT;
 
+#ifndef MG_PRB_NO_PLAN_KERNELS  // plan building runs in pagerank.cu only
 __global__ void __launch_bounds__(PRB_NT) prb_count_kernel(const int32_t *__restrict__ off, int64_t n,
                                                            int64_t *__restrict__ counts /* [chunk][BINS+1] */) {
   __shared__ int64_t s[PRB_BINS + 1];
@@ -178,6 +197,7 @@ __global__ void __launch_bounds__(PRB_NT) prb_hubs_kernel(const int32_t *__restr
   }
   if (threadIdx.x == 0) hbase[nheavy] = carry;
 }
+#endif  // MG_PRB_NO_PLAN_KERNELS
 
 struct PrbArgs {
   const int32_t *off, *idx;
@@ -186,6 +206,10 @@ struct PrbArgs {
   int32_t *hcount;
   Comp *hpart;
   double *hcontrib;
+  // Dynamic schedule: warps take PRB_GRAB work items at a time from this counter
+  // (heaviest first) instead of a fixed grid stride; the launch's last CTA
+  // resets it. nullptr: fixed stride.
+  int32_t *grab;
   int64_t boff[PRB_BINS + 1];
   int64_t wstart[PRB_BINS + 1];
   int64_t nheavy;
@@ -330,10 +354,9 @@ __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa
 // finish(row, Comp) consumes a row sum; finish_hub(h, row, Comp) consumes a hub's.
 template <bool WEIGHTED, bool ADAPT = true, typename Gather, typename Finish, typename FinishHub>
 __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finish &&finish, FinishHub &&finish_hub) {
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t total = p.wstart[PRB_BINS];
   const int lane = threadIdx.x & 31;
-  for (int64_t wi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total; wi += nwarps) {
+  auto item = [&](int64_t wi) {
     const int64_t w = PRB_HEAVY_FIRST ? total - 1 - wi : wi;
     int bin = 0;
 #pragma unroll
@@ -352,7 +375,7 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
         default: acc = prb_rows32<32, WEIGHTED, ADAPT>(p, 5, wa, gather, &row); break;
       }
       if (row >= 0) finish(row, acc);
-      continue;
+      return;
     }
     switch (bin) {
       default: {
@@ -390,6 +413,19 @@ __device__ __forceinline__ void prb_run(const PrbArgs &p, Gather &&gather, Finis
         break;
       }
     }
+  };
+  if (p.grab) {
+    for (;;) {
+      int64_t base = 0;
+      if (lane == 0) base = atomicAdd(p.grab, PRB_GRAB);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= total) break;
+      const int64_t end = min(base + (int64_t)PRB_GRAB, total);
+      for (int64_t wi = base; wi < end; wi++) item(wi);
+    }
+  } else {
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t wi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total; wi += nwarps) item(wi);
   }
 }
 

@@ -112,6 +112,7 @@ __device__ __forceinline__ int merge_split(const int32_t *row_end, int nrows, in
   return lo;
 }
 
+#ifndef MG_PRB_NO_PLAN_KERNELS  // plan building runs in pagerank.cu only
 // Tile coordinates over the global sequence: tx[t], ty[t] for t = 0..ntiles.
 __global__ void prg_plan_kernel(const int32_t *__restrict__ off, int64_t n, int64_t m, int32_t ntiles,
                                 int32_t *__restrict__ tx, int32_t *__restrict__ ty) {
@@ -127,6 +128,7 @@ __global__ void prg_plan_kernel(const int32_t *__restrict__ off, int64_t n, int6
     ty[t] = (int32_t)(diag - lo);
   }
 }
+#endif  // MG_PRB_NO_PLAN_KERNELS
 
 // One shared-memory stage: widened copies of the tile's offsets (raw[k] =
 // off[xa + k]), edge indices (idx[k] = idx[ya + k]), weights, and per-row arrays

@@ -1,5 +1,5 @@
-"""BFS over a 1-D vertex partition: one GraphSlice per rank, one bitmap
-all-gather per level.
+"""BFS and PageRank over a 1-D vertex partition: one GraphSlice per rank, one
+all-gather per level / iteration.
 
 The reference lays out per-GPU vertex ranges (``GraphSlice`` per GPU,
 GASengine/csr_problem.cuh:339-365) but its enactor only ever runs GPU 0
@@ -11,7 +11,11 @@ discoveries in an n-bit bitmap (push from its frontier vertices, or pull into
 its unvisited vertices), the ranks all-gather those bitmaps, and every rank folds
 the same world x words array into the same next frontier, so levels, directions
 (Beamer's rule) and depths agree everywhere without a second exchange. Depths
-equal the single-GPU BFS's.
+equal the single-GPU BFS's. PageRank (normalised, uniform teleport) keeps the
+whole iterate on every rank: a step computes the rank's own rows with the
+degree-binned gather over its in-edges, the slices are all-gathered, and the
+merge forms the next gather vector, the L1 change and the dangling mass with
+fixed-order sums, so every rank stops at the same iteration.
 
 Exchanges: :class:`CollectiveExchange` all-gathers over a torch.distributed
 group (NCCL on the slice's own CUDA stream, one GPU per rank; gloo for host
@@ -70,6 +74,10 @@ def slice_rows(row_offsets, col_idx, lo: int, hi: int, symmetric: bool = False):
 def _level(lv: "L.MgPartLevel") -> dict:
     return {"frontier": lv.frontier, "frontier_edges": lv.frontier_edges, "level": lv.level,
             "done": bool(lv.done), "direction": "pull" if lv.direction == L.MG_DIR_PULL else "push"}
+
+
+def _pr_level(lv: "L.MgPartLevel") -> dict:
+    return {"level": lv.level, "done": bool(lv.done), "residual": lv.residual}
 
 
 class GraphSlice:
@@ -169,6 +177,43 @@ class GraphSlice:
         _check(self._lib.mg_part_bfs_result(self._h, C.c_void_p(ptr), int(dev), C.byref(st)), "mg_part_bfs_result")
         return res, st.as_dict()
 
+    # -- PageRank (normalised, uniform teleport, unweighted) -------------------------
+    def pr_begin(self, alpha: float = 0.85, tol: float = 1e-6, max_iter: int = 50) -> dict:
+        o = L.MgPrOpts()
+        o.mode = L.MG_PR_NORMALIZED
+        o.alpha, o.tol, o.max_iter = float(alpha), float(tol), int(max_iter)
+        lv = L.MgPartLevel()
+        _check(self._lib.mg_part_pr_begin(self._h, C.byref(o), C.byref(lv)), "mg_part_pr_begin")
+        return _pr_level(lv)
+
+    def pr_step(self, slice_) -> None:
+        """This rank's new ranks of [lo, hi) into the first hi - lo entries of
+        `slice_` (float32 CUDA tensor), on the slice's stream."""
+        if not (_is_torch(slice_) and slice_.is_cuda and slice_.numel() >= self.hi - self.lo):
+            raise ValueError(f"slice must be a CUDA tensor of at least {self.hi - self.lo} floats")
+        _check(self._lib.mg_part_pr_step(self._h, C.c_void_p(slice_.data_ptr())), "mg_part_pr_step")
+
+    def pr_merge(self, gathered, world: int, stride: int, cuts) -> dict:
+        if not (_is_torch(gathered) and gathered.is_cuda and gathered.numel() >= world * stride):
+            raise ValueError(f"gathered must be a CUDA tensor of {world} x {stride} floats")
+        c = np.ascontiguousarray(cuts, dtype=np.int64)
+        lv = L.MgPartLevel()
+        _check(self._lib.mg_part_pr_merge(self._h, C.c_void_p(gathered.data_ptr()), int(world), int(stride),
+                                          c.ctypes.data, C.byref(lv)), "mg_part_pr_merge")
+        return _pr_level(lv)
+
+    def pr_result(self, out=None):
+        """(ranks of all n vertices, stats) of the last PageRank run."""
+        if out is None:
+            res = np.empty(self.n, dtype=np.float32)
+            ptr, dev = res.ctypes.data, False
+        else:
+            res = out
+            ptr, dev = (out.data_ptr(), bool(out.is_cuda)) if _is_torch(out) else (out.ctypes.data, False)
+        st = L.MgStats()
+        _check(self._lib.mg_part_pr_result(self._h, C.c_void_p(ptr), int(dev), C.byref(st)), "mg_part_pr_result")
+        return res, st.as_dict()
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.mg_part_destroy(self._h)
@@ -258,3 +303,45 @@ def bfs_partitioned_local(parts, srcs, direction: str = "auto", iter_num: int = 
     depth, st = parts[0].result(out)
     st["directions"] = levels
     return depth, st
+
+
+def pagerank_partitioned(part, cuts, exchange, alpha: float = 0.85, tol: float = 1e-6, max_iter: int = 50,
+                         out=None):
+    """Normalised PageRank (uniform teleport) over the ranks of `exchange`; every
+    rank calls it with its slice and the same cuts. Each iteration all-gathers
+    the ranks' new values of their own vertices (slices padded to the largest).
+    Returns (ranks of all n vertices, stats) on every rank."""
+    import torch
+
+    cuts = np.asarray(cuts, dtype=np.int64)
+    stride = int(np.diff(cuts).max()) if cuts.size > 1 else 0
+    device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
+    buf = torch.zeros(max(stride, 1), dtype=torch.float32, device=getattr(part, "device", device))
+    lv = part.pr_begin(alpha, tol, max_iter)
+    while not lv["done"]:
+        part.pr_step(buf)
+        gathered = exchange.gather(part, buf)
+        lv = part.pr_merge(gathered, exchange.world, max(stride, 1), cuts)
+    return part.pr_result(out)
+
+
+def pagerank_partitioned_local(parts, cuts, alpha: float = 0.85, tol: float = 1e-6, max_iter: int = 50,
+                               out=None):
+    """The same PageRank with every slice on the current GPU (one shared buffer
+    stands in for the all-gather). Returns the first slice's ranks and stats."""
+    import torch
+
+    cuts = np.asarray(cuts, dtype=np.int64)
+    world = len(parts)
+    stride = max(int(np.diff(cuts).max()), 1)
+    buf = torch.zeros(world * stride, dtype=torch.float32, device="cuda")
+    lvs = [p.pr_begin(alpha, tol, max_iter) for p in parts]
+    while not lvs[0]["done"]:
+        for r, p in enumerate(parts):
+            p.pr_step(buf[r * stride:(r + 1) * stride])
+        for p in parts:
+            p.synchronize()
+        lvs = [p.pr_merge(buf, world, stride, cuts) for p in parts]
+        if any(lv != lvs[0] for lv in lvs[1:]):
+            raise RuntimeError(f"partitions disagree on the iteration state: {lvs}")
+    return parts[0].pr_result(out)

@@ -198,6 +198,7 @@ def test_hub_column_cache_partial(weighted):
         xb, stb = g.pagerank(mode="normalized", weighted=weighted, gather="binned")
         xh, _ = g.pagerank(mode="normalized", weighted=weighted, gather="cached", use_graph=False)
     assert (x == xh).all()
+    assert st["status_detail"] > 0 and stb["status_detail"] == 0  # cached columns reported
     assert st["iterations"] == stb["iterations"]
     xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, w, 0.85, 0.0, st["iterations"])
     assert np.abs(x - xr).sum() <= L1_TOL

@@ -1,7 +1,9 @@
-"""BFS over a 1-D vertex partition on the GPU (mg_part_* through the C ABI):
-slices of one graph run as separate partitions on one GPU, exchanging through a
-shared buffer, and as a one-rank NCCL group; depths bit-exact against the
-oracle and the single-GPU BFS, levels and traversed edges equal."""
+"""BFS and PageRank over a 1-D vertex partition on the GPU (mg_part_* through the
+C ABI): slices of one graph run as separate partitions on one GPU, exchanging
+through a shared buffer, and as a one-rank NCCL group. BFS depths bit-exact
+against the oracle and the single-GPU BFS, levels and traversed edges equal;
+PageRank within 1e-6 L1 of the FP64 oracle at the same iteration count, and the
+same iteration count as the single-GPU solver."""
 import os
 import socket
 
@@ -11,7 +13,10 @@ import pytest
 import oracle
 import mirrorofmapgraph_b200 as mg
 from mirrorofmapgraph_b200.partition import (CollectiveExchange, GraphSlice, bfs_partitioned,
-                                             bfs_partitioned_local, partition_cuts)
+                                             bfs_partitioned_local, pagerank_partitioned,
+                                             pagerank_partitioned_local, partition_cuts)
+
+PR_L1_TOL = 1e-6  # FP32 slices vs the FP64 oracle at the same iteration count
 
 pytestmark = pytest.mark.gpu
 
@@ -114,5 +119,58 @@ def test_partitioned_bfs_over_a_one_rank_nccl_group():
             out = torch.empty(h.n, dtype=torch.int32, device="cuda")
             d2, _ = bfs_partitioned(p, [1], CollectiveExchange(), out=out)
             np.testing.assert_array_equal(out.cpu().numpy(), ref)
+            x, st = pagerank_partitioned(p, [0, h.n], CollectiveExchange())
+            xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+            assert np.abs(x - xr).sum() <= PR_L1_TOL
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4])
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_partitioned_pagerank_matches_oracle_and_single_gpu(world, symmetric):
+    h = mg.gen_rmat(14, 8, 21, symmetrize=symmetric)
+    c = partition_cuts(h.row_offsets, world)
+    parts = _slices(h, world, symmetric)
+    try:
+        x, st = pagerank_partitioned_local(parts, c)
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+        assert np.abs(x - xr).sum() <= PR_L1_TOL
+        for p in parts[1:]:
+            np.testing.assert_array_equal(p.pr_result()[0], x)
+        with mg.Graph(h.row_offsets, h.col_idx, symmetric=symmetric) as g:
+            xs, ss = g.pagerank(mode="normalized", alpha=0.85, tol=1e-6, max_iter=50)
+        assert ss["iterations"] == st["iterations"]
+        assert np.abs(x - xs).sum() <= PR_L1_TOL
+        assert st["residual"] < 1e-6 or st["iterations"] == 50
+        x3, s3 = pagerank_partitioned_local(parts, c, max_iter=3)
+        assert s3["iterations"] == 3
+        xr3, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, 3)
+        assert np.abs(x3 - xr3).sum() <= PR_L1_TOL
+    finally:
+        for p in parts:
+            p.close()
+
+
+def test_partitioned_pagerank_hub_rows_and_protocol_errors():
+    h = mg.gen_rmat(15, 16, 4, symmetrize=True)  # rows of >= 2,048 edges: chunked hub rows
+    assert np.diff(h.row_offsets).max() >= 4096
+    c = partition_cuts(h.row_offsets, 3)
+    parts = _slices(h, 3, True)
+    try:
+        x, st = pagerank_partitioned_local(parts, c)
+        xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+        assert np.abs(x - xr).sum() <= PR_L1_TOL
+        import torch
+        buf = torch.zeros(h.n, dtype=torch.float32, device="cuda")
+        with pytest.raises(mg.MapGraphError):
+            parts[0].pr_merge(buf, 1, h.n, [0, h.n])  # no step pending
+        parts[0].pr_begin()
+        parts[0].pr_step(buf)
+        with pytest.raises(mg.MapGraphError):
+            parts[0].pr_step(buf)  # step twice
+        with pytest.raises(mg.MapGraphError):
+            parts[0].pr_merge(buf, 1, h.n, [0, h.n])  # cuts without this slice's range
+    finally:
+        for p in parts:
+            p.close()

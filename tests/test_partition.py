@@ -1,8 +1,9 @@
 """1-D vertex partition (host logic, CPU): cut points, row slices, and the level
-protocol of bfs_partitioned over two and three gloo ranks. Each rank's device
-step is stood in for by a NumPy slice with the GraphSlice method signatures
-(begin / step / merge / result on n-bit bitmaps); depths are checked against the
-oracle's BFS."""
+protocols of bfs_partitioned and pagerank_partitioned over two and three gloo
+ranks. Each rank's device step is stood in for by a NumPy slice with the
+GraphSlice method signatures (begin / step / merge / result on n-bit bitmaps;
+pr_begin / pr_step / pr_merge / pr_result on padded float slices); depths and
+ranks are checked against the oracle."""
 import os
 import socket
 
@@ -129,10 +130,42 @@ class _NumpySlice:
     def result(self, out=None):
         return self.depth.copy(), {"iterations": self.level, "edges_traversed": self.vdeg}
 
+    # PageRank protocol (normalised, uniform teleport): FP64 stand-in.
+    def pr_begin(self, alpha=0.85, tol=1e-6, max_iter=50):
+        self.alpha, self.tol, self.max_iter = alpha, tol, max_iter
+        self.x = np.full(self.n, 1.0 / self.n)
+        self.plevel, self.resid = 0, 0.0
+        self.pdone = max_iter <= 0
+        return {"level": 0, "done": self.pdone, "residual": 0.0}
+
+    def _y(self):
+        return np.where(self.deg > 0, self.x / np.maximum(self.deg, 1), 0.0)
+
+    def pr_step(self, slice_):
+        import torch
+        y, t = self._y(), 1.0 / self.n
+        d = self.x[self.deg == 0].sum()
+        v = np.arange(self.lo, self.hi)
+        acc = np.array([y[self.ri[self.co[u]:self.co[u + 1]]].sum() for u in v])
+        slice_[: self.hi - self.lo] = torch.from_numpy((self.alpha * (acc + d * t) + (1 - self.alpha) * t)
+                                                       .astype(np.float32))
+
+    def pr_merge(self, gathered, world, stride, cuts):
+        g = gathered.numpy().reshape(world, stride).astype(np.float64)
+        new = np.concatenate([g[r, : cuts[r + 1] - cuts[r]] for r in range(world)])
+        self.resid = float(np.abs(new - self.x).sum())
+        self.x = new
+        self.plevel += 1
+        self.pdone = self.resid < self.tol or self.plevel >= self.max_iter
+        return {"level": self.plevel, "done": self.pdone, "residual": self.resid}
+
+    def pr_result(self, out=None):
+        return self.x.copy(), {"iterations": self.plevel, "residual": self.resid}
+
 
 def _worker(rank, world, port, out_dir):
     import torch.distributed as dist
-    from mirrorofmapgraph_b200.partition import CollectiveExchange, bfs_partitioned
+    from mirrorofmapgraph_b200.partition import CollectiveExchange, bfs_partitioned, pagerank_partitioned
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
@@ -146,6 +179,9 @@ def _worker(rank, world, port, out_dir):
                 res[f"{name}_{mode}"] = d
                 res[f"{name}_{mode}_levels"] = np.array([st["iterations"], st["edges_traversed"]])
                 res[f"{name}_{mode}_dirs"] = np.array([x == "pull" for x in st["directions"]])
+            x, st = pagerank_partitioned(part, c, ex)
+            res[f"{name}_pr"] = x
+            res[f"{name}_pr_iters"] = np.array([st["iterations"]])
         np.savez(os.path.join(out_dir, f"r{rank}.npz"), **res)
     finally:
         dist.destroy_process_group()
@@ -175,6 +211,12 @@ def test_partitioned_bfs_protocol_over_gloo_ranks(tmp_path, world):
             assert lv[0] == ref.max() + 1
             assert lv[1] == int(np.diff(h.row_offsets)[ref >= 0].sum())
             dirs = z0[f"{name}_{mode}_dirs"]
+            it = int(z0[f"{name}_pr_iters"][0])
+            xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, it)
+            for r in range(world):
+                z = np.load(tmp_path / f"r{r}.npz")
+                assert np.abs(z[f"{name}_pr"] - xr).sum() <= 1e-6
+                np.testing.assert_array_equal(z[f"{name}_pr"], z0[f"{name}_pr"])
             if mode == "push":
                 assert not dirs.any()
             if mode == "pull":
