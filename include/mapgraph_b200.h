@@ -319,6 +319,18 @@ mg_status mg_part_pr_merge(mg_part *p, const float *gathered, int32_t world, int
 /* Ranks of all n vertices (host or device output) and the run's counters. */
 mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_stats *stats);
 
+/* ---- Test hooks: host-side fault injection ----------------------------------
+ * For failure-path tests; nothing here faults, traps or hangs a device.
+ * mg_debug_fail_alloc(k): the k-th device allocation from now, and every later
+ *   one, fails as if the device were out of memory (the call in progress returns
+ *   MG_ERR_OOM); k = 0 disarms.
+ * mg_debug_barrier_skew(extra, poll_limit): the persistent BFS kernel's grid
+ *   barriers wait for `extra` arrivals more than there are blocks, polling at
+ *   most poll_limit times, so the next mg_bfs that takes the persistent path
+ *   returns MG_ERR_TIMEOUT and leaves the device usable; extra = 0 restores. */
+mg_status mg_debug_fail_alloc(int64_t k);
+mg_status mg_debug_barrier_skew(int32_t extra, int64_t poll_limit);
+
 #ifdef __cplusplus
 }
 #endif

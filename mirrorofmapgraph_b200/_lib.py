@@ -115,6 +115,8 @@ SIGNATURES = {
     "mg_part_pr_step": (C.c_int, [_P, _P]),
     "mg_part_pr_merge": (C.c_int, [_P, _P, C.c_int32, C.c_int64, _P, C.POINTER(MgPartLevel)]),
     "mg_part_pr_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
+    "mg_debug_fail_alloc": (C.c_int, [C.c_int64]),
+    "mg_debug_barrier_skew": (C.c_int, [C.c_int32, C.c_int64]),
 }
 
 _lib = None

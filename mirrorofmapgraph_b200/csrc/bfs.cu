@@ -58,6 +58,8 @@ struct BfsArgs {
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
+  uint32_t bar_extra;            // test hook (mg_debug_barrier_skew): a barrier that cannot complete
+  unsigned long long bar_limit;  // barrier polls before MG_ERR_TIMEOUT
 };
 
 __device__ void bfs_level_end(const BfsArgs &a) {
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
       if (bins) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)bins);
       if (bexp) atomicAdd((unsigned long long *)&c->vertices_expanded, (unsigned long long)bexp);
     }
-    if (!grid_barrier(&c->bar_count, &c->bar_gen, PERSIST_WAIT)) {
+    if (!grid_barrier(&c->bar_count, &c->bar_gen, a.bar_limit, a.bar_extra)) {
       if (threadIdx.x == 0) {
         c->status = MG_ERR_TIMEOUT;
         c->done = 1;
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
       expand_big<BFS_NT>(sm.b, a.ro, big, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
       const int64_t bmf2 = block_sum<BFS_NT>(x.mf, s_sum);
       if (threadIdx.x == 0 && bmf2) atomicAdd((unsigned long long *)&c->pm[out], (unsigned long long)bmf2);
-      if (!grid_barrier(&c->bar_count, &c->bar_gen, PERSIST_WAIT)) {
+      if (!grid_barrier(&c->bar_count, &c->bar_gen, a.bar_limit, a.bar_extra)) {
         if (threadIdx.x == 0) {
           c->status = MG_ERR_TIMEOUT;
           c->done = 1;
@@ -494,6 +496,8 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   a.ctl = g->ctl;
   a.h = 0;
   a.use_cond = 0;
+  a.bar_extra = (uint32_t)debug_barrier_extra();
+  a.bar_limit = a.bar_extra ? debug_barrier_limit() : PERSIST_WAIT;
 
   const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
   MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
@@ -679,6 +683,8 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   a.ctl = g->ctl;
   a.h = 0;
   a.use_cond = 0;
+  a.bar_extra = (uint32_t)debug_barrier_extra();
+  a.bar_limit = a.bar_extra ? debug_barrier_limit() : PERSIST_WAIT;
 
   const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
   MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));

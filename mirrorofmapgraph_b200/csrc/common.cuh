@@ -92,14 +92,18 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // wait is bounded: after `limit` polls the block gives up and the function
 // returns false (the caller reports MG_ERR_TIMEOUT and stops), so a missing
 // block cannot hang the GPU. Every thread of every block must call it.
-__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned long long limit) {
+// `extra` raises the number of arrivals the barrier waits for (a test hook: a
+// barrier that cannot complete, to check that the bounded wait reports
+// MG_ERR_TIMEOUT); 0 in normal runs.
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned long long limit,
+                                             unsigned extra = 0) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned g = *(volatile unsigned *)gen;  // read before arriving: gen moves only after every arrival
     __threadfence();
     int ok = 1;
-    if (atomicAdd(count, 1u) + 1 == gridDim.x) {
+    if (atomicAdd(count, 1u) + 1 == gridDim.x + extra) {
       *count = 0;
       __threadfence();
       atomicAdd(gen, 1u);

@@ -11,6 +11,7 @@
 // CSR edge id, which makes it identical to the reference's stable sort by column
 // (within a column, edges in CSR order) and therefore deterministic.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdarg>
 #include <cstring>
@@ -31,9 +32,49 @@ void mg_set_error(const char *fmt, ...) {
   va_end(ap);
 }
 
+// Test hooks: host-side fault injection (no device fault is ever caused).
+// g_fail_alloc: 0 off; k > 0: the k-th allocation from now and every later one
+// fail (until the hook is disarmed), so no retry can mask the failure.
+static std::atomic<int64_t> g_fail_alloc{0};
+static std::atomic<int32_t> g_bar_extra{0};
+static std::atomic<unsigned long long> g_bar_limit{1ull << 12};
+
+cudaError_t mg_malloc_async(void **p, size_t bytes, cudaStream_t s) {
+  int64_t k = g_fail_alloc.load();
+  while (k > 1 && !g_fail_alloc.compare_exchange_weak(k, k - 1)) {
+  }
+  if (k == 1) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocAsync(p, bytes, s);
+}
+
+int32_t debug_barrier_extra() { return g_bar_extra.load(); }
+unsigned long long debug_barrier_limit() { return g_bar_limit.load(); }
+
+extern "C" mg_status mg_debug_fail_alloc(int64_t k) {
+  if (k < 0) {
+    mg_set_error("mg_debug_fail_alloc: k must be >= 0");
+    return MG_ERR_ARG;
+  }
+  g_fail_alloc.store(k);
+  return MG_OK;
+}
+
+extern "C" mg_status mg_debug_barrier_skew(int32_t extra, int64_t poll_limit) {
+  if (extra < 0 || poll_limit <= 0) {
+    mg_set_error("mg_debug_barrier_skew: extra must be >= 0 and poll_limit > 0");
+    return MG_ERR_ARG;
+  }
+  g_bar_extra.store(extra);
+  g_bar_limit.store((unsigned long long)poll_limit);
+  return MG_OK;
+}
+
 mg_status dev_alloc(mg_graph *g, void **p, size_t bytes) {
   *p = nullptr;
-  cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), g->stream);
+  cudaError_t e = mg_malloc_async(p, std::max<size_t>(bytes, 1), g->stream);
   if (e == cudaErrorMemoryAllocation) {
     // Return the pool's idle blocks to the driver and try once more.
     cudaGetLastError();
@@ -41,7 +82,7 @@ mg_status dev_alloc(mg_graph *g, void **p, size_t bytes) {
     if (cudaStreamSynchronize(g->stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess)
       cudaMemPoolTrimTo(pool, 0);
     cudaGetLastError();
-    e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), g->stream);
+    e = mg_malloc_async(p, std::max<size_t>(bytes, 1), g->stream);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -420,12 +461,12 @@ static mg_status build_csc(mg_graph *g) {
   const int64_t n = g->n, m = g->m;
   cudaStream_t s = g->stream;
   const size_t vbytes = g->vtype == MG_DTYPE_NONE ? 0 : 4;
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->co, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->ri, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
-  MG_CUDA_TRY(cudaMallocAsync((void **)&g->perm, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
-  if (vbytes) MG_CUDA_TRY(cudaMallocAsync(&g->cvals, vbytes * (m + MG_EDGE_PAD), s));
+  g->csc_owned = true;  // set first: a failure below frees what was allocated
+  MG_CUDA_TRY(mg_malloc_async((void **)&g->co, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
+  MG_CUDA_TRY(mg_malloc_async((void **)&g->ri, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  MG_CUDA_TRY(mg_malloc_async((void **)&g->perm, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  if (vbytes) MG_CUDA_TRY(mg_malloc_async(&g->cvals, vbytes * (m + MG_EDGE_PAD), s));
   mg::fill_pad_kernel<<<1, 32, 0, s>>>(g->co, n, g->ri, g->cvals, m);
-  g->csc_owned = true;
   g->has_csc = true;
   const int64_t ntiles = std::max<int64_t>(1, (n + SCAN_TILE - 1) / SCAN_TILE);
   const size_t need = Carve::need({sizeof(int32_t) * (size_t)(n + 1), sizeof(int32_t) * (size_t)(n + 1),
@@ -605,9 +646,9 @@ static mg_status create_impl(const int32_t *row_offsets, const int32_t *col_idx,
       return fail(_e == cudaErrorMemoryAllocation ? MG_ERR_OOM : MG_ERR_CUDA);                  \
     }                                                                                           \
   } while (0)
-  CREATE_TRY(cudaMallocAsync((void **)&g->ro, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
-  CREATE_TRY(cudaMallocAsync((void **)&g->ci, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
-  if (vb) CREATE_TRY(cudaMallocAsync(&g->vals, vb * (m + MG_EDGE_PAD), s));
+  CREATE_TRY(mg_malloc_async((void **)&g->ro, sizeof(int32_t) * (n + 1 + MG_OFF_PAD), s));
+  CREATE_TRY(mg_malloc_async((void **)&g->ci, sizeof(int32_t) * (m + MG_EDGE_PAD), s));
+  if (vb) CREATE_TRY(mg_malloc_async(&g->vals, vb * (m + MG_EDGE_PAD), s));
   mg::fill_pad_kernel<<<1, 32, 0, s>>>(g->ro, n, g->ci, g->vals, m);
   CREATE_TRY(cudaMemcpyAsync(g->ro, row_offsets, sizeof(int32_t) * (n + 1), kind, s));
   if (m > 0) CREATE_TRY(cudaMemcpyAsync(g->ci, col_idx, sizeof(int32_t) * m, kind, s));

@@ -69,6 +69,7 @@ struct DevCtl {
   int64_t pm[3];
   int32_t pq[3];
   int32_t pb[3];  // deferred big vertices per level (persistent BFS)
+  int32_t tile_next;  // next frontier tile of the dynamic schedule (SSSP rounds; reset at level end)
   uint32_t bar_count;
   uint32_t bar_gen;
 };
@@ -116,6 +117,16 @@ struct mg_graph {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   void *cache = nullptr;       // cached executable loop graphs (engine.cu)
 };
+
+// Every device allocation of the library goes through here: cudaMallocAsync on
+// stream s, unless the allocation-failure test hook (mg_debug_fail_alloc) says
+// this one fails, in which case it returns cudaErrorMemoryAllocation without
+// allocating.
+cudaError_t mg_malloc_async(void **p, size_t bytes, cudaStream_t s);
+// Barrier test hook (mg_debug_barrier_skew): extra arrivals the persistent
+// kernels' grid barriers wait for (0 normally) and their poll budget then.
+int32_t debug_barrier_extra();
+unsigned long long debug_barrier_limit();
 
 // Device memory of a graph's workspaces and plans, taken from the device's
 // stream-ordered pool on the graph's stream: freed blocks stay in the pool, so a

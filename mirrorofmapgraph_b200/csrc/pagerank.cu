@@ -89,8 +89,14 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
     const int64_t items = g->n + g->m;
     const int64_t nt = (items + PRG_IPC - 1) / PRG_IPC;
     p.ntiles = (int32_t)std::max<int64_t>(nt, 1);
-    MG_TRY(dev_alloc(g, (void **)&p.tx, sizeof(int32_t) * (p.ntiles + 1)));
-    MG_TRY(dev_alloc(g, (void **)&p.ty, sizeof(int32_t) * (p.ntiles + 1)));
+    mg_status st = dev_alloc(g, (void **)&p.tx, sizeof(int32_t) * (p.ntiles + 1));
+    if (st == MG_OK) st = dev_alloc(g, (void **)&p.ty, sizeof(int32_t) * (p.ntiles + 1));
+    if (st != MG_OK) {  // no half-built plan survives a failure
+      dev_free(g, p.tx);
+      dev_free(g, p.ty);
+      p.tx = p.ty = nullptr;
+      return st;
+    }
     prg_plan_kernel<<<(p.ntiles + 256) / 256, 256, 0, g->stream>>>(csr ? g->ro : g->co, g->n, g->m, p.ntiles, p.tx,
                                                                     p.ty);
     MG_CUDA_TRY(cudaGetLastError());
@@ -102,10 +108,10 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
 // Degree-binned plan of any row-offset array (n + 1 entries) on stream s: the
 // CSC of a graph (forward gather), its CSR (adjoint, row sums) or the owned rows
 // of a partition slice.
-mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
+static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
   using namespace mg;
   auto alloc = [&](void **p, size_t bytes) -> mg_status {
-    if (cudaMallocAsync(p, std::max<size_t>(bytes, 4), s) != cudaSuccess) {
+    if (mg_malloc_async(p, std::max<size_t>(bytes, 4), s) != cudaSuccess) {
       cudaGetLastError();
       *p = nullptr;
       mg_set_error("PageRank plan: device allocation of %zu bytes failed", bytes);
@@ -115,7 +121,7 @@ mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinP
   };
   const int64_t nchunks = std::max<int64_t>(1, (n + PRB_CHUNK_ROWS - 1) / PRB_CHUNK_ROWS);
   int64_t *counts = nullptr;
-  MG_CUDA_TRY(cudaMallocAsync((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
+  MG_CUDA_TRY(mg_malloc_async((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
   int64_t *totals = counts + nchunks * (PRB_BINS + 1);
   int64_t *dboff = totals + (PRB_BINS + 1);
   prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts);
@@ -155,6 +161,14 @@ mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinP
   MG_CUDA_TRY(cudaGetLastError());
   MG_CUDA_TRY(cudaFreeAsync(counts, s));
   return MG_OK;
+}
+
+// A failed build releases what it had allocated.
+mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
+  bp = mg::BinPlan();
+  const mg_status st = bin_plan_build_impl(s, off, n, bp);
+  if (st != MG_OK) bin_plan_release(s, bp);
+  return st;
 }
 
 void bin_plan_release(cudaStream_t s, mg::BinPlan &bp) {
@@ -695,10 +709,18 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
     hc = HubCache();
   }
   if (!hc.ok) {
+    // leftovers of a build that failed part-way
+    for (void *q : {(void *)hc.cidx, (void *)hc.slot, (void *)hc.hv}) dev_free(g, q);
+    hc = HubCache();
     const int64_t n = g->n, m = g->m;
     cudaStream_t s = g->stream;
     unsigned *hist = nullptr;
-    MG_CUDA_TRY(cudaMallocAsync((void **)&hist, sizeof(unsigned) * (65536 + 1), s));
+    MG_CUDA_TRY(mg_malloc_async((void **)&hist, sizeof(unsigned) * (65536 + 1), s));
+    auto alloc = [&](void **q, size_t bytes) -> mg_status {
+      const mg_status st = dev_alloc(g, q, bytes);
+      if (st != MG_OK) dev_free(g, hist);
+      return st;
+    };
     MG_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(unsigned) * (65536 + 1), s));
     hub_hist_kernel<<<g->num_sms * 4, 256, 0, s>>>(g->ro, n, hist);
     std::vector<unsigned> h(65536);
@@ -711,9 +733,9 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
       cum += h[d];
       thr = d;
     }
-    MG_TRY(dev_alloc(g, (void **)&hc.slot, sizeof(int32_t) * std::max<int64_t>(n, 1)));
-    MG_TRY(dev_alloc(g, (void **)&hc.hv, sizeof(int32_t) * std::max<int64_t>(cap, 1)));
-    MG_TRY(dev_alloc(g, (void **)&hc.cidx, sizeof(int32_t) * (m + 8)));
+    MG_TRY(alloc((void **)&hc.slot, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    MG_TRY(alloc((void **)&hc.hv, sizeof(int32_t) * std::max<int64_t>(cap, 1)));
+    MG_TRY(alloc((void **)&hc.cidx, sizeof(int32_t) * (m + 8)));
     unsigned *count = hist + 65536;
     hub_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(g->ro, n, thr, cap, hc.slot, hc.hv, count);
     hub_remap_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ri, m, hc.slot, hc.cidx);

@@ -384,7 +384,7 @@ struct mg_part {
 namespace {
 
 mg_status part_alloc(mg_part *p, void **ptr, size_t bytes) {
-  cudaError_t e = cudaMallocAsync(ptr, std::max<size_t>(bytes, 4), p->stream);
+  cudaError_t e = mg_malloc_async(ptr, std::max<size_t>(bytes, 4), p->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     *ptr = nullptr;

@@ -27,6 +27,9 @@ namespace mg {
 
 constexpr int SSSP_NT = 256;
 constexpr int SSSP_CTA_TH = 512;
+#ifndef MG_SSSP_DYNAMIC
+#define MG_SSSP_DYNAMIC 1
+#endif
 
 struct SsspArgs {
   const int32_t *ro, *ci, *w;   // CSR with weights (w == nullptr: unit weights)
@@ -105,6 +108,7 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   c->cur = cur ^ 1;
   c->blocks_done = 0;
   c->big_len = 0;
+  c->tile_next = 0;
   const bool over = vload(&c->overflow) != 0;
   // near-far: an empty near frontier with vertices waiting in the far pile is a
   // split (the far kernels refill the near frontier), not the end
@@ -135,7 +139,19 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
   const BigList big{a.big_v, &c->big_len, defer_threshold<SSSP_NT>(nin, SSSP_CTA_TH)};
+#if MG_SSSP_DYNAMIC
+  // Tiles of the frontier are handed out one at a time from a counter (reset at
+  // the end of the round), so CTAs that drew light tiles take more.
+  __shared__ int32_t s_tile;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&c->tile_next, 1);
+    __syncthreads();
+    const int64_t tile = (int64_t)s_tile * SSSP_NT;
+    __syncthreads();
+    if (tile >= nin) break;
+#else
   for (int64_t tile = (int64_t)blockIdx.x * SSSP_NT; tile < nin; tile += (int64_t)gridDim.x * SSSP_NT) {
+#endif
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
     if (v >= 0) {

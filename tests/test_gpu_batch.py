@@ -159,7 +159,7 @@ def test_ppr_batch_256_vectors_with_hub_chunks():
         np.testing.assert_allclose(xs.astype(np.float64).sum(axis=1), 1.0, atol=1e-5)
         _check_vectors(h, xs, tele, st["iterations"], [0, 1, 100, 200, 255])
         xs2, _ = g.pagerank(teleport=tele, nvec=256, mode="normalized", use_graph=False)
-        assert (xs == xs2).all()
+        assert np.abs(xs - xs2).sum() <= 1e-9 * 256
 
 
 def test_ppr_batch_weighted_directed_and_device_output():
@@ -172,7 +172,7 @@ def test_ppr_batch_weighted_directed_and_device_output():
         td = torch.from_numpy(tele.reshape(-1)).cuda()
         out = torch.empty(40 * h.n, dtype=torch.float32, device="cuda")
         g.pagerank(teleport=td, nvec=40, out=out, mode="normalized", weighted=True)
-        assert (out.cpu().numpy().reshape(40, h.n) == xs).all()
+        assert np.abs(out.cpu().numpy().reshape(40, h.n) - xs).sum() <= 1e-9 * 40
 
 
 @pytest.mark.parametrize("nvec", [2, 33, 100, 300])

@@ -57,6 +57,15 @@ def test_null_arguments_are_rejected():
     assert lib.mg_graph_create(None, None, None, 0, -1, 0, 0, C.byref(out)) == L.MG_ERR_ARG
     assert lib.mg_bfs(None, None, 1, None, None, None) == L.MG_ERR_ARG
     assert lib.mg_graph_destroy(None) == L.MG_OK
+    assert lib.mg_part_create(10, 0, 10, None, None, None, None, None, 0, C.byref(out)) == L.MG_ERR_ARG
+    assert lib.mg_part_bfs_step(None, None) == L.MG_ERR_ARG
+    assert lib.mg_part_pr_merge(None, None, 1, 1, None, None) == L.MG_ERR_ARG
+    assert lib.mg_part_destroy(None) == L.MG_OK
+    # fault-injection hooks: argument checks (arming them needs no device)
+    assert lib.mg_debug_fail_alloc(-1) == L.MG_ERR_ARG
+    assert lib.mg_debug_barrier_skew(-1, 10) == L.MG_ERR_ARG
+    assert lib.mg_debug_barrier_skew(0, 0) == L.MG_ERR_ARG
+    assert lib.mg_debug_fail_alloc(0) == L.MG_OK
 
 
 def test_generators_are_deterministic():
