@@ -283,6 +283,53 @@ def cpu_reference_run(h, src):
     return {"bfs": (eb, tb), "cc": (h.m, tc), "pagerank": (h.m * max(sweeps, 0), tp), "pr_sweeps": sweeps}
 
 
+def host_info() -> dict:
+    """Host cores and CPU model (the CPU figures are quoted with them)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except Exception:
+        ncores = os.cpu_count() or 1
+    return {"nproc": ncores, "cpu_model": model}
+
+
+def cpu_restatements(hs, src) -> dict:
+    """Timed FP64/int restatements (oracle/) of the paths the reference has no CPU
+    code for at these sizes, on the CPU sample graph, single-threaded: Dijkstra
+    SSSP (the reference's CPUSSSP is O(n^2): hours at scale 22), one personalised
+    PageRank vector and the PageRank adjoint."""
+    import oracle
+    out = {}
+    t0 = time.perf_counter()
+    d = oracle.sssp(hs.row_offsets, hs.col_idx, hs.weights_i32, [src])
+    t = time.perf_counter() - t0
+    deg = np.diff(hs.row_offsets).astype(np.int64)
+    out["sssp_dijkstra"] = {"gteps": float(deg[d < 2**31 - 1].sum()) / t / 1e9, "s": t,
+                            "kind": "restatement (heap Dijkstra, int32)"}
+    tele = np.zeros(hs.n)
+    tele[np.random.default_rng(SEED + 3).choice(hs.n, 16, replace=False)] = 1.0 / 16
+    t0 = time.perf_counter()
+    x, it, _ = oracle.pr_normalized(hs.row_offsets, hs.col_idx, None, ALPHA, PR_TOL, PR_MAX_IT, teleport=tele)
+    t = time.perf_counter() - t0
+    out["ppr_vector"] = {"gteps": hs.m * it / t / 1e9, "s": t, "iterations": int(it),
+                         "kind": "restatement (FP64 power iteration)"}
+    wv = np.random.default_rng(SEED + 4).standard_normal(hs.n)
+    t0 = time.perf_counter()
+    _, _, _, ita = oracle.pr_adjoint(hs.row_offsets, hs.col_idx, None, x, wv, ALPHA, 1e-9, 400)
+    t = time.perf_counter() - t0
+    out["pagerank_adjoint"] = {"gteps": hs.m * ita / t / 1e9, "s": t, "iterations": int(ita),
+                               "kind": "restatement (FP64 adjoint solve + edge gradients)"}
+    return out
+
+
 def cpu_sample_graph():
     import mirrorofmapgraph_b200 as mg
     return mg.gen_rmat(CPU_SAMPLE_SCALE, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
@@ -355,6 +402,7 @@ def run_reference(args):
             "data": "synthetic (seeded R-MAT)",
             "config": {"workload": f"rmat_s{CPU_SAMPLE_SCALE}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
                                    "CPUBFS + CPUCC + CPUPR", "scale": CPU_SAMPLE_SCALE, "n": h.n, "m": h.m},
+            "host": host_info(),
             "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs, "kind": "reference",
                              "sample": f"{procs} concurrent copies of the reference's serial CPUBFS/CPUCC/CPUPR, "
                                        f"each {args.steps} step(s) on R-MAT scale {CPU_SAMPLE_SCALE} from its own "
@@ -567,7 +615,11 @@ def run_ours(args):
                     "value": ce / cs / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
                     "sample": f"reference CPUBFS + CPUCC + CPUPR (serial, oracle/_ref) once on R-MAT scale "
                               f"{CPU_SAMPLE_SCALE} (same generator); {cs:.1f} s of CPU work",
-                    "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")}}
+                    "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")},
+                    "host": host_info(),
+                    "sssp": "reference CPUSSSP not run: O(n^2), hours at scale 22 (timed at the 4,096-vertex "
+                            "ER case in the tests); see restatements",
+                    "restatements": cpu_restatements(hs, sources(hs, 1, SEED + 1)[0])}
             else:
                 line["cpu_baseline"] = {"value": None, "unavailable": "oracle/_ref not built"}
         except Exception as e:

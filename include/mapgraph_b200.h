@@ -319,6 +319,27 @@ mg_status mg_part_pr_merge(mg_part *p, const float *gathered, int32_t world, int
 /* Ranks of all n vertices (host or device output) and the run's counters. */
 mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_stats *stats);
 
+/* ---- Per-level trace of the last run ----------------------------------------
+ * What the reference prints with verbose=1 (frontier size per iteration,
+ * GASengine/enactor_vertex_centric.cuh:2528-2546), recorded on the device by the
+ * level-end code of mg_bfs, mg_sssp and single-vector mg_pagerank (MG_PR_NORMALIZED)
+ * on a graph, for the first MG_TRACE_LEVELS levels. One record per level:
+ *   BFS:      frontier = vertices expanded, frontier_edges = their out-edges,
+ *             direction = MG_DIR_PUSH / MG_DIR_PULL;
+ *   SSSP:     frontier = vertices relaxed, frontier_edges = out-edges of the
+ *             vertices this round improved;
+ *   PageRank: frontier = n, value = the iteration's L1 change.
+ * *count = records written (min(levels, cap, MG_TRACE_LEVELS)). */
+#define MG_TRACE_LEVELS 4096
+typedef struct mg_level_record {
+  int32_t level;
+  int32_t direction;
+  int64_t frontier;
+  int64_t frontier_edges;
+  double value;
+} mg_level_record;
+mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count);
+
 /* ---- Test hooks: host-side fault injection ----------------------------------
  * For failure-path tests; nothing here faults, traps or hangs a device.
  * mg_debug_fail_alloc(k): the k-th device allocation from now, and every later

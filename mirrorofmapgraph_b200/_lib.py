@@ -57,6 +57,14 @@ class MgPartLevel(C.Structure):
                 ("residual", C.c_double)]
 
 
+class MgLevelRecord(C.Structure):
+    _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_int64),
+                ("frontier_edges", C.c_int64), ("value", C.c_double)]
+
+
+MG_TRACE_LEVELS = 4096
+
+
 class MgHostCsr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("row_offsets", C.POINTER(C.c_int32)),
                 ("col_idx", C.POINTER(C.c_int32)), ("weights_i32", C.POINTER(C.c_int32)),
@@ -115,6 +123,7 @@ SIGNATURES = {
     "mg_part_pr_step": (C.c_int, [_P, _P]),
     "mg_part_pr_merge": (C.c_int, [_P, _P, C.c_int32, C.c_int64, _P, C.POINTER(MgPartLevel)]),
     "mg_part_pr_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
+    "mg_graph_trace": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "mg_debug_fail_alloc": (C.c_int, [C.c_int64]),
     "mg_debug_barrier_skew": (C.c_int, [C.c_int32, C.c_int64]),
 }

@@ -69,6 +69,8 @@ __device__ void bfs_level_end(const BfsArgs &a) {
   const int64_t mf = vload(&c->mf_next);
   const int64_t vdeg = vload(&c->visited_deg) + mf;
   const int lvl = vload(&c->level) + 1;
+  trace_level(c, lvl - 1, vload(&c->dir) == 1 ? MG_DIR_PULL : MG_DIR_PUSH, vload(&c->qlen[cur]),
+              vload(&c->mf_front), 0.0);
   c->visited_deg = vdeg;
   c->mf_front = mf;
   c->level = lvl;
@@ -257,6 +259,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
       }
     }
     // Level end (bfs_level_end's rules), computed alike in every block.
+    if (blockIdx.x == 0 && threadIdx.x == 0) trace_level(c, lvl, MG_DIR_PUSH, nin, mf, 0.0);
     const int32_t nf = vload(&c->pq[out]);
     mf = vload(&c->pm[out]);
     vdeg += mf;

@@ -29,6 +29,7 @@ int main(int argc, char **argv) {
     std::printf("num_srcs=%d, src=%d, iter_num=%d\n", (int)srcs.size(), s, o.iter_num);
     mg_stats st;
     mgcli::check(mg_bfs(g, &s, 1, depth.data(), &o, &st), "mg_bfs");
+    mgcli::print_trace(cfg, g);
     std::printf("Kernel time took: %.4f ms\n", st.kernel_ms);
     std::printf("Total iteration: %lld\n", (long long)st.iterations);
     std::printf("Traversed edge: %lld\n", (long long)st.edges_traversed);

@@ -164,6 +164,18 @@ std::vector<int32_t> select_sources(const Config &cfg, const Args &args, const m
   return srcs;
 }
 
+void print_trace(const Config &cfg, mg_graph *g) {
+  if (cfg.getInt("verbose") == 0) return;
+  std::vector<mg_level_record> rec(MG_TRACE_LEVELS);
+  int32_t cnt = 0;
+  check(mg_graph_trace(g, rec.data(), MG_TRACE_LEVELS, &cnt), "mg_graph_trace");
+  for (int32_t i = 0; i < cnt; i++)
+    std::printf("iteration %d: frontier %lld, frontier edges %lld, %s%s%.3g\n", rec[i].level,
+                (long long)rec[i].frontier, (long long)rec[i].frontier_edges,
+                rec[i].direction == MG_DIR_PULL ? "pull" : "push", rec[i].value != 0.0 ? ", residual " : "",
+                rec[i].value != 0.0 ? rec[i].value : 0.0);
+}
+
 void check(mg_status st, const char *where) {
   if (st != MG_OK) {
     std::fprintf(stderr, "%s: %s: %s\n", where, mg_status_string(st), mg_last_error());

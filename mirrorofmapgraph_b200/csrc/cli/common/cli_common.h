@@ -64,4 +64,8 @@ mg_graph *upload(const mg_host_csr &g, bool with_values, mg_dtype vt);
 // Exits with the engine's message when st != MG_OK.
 void check(mg_status st, const char *where);
 
+// verbose=1: the last run's per-level records (the reference prints the frontier
+// size of every iteration, GASengine/enactor_vertex_centric.cuh:2528-2546).
+void print_trace(const Config &cfg, mg_graph *g);
+
 }  // namespace mgcli

@@ -30,6 +30,7 @@ int main(int argc, char **argv) {
   std::vector<float> rank(h.n);
   mg_stats st;
   mgcli::check(mg_pagerank(g, nullptr, 1, rank.data(), &o, &st), "mg_pagerank");
+  mgcli::print_trace(cfg, g);
   std::printf("Kernel time took: %.4f ms\n", st.kernel_ms);
   std::printf("Total iteration: %lld\n", (long long)st.iterations);
   if (!args.output.empty()) {

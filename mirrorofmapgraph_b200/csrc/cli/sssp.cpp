@@ -27,6 +27,7 @@ int main(int argc, char **argv) {
     }
     mg_stats st;
     mgcli::check(mg_sssp(g, &s, 1, dist.data(), &o, &st), "mg_sssp");
+    mgcli::print_trace(cfg, g);
     std::printf("Kernel time took: %.4f ms\n", st.kernel_ms);
     std::printf("Total iteration: %lld\n", (long long)st.iterations);
     std::printf("Traversed edge: %lld\n", (long long)st.edges_traversed);

@@ -53,6 +53,24 @@ cudaError_t mg_malloc_async(void **p, size_t bytes, cudaStream_t s) {
 int32_t debug_barrier_extra() { return g_bar_extra.load(); }
 unsigned long long debug_barrier_limit() { return g_bar_limit.load(); }
 
+extern "C" mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count) {
+  if (!g || !count || (cap > 0 && !out)) {
+    mg_set_error("mg_graph_trace: null argument");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  int32_t len = 0;
+  MG_CUDA_TRY(cudaMemcpyAsync(&len, &g->ctl->trace_len, sizeof(int32_t), cudaMemcpyDeviceToHost, g->stream));
+  MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  len = std::max(0, std::min(std::min(len, (int32_t)MG_TRACE_LEVELS), std::max(cap, 0)));
+  if (len > 0)
+    MG_CUDA_TRY(cudaMemcpyAsync(out, trace_of(g->ctl), sizeof(mg_level_record) * (size_t)len, cudaMemcpyDeviceToHost,
+                                g->stream));
+  MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  *count = len;
+  return MG_OK;
+}
+
 extern "C" mg_status mg_debug_fail_alloc(int64_t k) {
   if (k < 0) {
     mg_set_error("mg_debug_fail_alloc: k must be >= 0");
@@ -653,7 +671,8 @@ static mg_status create_impl(const int32_t *row_offsets, const int32_t *col_idx,
   CREATE_TRY(cudaMemcpyAsync(g->ro, row_offsets, sizeof(int32_t) * (n + 1), kind, s));
   if (m > 0) CREATE_TRY(cudaMemcpyAsync(g->ci, col_idx, sizeof(int32_t) * m, kind, s));
   if (vb && m > 0) CREATE_TRY(cudaMemcpyAsync(g->vals, edge_vals, vb * m, kind, s));
-  if (dev_alloc(g, (void **)&g->ctl, sizeof(DevCtl) + 64) != MG_OK) return fail(MG_ERR_OOM);
+  if (dev_alloc(g, (void **)&g->ctl, MG_TRACE_OFF + sizeof(mg_level_record) * MG_TRACE_LEVELS) != MG_OK)
+    return fail(MG_ERR_OOM);
   g->ctl_host = pinned_ctl_get();
   if (!g->ctl_host) {
     mg_set_error("mg_graph_create: pinned host allocation failed");

@@ -70,6 +70,7 @@ struct DevCtl {
   int32_t pq[3];
   int32_t pb[3];  // deferred big vertices per level (persistent BFS)
   int32_t tile_next;  // next frontier tile of the dynamic schedule (SSSP rounds; reset at level end)
+  int32_t trace_len;  // per-level trace records written by this run (mg_graph_trace)
   uint32_t bar_count;
   uint32_t bar_gen;
 };
@@ -134,6 +135,25 @@ unsigned long long debug_barrier_limit();
 // device-wide synchronisation.
 mg_status dev_alloc(mg_graph *g, void **p, size_t bytes);
 void dev_free(mg_graph *g, void *p);
+
+// Per-level trace records live in the control block's allocation, behind the
+// DevCtl and its 64 spare bytes, so kernels reach them from the DevCtl pointer.
+constexpr size_t MG_TRACE_OFF = (sizeof(DevCtl) + 64 + 15) & ~(size_t)15;
+__host__ __device__ inline mg_level_record *trace_of(DevCtl *c) {
+  return reinterpret_cast<mg_level_record *>(reinterpret_cast<char *>(c) + MG_TRACE_OFF);
+}
+__device__ inline void trace_level(DevCtl *c, int32_t level, int32_t dir, int64_t frontier, int64_t edges,
+                                   double value) {
+  if (level < 0 || level >= MG_TRACE_LEVELS) return;
+  mg_level_record r;
+  r.level = level;
+  r.direction = dir;
+  r.frontier = frontier;
+  r.frontier_edges = edges;
+  r.value = value;
+  trace_of(c)[level] = r;
+  if (level + 1 > c->trace_len) c->trace_len = level + 1;
+}
 
 // Grows a workspace to at least `bytes` (contents are not preserved).
 mg_status ws_reserve(mg_graph *g, Workspace &w, size_t bytes);

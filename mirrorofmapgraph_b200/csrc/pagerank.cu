@@ -381,6 +381,7 @@ __device__ void solve_iteration_end(const SolveArgs &a, int cur, const double *h
   d = block_sum<NT>(d, s_red);
   if (threadIdx.x == 0) {
     const int lvl = c->level + 1;
+    trace_level(c, lvl - 1, MG_DIR_PUSH, a.n, 0, r);
     c->level = lvl;
     c->dsum[0] = r;
     c->dprev[1] = d;

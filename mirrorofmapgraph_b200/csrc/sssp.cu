@@ -101,6 +101,7 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   const int cur = vload(&c->cur);
   const int32_t nf = vload(&c->qlen[cur ^ 1]);
   const int lvl = vload(&c->level) + 1;
+  trace_level(c, lvl - 1, MG_DIR_PUSH, vload(&c->qlen[cur]), vload(&c->mf_next), 0.0);
   c->visited_deg = vload(&c->visited_deg) + vload(&c->mf_next);
   c->mf_next = 0;
   c->level = lvl;

@@ -173,6 +173,18 @@ class Graph:
         names = ["row_offsets", "col_idx", "edge_vals", "col_offsets", "row_idx", "csc_perm"]
         return {k: p.value for k, p in zip(names, ptrs)}
 
+    def trace(self) -> list[dict]:
+        """Per-level records of the last mg_bfs / mg_sssp / single-vector normalised
+        PageRank run on this graph (the reference's verbose per-iteration print):
+        level, direction, frontier size, frontier out-edges, value (PageRank: the
+        iteration's L1 change)."""
+        recs = (L.MgLevelRecord * L.MG_TRACE_LEVELS)()
+        cnt = C.c_int32()
+        _check(self._lib.mg_graph_trace(self._h, recs, L.MG_TRACE_LEVELS, C.byref(cnt)), "mg_graph_trace")
+        names = {L.MG_DIR_PUSH: "push", L.MG_DIR_PULL: "pull"}
+        return [{"level": r.level, "direction": names.get(r.direction, "push"), "frontier": r.frontier,
+                 "frontier_edges": r.frontier_edges, "value": r.value} for r in recs[: cnt.value]]
+
     # -- helpers ----------------------------------------------------------------
     def _out(self, out, count, dtype):
         if out is None:

@@ -91,6 +91,13 @@ def test_drivers_match_reference_cpu_results(bins, mtx_fixtures, tmp_path, name)
         r = _run(bins["bfs"], "-g", g, "-o", out, "-p", "directed=0")
         assert r.returncode == 0, r.stderr
         assert _read(out, np.int64).tolist() == d["cpubfs_undirected"]
+    # verbose=1 prints one line per level; the frontier sizes are the depth histogram
+    r = _run(bins["bfs"], "-g", g, "-p", "verbose=1")
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("iteration ")]
+    depth = np.array(d["cpubfs_directed"])
+    assert [int(ln.split("frontier ")[1].split(",")[0]) for ln in lines] == \
+        np.bincount(depth[depth >= 0]).tolist()
 
 
 @pytest.mark.gpu
