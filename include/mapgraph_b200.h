@@ -111,8 +111,11 @@ typedef struct mg_pr_opts {
   int32_t autotune;      /* NORMALIZED forward with gather_kernel 0: 1 makes the first such solve on a graph
                             time the degree-binned kernel without and with column caches of 8K, 16K, 20K and
                             the most that fits (4 iterations each) and keep the fastest for every later solve;
-                            stats->status_detail reports the choice (cache columns, 0 for none) [0] */
-  int32_t reserved[1];
+                            stats->status_detail reports the choice (cache columns, 0 for none);
+                            with nvec > 1 and group_width 0 it picks the group width instead (64, 128
+                            or 256 vectors per pass, timed over 4 iterations each) [0] */
+  int32_t group_width;   /* nvec > 1: vectors iterated together per pass, a multiple of 32 up to 256
+                            [0: 256, or the autotuned width]; stats->status_detail reports it */
 } mg_pr_opts;
 
 /* ---- status ------------------------------------------------------------- */

@@ -48,7 +48,7 @@ class MgPrOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("directed", C.c_int32), ("max_iter", C.c_int32), ("weighted", C.c_int32),
                 ("alpha", C.c_double), ("tol", C.c_double), ("compensated", C.c_int32),
                 ("device_output", C.c_int32), ("use_graph", C.c_int32), ("gather_kernel", C.c_int32),
-                ("autotune", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("autotune", C.c_int32), ("group_width", C.c_int32)]
 
 
 class MgPartLevel(C.Structure):

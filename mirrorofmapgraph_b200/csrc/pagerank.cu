@@ -59,6 +59,7 @@ struct PlanSet {
   bool bcsc_ok = false, bcsr_ok = false;
   HubCache hubs;
   int32_t tuned_cap = -1;  // autotuned column-cache capacity (-1 not tuned, 0 no cache)
+  int32_t tuned_ppr_w = -1;  // autotuned personalised-PageRank group width (-1 not tuned)
 };
 
 }  // namespace mg
@@ -1328,7 +1329,37 @@ static void ppr_launch_init(const mg::PprArgs &a, int grid, cudaStream_t st) {
 }
 
 static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, float *ranks_out, int out_is_device,
-                              const mg_pr_opts &o, mg_stats *stats) {
+                              const mg_pr_opts &o, mg_stats *stats, int32_t gw);
+
+// Group-width autotuner of the batched personalised PageRank (mg_pr_opts.autotune
+// with nvec > 1): runs the first vectors at 64, 128 and 256 vectors per pass for
+// four iterations each (second of two runs, so the executable graph is cached)
+// and keeps the width with the most vector-iterations per second for the graph.
+static mg_status ppr_autotune(mg_graph *g, const float *tele_dev, int32_t nvec, float *ranks, const mg_pr_opts &o) {
+  using namespace mg;
+  mg_pr_opts t = o;
+  t.max_iter = 4;
+  t.tol = 1e-300;  // run all four iterations
+  double best = -1.0;
+  int32_t best_w = PPR_MAXW;
+  const int32_t cap = std::min<int32_t>(((nvec + 31) / 32) * 32, PPR_MAXW);
+  for (int32_t w : {64, 128, 256}) {
+    if (w > cap) continue;
+    const int32_t nv = std::min(nvec, w);
+    mg_stats st;
+    for (int rep = 0; rep < 2; rep++) MG_TRY(pagerank_ppr(g, tele_dev, nv, ranks, o.device_output, t, &st, w));
+    const double rate = st.kernel_ms > 0 ? (double)nv * (double)st.iterations / st.kernel_ms : 0.0;
+    if (rate > best) {
+      best = rate;
+      best_w = w;
+    }
+  }
+  plans_of(g)->tuned_ppr_w = best_w;
+  return MG_OK;
+}
+
+static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, float *ranks_out, int out_is_device,
+                              const mg_pr_opts &o, mg_stats *stats, int32_t gw) {
   using namespace mg;
   const bool weighted = o.weighted != 0;
   if (!g->has_csc) {
@@ -1343,7 +1374,7 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
   MG_TRY(get_bin_plan(g, false, &bins));
   if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
-  const int32_t kmax = std::min<int32_t>(nvec, PPR_MAXW);
+  const int32_t kmax = std::min<int32_t>(nvec, gw);
   const int vpl = kmax > 128 ? 8 : kmax > 64 ? 4 : kmax > 32 ? 2 : 1;
   const int32_t W = 32 * vpl;
   int occ = 1;
@@ -1416,8 +1447,8 @@ static mg_status pagerank_ppr(mg_graph *g, const float *tele_dev, int32_t nvec, 
   mg_stats total;
   std::memset(&total, 0, sizeof(total));
   const dim3 tblk(32, 8), tgrid((unsigned)((n + 31) / 32), (unsigned)(W / 32));
-  for (int32_t c0 = 0; c0 < nvec; c0 += PPR_MAXW) {
-    const int32_t k = std::min<int32_t>(PPR_MAXW, nvec - c0);
+  for (int32_t c0 = 0; c0 < nvec; c0 += kmax) {
+    const int32_t k = std::min<int32_t>(kmax, nvec - c0);
     MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
     ppr_pack_kernel<<<tgrid, tblk, 0, s>>>(tele_dev ? tele_dev + (size_t)c0 * n : nullptr, k, n, W, tele);
     MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
@@ -1522,7 +1553,21 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
       MG_CUDA_TRY(cudaMemcpyAsync(tele_dev, teleport, sizeof(float) * n * nvec, cudaMemcpyHostToDevice, g->stream));
     }
   }
-  if (nvec > 1) return pagerank_ppr(g, tele_dev, nvec, ranks, o.device_output, o, stats);
+  if (nvec > 1) {
+    int32_t gw = o.group_width > 0 ? o.group_width : mg::PPR_MAXW;
+    if (gw % 32 != 0 || gw > mg::PPR_MAXW) {
+      mg_set_error("mg_pagerank: group_width must be a multiple of 32 up to %d", mg::PPR_MAXW);
+      return MG_ERR_ARG;
+    }
+    if (o.group_width <= 0 && o.autotune) {
+      mg::PlanSet *ps = plans_of(g);
+      if (ps->tuned_ppr_w < 0) MG_TRY(ppr_autotune(g, tele_dev, nvec, ranks, o));
+      gw = ps->tuned_ppr_w;
+    }
+    MG_TRY(pagerank_ppr(g, tele_dev, nvec, ranks, o.device_output, o, stats, gw));
+    if (stats) stats->status_detail = gw;
+    return MG_OK;
+  }
   mg_stats total;
   std::memset(&total, 0, sizeof(total));
   for (int32_t k = 0; k < nvec; k++) {

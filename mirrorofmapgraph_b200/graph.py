@@ -270,9 +270,10 @@ class Graph:
     @staticmethod
     def _pr_opts(mode="refcompat", directed=1, max_iter=0, weighted=False, alpha=0.85, tol=None,
                  compensated=True, device_output=False, use_graph=True, gather="binned",
-                 autotune=False) -> L.MgPrOpts:
+                 autotune=False, group_width=0) -> L.MgPrOpts:
         o = L.MgPrOpts()
         o.autotune = 1 if autotune else 0
+        o.group_width = int(group_width)
         o.gather_kernel = {"binned": 0, "tma": 1, "cached": 2}[gather]
         o.mode = {"refcompat": L.MG_PR_REFCOMPAT, "normalized": L.MG_PR_NORMALIZED}[mode]
         o.directed = int(directed)

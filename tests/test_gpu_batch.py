@@ -184,3 +184,19 @@ def test_ppr_batch_widths_and_groups(nvec):
         xs, st = g.pagerank(teleport=tele, nvec=nvec, mode="normalized", tol=1e-30, max_iter=25)
         assert st["iterations"] == 25
         _check_vectors(h, xs, tele, 25, sorted({0, nvec // 2, nvec - 1}))
+
+
+@pytest.mark.parametrize("width", [32, 64, 128])
+def test_ppr_group_width_and_autotuned_width(width):
+    # Fixed 25 iterations: every group runs the same schedule whatever its width.
+    h = mg.gen_rmat(12, 8, 7, symmetrize=True)
+    tele = _sparse_teleports(h.n, 150, 11)
+    with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+        xs, st = g.pagerank(teleport=tele, nvec=150, mode="normalized", tol=1e-30, max_iter=25, group_width=width)
+        assert st["status_detail"] == width and st["iterations"] == 25
+        _check_vectors(h, xs, tele, 25, [0, width - 1, width, 149])
+        xa, sa = g.pagerank(teleport=tele, nvec=150, mode="normalized", tol=1e-30, max_iter=25, autotune=True)
+        assert sa["status_detail"] in (64, 128, 256)
+        assert np.abs(xa - xs).sum() <= 1e-9 * 150
+        with pytest.raises(mg.MapGraphError):
+            g.pagerank(teleport=tele, nvec=150, mode="normalized", group_width=48)
