@@ -52,7 +52,8 @@ typedef enum mg_dtype {
 #define MG_GRAPH_DEVICE_INPUT 0x4u /* input arrays are device pointers on the current device */
 
 /* BFS direction policy (mg_opts.direction) */
-#define MG_DIR_AUTO 0 /* push/pull switch chosen on the device each level */
+#define MG_DIR_AUTO 0 /* push/pull switch chosen on the device each level (Beamer's rule); graphs of mean
+                         out-degree <= 8 run top-down only */
 #define MG_DIR_PUSH 1 /* top-down only (the reference engine's only mode) */
 #define MG_DIR_PULL 2 /* bottom-up wherever possible (after the first level) */
 
@@ -331,7 +332,8 @@ mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_
  *             direction = MG_DIR_PUSH / MG_DIR_PULL;
  *   SSSP:     frontier = vertices relaxed, frontier_edges = out-edges of the
  *             vertices this round improved;
- *   PageRank: frontier = n, value = the iteration's L1 change.
+ *   PageRank: frontier = n, value = the iteration's L1 change;
+ *   every record: time_ns, the device clock at the level's end.
  * *count = records written (min(levels, cap, MG_TRACE_LEVELS)). */
 #define MG_TRACE_LEVELS 4096
 typedef struct mg_level_record {
@@ -340,6 +342,8 @@ typedef struct mg_level_record {
   int64_t frontier;
   int64_t frontier_edges;
   double value;
+  uint64_t time_ns; /* device clock (PTX %globaltimer) when the level ended: differences give per-level
+                       durations */
 } mg_level_record;
 mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count);
 

@@ -59,7 +59,7 @@ class MgPartLevel(C.Structure):
 
 class MgLevelRecord(C.Structure):
     _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_int64),
-                ("frontier_edges", C.c_int64), ("value", C.c_double)]
+                ("frontier_edges", C.c_int64), ("value", C.c_double), ("time_ns", C.c_uint64)]
 
 
 MG_TRACE_LEVELS = 4096

@@ -151,6 +151,9 @@ __device__ inline void trace_level(DevCtl *c, int32_t level, int32_t dir, int64_
   r.frontier = frontier;
   r.frontier_edges = edges;
   r.value = value;
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  r.time_ns = t;
   trace_of(c)[level] = r;
   if (level + 1 > c->trace_len) c->trace_len = level + 1;
 }

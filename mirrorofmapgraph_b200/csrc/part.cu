@@ -657,7 +657,8 @@ extern "C" mg_status mg_part_bfs_begin(mg_part *p, const int32_t *srcs, int32_t 
   MG_CUDA_TRY(cudaGetLastError());
   MG_CUDA_TRY(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(PartCtl), cudaMemcpyDeviceToHost, s));
   MG_CUDA_TRY(cudaStreamSynchronize(s));
-  p->mode = o.direction;
+  // AUTO on sparse graphs stays top-down, as in mg_bfs (mean out-degree <= 8)
+  p->mode = (o.direction == MG_DIR_AUTO && p->m_total <= 8 * p->n) ? MG_DIR_PUSH : o.direction;
   p->iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, p->n + 1) : (int32_t)(p->n + 1);
   p->level = 0;
   p->dir = 0;

@@ -182,8 +182,13 @@ class Graph:
         cnt = C.c_int32()
         _check(self._lib.mg_graph_trace(self._h, recs, L.MG_TRACE_LEVELS, C.byref(cnt)), "mg_graph_trace")
         names = {L.MG_DIR_PUSH: "push", L.MG_DIR_PULL: "pull"}
-        return [{"level": r.level, "direction": names.get(r.direction, "push"), "frontier": r.frontier,
-                 "frontier_edges": r.frontier_edges, "value": r.value} for r in recs[: cnt.value]]
+        out = [{"level": r.level, "direction": names.get(r.direction, "push"), "frontier": r.frontier,
+                "frontier_edges": r.frontier_edges, "value": r.value, "time_ns": r.time_ns}
+               for r in recs[: cnt.value]]
+        # duration of each level: from the previous level's end (the first has none)
+        for a, b in zip(out, out[1:]):
+            b["ns"] = b["time_ns"] - a["time_ns"]
+        return out
 
     # -- helpers ----------------------------------------------------------------
     def _out(self, out, count, dtype):

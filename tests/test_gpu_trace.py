@@ -26,6 +26,7 @@ def test_bfs_trace_matches_levels(kind):
             assert [r["frontier_edges"] for r in tr] == edges
             assert sum(r["direction"] == "pull" for r in tr) == st["status_detail"]
             assert [r["level"] for r in tr] == list(range(len(tr)))
+            assert all(r["ns"] >= 0 for r in tr[1:])  # level ends in order on the device clock
 
 
 def test_sssp_and_pagerank_traces():
