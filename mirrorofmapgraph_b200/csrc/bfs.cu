@@ -129,6 +129,7 @@ struct PushCtx {
   int32_t qcap;
   int32_t level;
   int64_t mf;
+  BlockQueue *bq = nullptr;  // staging of discoveries (nullptr: straight to the queue)
 };
 
 __device__ __forceinline__ void bfs_visit(PushCtx &x, int32_t u) {
@@ -143,11 +144,12 @@ __device__ __forceinline__ void bfs_visit(PushCtx &x, int32_t u) {
     x.label[u] = x.level + 1;
     x.mf += x.ro[u + 1] - x.ro[u];
   }
-  warp_append(disc, u, x.qout, x.qlen_out, x.qcap, x.overflow);
+  staged_append(x.bq, disc, u, x.qout, x.qlen_out, x.qcap, x.overflow);
 }
 
 __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
   __shared__ ExpandSmem<BFS_NT> sm;
+  __shared__ BlockQueue bq;
   __shared__ int64_t s_sum[BFS_NT / 32 + 1];
   if (bfs_skip(a, 0)) return;
   DevCtl *c = a.ctl;
@@ -155,6 +157,8 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
   const int32_t nin = vload(&c->qlen[cur]);
   const int32_t *qin = cur ? a.q1 : a.q0;
   PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
+  bq_init(bq);
+  x.bq = &bq;
   int64_t insp = 0, nexp = 0;
   const BigList big{a.big_v, &c->big_len, defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
   for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
@@ -166,6 +170,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
     if (a.both)
       expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
   }
+  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
   const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
   const int64_t bins = block_sum<BFS_NT>(insp, s_sum);
   const int64_t bexp = block_sum<BFS_NT>(nexp, s_sum);
@@ -201,6 +206,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
     ExpandSmem<BFS_NT> e;
     BigSmem<BFS_NT> b;
   } sm;
+  __shared__ BlockQueue bq;
   __shared__ int64_t s_sum[BFS_NT / 32 + 1];
   DevCtl *c = a.ctl;
   // Entry state, as the seed kernel or the last per-level kernel left it; every
@@ -211,6 +217,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
   int64_t mf = vload(&c->mf_front), vdeg = vload(&c->visited_deg);
   const int32_t iter_cap = vload(&c->iter_cap);
   if (vload(&c->done) || vload(&c->dir) != 0 || nin > PERSIST_MAX || mf > PERSIST_EDGES) return;
+  bq_init(bq);
   for (;;) {
     // Per-level counters rotate over three slots: this level appends to `out`;
     // `zero` is the slot the next level appends to (nobody touches it now).
@@ -222,6 +229,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
     }
     const int32_t *qin = sel ? a.q1 : a.q0;
     PushCtx x{a.label, a.vis, a.ro, sel ? a.q0 : a.q1, &c->pq[out], &c->overflow, a.qcap, lvl, 0};
+    x.bq = &bq;
     const BigList big{a.big_v, &c->pb[out], defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
     const int32_t *ci = a.ci, *ri = a.ri;
     int64_t insp = 0, nexp = 0;
@@ -233,6 +241,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
       if (a.both)
         expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
     }
+    bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
     const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
     const int64_t bins = block_sum<BFS_NT>(insp, s_sum);
     const int64_t bexp = block_sum<BFS_NT>(nexp, s_sum);
@@ -252,6 +261,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
       // The deferred vertices' edges, spread over the whole grid.
       x.mf = 0;
       expand_big<BFS_NT>(sm.b, a.ro, big, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+      bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
       const int64_t bmf2 = block_sum<BFS_NT>(x.mf, s_sum);
       if (threadIdx.x == 0 && bmf2) atomicAdd((unsigned long long *)&c->pm[out], (unsigned long long)bmf2);
       if (!grid_barrier(&c->bar_count, &c->bar_gen, a.bar_limit, a.bar_extra)) {
@@ -303,13 +313,17 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
 // CTA; the last CTA closes the level.
 __global__ void __launch_bounds__(BFS_NT) bfs_push_big_kernel(BfsArgs a) {
   __shared__ BigSmem<BFS_NT> sm;
+  __shared__ BlockQueue bq;
   __shared__ int64_t s_sum[BFS_NT / 32 + 1];
   if (bfs_skip(a, 0)) return;
   DevCtl *c = a.ctl;
   const int cur = vload(&c->cur);
   PushCtx x{a.label, a.vis, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap, vload(&c->level), 0};
+  bq_init(bq);
+  x.bq = &bq;
   const int32_t *ci = a.ci;
   expand_big<BFS_NT>(sm, a.ro, BigList{a.big_v, &c->big_len}, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); });
+  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
   const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
   if (threadIdx.x == 0 && bmf) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)bmf);
   if (last_block(&c->blocks_done) && threadIdx.x == 0) bfs_level_end(a);

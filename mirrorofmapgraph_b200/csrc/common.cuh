@@ -143,6 +143,55 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t *qu
   }
 }
 
+// Block-local staging of the vertices a level adds to a frontier queue: threads
+// take slots with a shared-memory atomic and the block appends its whole batch to
+// the queue with one global atomic when it flushes. With one global atomic per
+// warp instead, a level that adds ~10^6 vertices serialises on the queue's length
+// word (R-MAT s22 BFS: a 6.1 M-edge push level took 510 us).
+constexpr int BQ_CAP = 2048;
+struct BlockQueue {
+  int32_t n;
+  int32_t base;
+  int32_t v[BQ_CAP];
+};
+
+__device__ __forceinline__ void bq_init(BlockQueue &bq) {
+  if (threadIdx.x == 0) bq.n = 0;
+  __syncthreads();
+}
+
+// Every thread of the block calls it (it synchronises the block).
+__device__ __forceinline__ void bq_flush(BlockQueue &bq, int32_t *qout, int32_t *qlen, int32_t cap,
+                                         int32_t *overflow) {
+  __syncthreads();
+  const int32_t n = min(bq.n, BQ_CAP);
+  if (threadIdx.x == 0) bq.base = n ? atomicAdd(qlen, n) : 0;
+  __syncthreads();
+  for (int32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int32_t pos = bq.base + i;
+    if (pos < cap) qout[pos] = bq.v[i];
+    else *overflow = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) bq.n = 0;
+  __syncthreads();
+}
+
+// Appends item (where pred) through the staging area, or straight to the queue
+// when there is none or it is full.
+__device__ __forceinline__ void staged_append(BlockQueue *bq, bool pred, int32_t item, int32_t *queue, int32_t *len,
+                                              int32_t cap, int32_t *overflow) {
+  bool spill = pred;
+  if (pred && bq) {
+    const int32_t pos = atomicAdd(&bq->n, 1);
+    if (pos < BQ_CAP) {
+      bq->v[pos] = item;
+      spill = false;
+    }
+  }
+  warp_append(spill, item, queue, len, cap, overflow);
+}
+
 __device__ __forceinline__ int32_t ld_nc(const int32_t *p) { return __ldg(p); }
 
 }  // namespace mg

@@ -27,6 +27,9 @@ namespace mg {
 
 constexpr int SSSP_NT = 256;
 constexpr int SSSP_CTA_TH = 512;
+#ifndef MG_SSSP_STAGE
+#define MG_SSSP_STAGE 1
+#endif
 #ifndef MG_SSSP_DYNAMIC
 #define MG_SSSP_DYNAMIC 1
 #endif
@@ -65,6 +68,7 @@ struct RelaxCtx {
   int64_t thr;
   uint32_t *infar;
   int32_t *far_out, *far_len_out;
+  BlockQueue *bq = nullptr;  // staging of the next frontier (nullptr: straight to the queue)
 };
 
 // Relaxes edge (v, u) of weight w, dv = dist[v] as read when v was expanded.
@@ -82,7 +86,7 @@ __device__ __forceinline__ void relax_d(RelaxCtx &x, int32_t dv, int32_t u, int3
       else far = !(atomicOr(x.infar + (u >> 5), bit) & bit);
     }
   }
-  warp_append(push, u, x.qout, x.qlen_out, x.qcap, x.overflow);
+  staged_append(x.bq, push, u, x.qout, x.qlen_out, x.qcap, x.overflow);
   if (x.delta > 0) warp_append(far, u, x.far_out, x.far_len_out, x.qcap, x.overflow);
 }
 
@@ -125,6 +129,7 @@ __device__ void sssp_level_end(const SsspArgs &a) {
 
 __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   __shared__ ExpandSmem<SSSP_NT> sm;
+  __shared__ BlockQueue bq;
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
   if (vload(&c->done)) {
@@ -136,6 +141,8 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   const int32_t *qin = cur ? a.q1 : a.q0;
   uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
   RelaxCtx x = relax_ctx(a, c, cur);
+  bq_init(bq);
+  if (MG_SSSP_STAGE) x.bq = &bq;
   const int32_t hi = ~a.vmask;  // instance bits of an item
   int64_t insp = 0, nexp = 0;
   const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
@@ -170,6 +177,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
         relax_d(x, d, (sv & hi) | ri[k], cw ? cw[k] : 1);
       }, nullptr, a.vmask);
   }
+  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
   const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
   const int64_t b1 = block_sum<SSSP_NT>(insp, s_sum);
   const int64_t b2 = block_sum<SSSP_NT>(nexp, s_sum);
@@ -185,6 +193,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
 // Grid-strided bin of a relaxation round; the last CTA closes the round.
 __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
   __shared__ BigSmem<SSSP_NT> sm;
+  __shared__ BlockQueue bq;
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
   if (vload(&c->done)) {
@@ -193,10 +202,13 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
   }
   const int cur = vload(&c->cur);
   RelaxCtx x = relax_ctx(a, c, cur);
+  bq_init(bq);
+  if (MG_SSSP_STAGE) x.bq = &bq;
   const int32_t hi = ~a.vmask;  // instance bits of an item
   const int32_t *ci = a.ci, *w = a.w;
   expand_big<SSSP_NT>(sm, a.ro, BigList{a.big_v, &c->big_len},
                       [&](int32_t sv, int32_t k) { relax(x, sv, (sv & hi) | ci[k], w ? w[k] : 1); }, a.vmask);
+  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
   const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
   const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
   if (threadIdx.x == 0) {
