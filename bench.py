@@ -90,8 +90,10 @@ class Clocks:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv") \
-            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/mg_clocks_{os.getpid()}.csv"
+        # raw samples: $MG_CLOCK_LOG (a directory) if set, else a temporary file
+        log_dir = os.environ.get("MG_CLOCK_LOG")
+        self.path = os.path.join(log_dir, f"clocks_rank{device_index}.csv") if log_dir and os.path.isdir(log_dir) \
+            else f"/tmp/mg_clocks_{os.getpid()}_{device_index}.csv"
 
     def start(self):
         try:

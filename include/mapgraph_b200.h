@@ -110,8 +110,9 @@ typedef struct mg_pr_opts {
                             staged in shared memory by TMA bulk copies; 2 degree-binned with the most-gathered
                             columns cached in shared memory (forward solve; the adjoint uses 0) */
   int32_t autotune;      /* NORMALIZED forward with gather_kernel 0: 1 makes the first such solve on a graph
-                            time the degree-binned kernel without and with column caches of 8K, 16K, 20K and
-                            the most that fits (4 iterations each) and keep the fastest for every later solve;
+                            time the degree-binned kernel without and with column caches of 20K, 32K and 40K
+                            columns (as many as fit; 4 iterations each) and keep the fastest for every later
+                            solve;
                             stats->status_detail reports the choice (cache columns, 0 for none);
                             with nvec > 1 and group_width 0 it picks the group width instead (64, 128
                             or 256 vectors per pass, timed over 4 iterations each) [0] */

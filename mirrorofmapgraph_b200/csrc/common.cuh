@@ -178,16 +178,26 @@ __device__ __forceinline__ void bq_flush(BlockQueue &bq, int32_t *qout, int32_t 
 }
 
 // Appends item (where pred) through the staging area, or straight to the queue
-// when there is none or it is full.
+// when there is none or it is full. One shared-memory atomic per warp, like
+// warp_append's one global atomic per warp.
 __device__ __forceinline__ void staged_append(BlockQueue *bq, bool pred, int32_t item, int32_t *queue, int32_t *len,
                                               int32_t cap, int32_t *overflow) {
-  bool spill = pred;
-  if (pred && bq) {
-    const int32_t pos = atomicAdd(&bq->n, 1);
-    if (pos < BQ_CAP) {
-      bq->v[pos] = item;
-      spill = false;
-    }
+  if (!bq) {
+    warp_append(pred, item, queue, len, cap, overflow);
+    return;
+  }
+  const unsigned active = __activemask();
+  const unsigned pm = __ballot_sync(active, pred);
+  if (pm == 0) return;
+  const int leader = __ffs(active) - 1;
+  int32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(&bq->n, __popc(pm));
+  base = __shfl_sync(active, base, leader);
+  bool spill = false;
+  if (pred) {
+    const int32_t pos = base + __popc(pm & lanemask_lt());
+    if (pos < BQ_CAP) bq->v[pos] = item;
+    else spill = true;
   }
   warp_append(spill, item, queue, len, cap, overflow);
 }

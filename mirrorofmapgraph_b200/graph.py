@@ -292,7 +292,14 @@ class Graph:
         return o
 
     def pagerank(self, teleport=None, nvec: int = 1, out=None, **kw):
-        """struct pagerank (refcompat) or the normalised / personalised power iteration."""
+        """struct pagerank (refcompat) or the normalised / personalised power iteration.
+
+        Keywords (mg_pr_opts): mode "refcompat" | "normalized", alpha, tol, max_iter,
+        weighted, directed (refcompat), gather "binned" | "cached" | "tma",
+        autotune (time the gathers, or with nvec > 1 the group width, once per
+        graph), group_width (nvec > 1: vectors per pass, a multiple of 32 <= 256),
+        compensated, use_graph. Returns (ranks, stats); with nvec > 1 the ranks are
+        nvec x n and stats["status_detail"] is the group width used."""
         t_p, t_dev, keep = _ptr(teleport, np.float32) if teleport is not None else (None, False, None)
         res, rp, dev = self._out(out, nvec * self.n, np.float32)
         st = L.MgStats()
