@@ -61,6 +61,8 @@ def test_null_arguments_are_rejected():
     assert lib.mg_part_bfs_step(None, None) == L.MG_ERR_ARG
     assert lib.mg_part_pr_merge(None, None, 1, 1, None, None) == L.MG_ERR_ARG
     assert lib.mg_part_destroy(None) == L.MG_OK
+    cnt = C.c_int32()
+    assert lib.mg_graph_trace(None, None, 0, C.byref(cnt)) == L.MG_ERR_ARG
     # fault-injection hooks: argument checks (arming them needs no device)
     assert lib.mg_debug_fail_alloc(-1) == L.MG_ERR_ARG
     assert lib.mg_debug_barrier_skew(-1, 10) == L.MG_ERR_ARG
