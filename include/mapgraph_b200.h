@@ -50,6 +50,12 @@ typedef enum mg_dtype {
 #define MG_GRAPH_SYMMETRIC 0x1u    /* caller asserts the CSR equals its transpose; the CSC aliases it */
 #define MG_GRAPH_NO_CSC 0x2u       /* skip the transpose (then directed == 0, pull BFS and PageRank are refused) */
 #define MG_GRAPH_DEVICE_INPUT 0x4u /* input arrays are device pointers on the current device */
+#define MG_GRAPH_ASYNC_UPLOAD 0x8u /* with MG_GRAPH_SYMMETRIC or MG_GRAPH_NO_CSC: mg_graph_create returns once
+                                      the upload and the validation are enqueued on the graph's stream, so the
+                                      copy overlaps work on other graphs; the input arrays must stay valid and
+                                      unchanged until mg_graph_sync or the first call on the graph returns,
+                                      and an invalid CSR is reported there (MG_ERR_ARG). Other graphs upload
+                                      synchronously whatever the flag. */
 
 /* BFS direction policy (mg_opts.direction) */
 #define MG_DIR_AUTO 0 /* push/pull switch chosen on the device each level (Beamer's rule); graphs of mean
@@ -139,6 +145,8 @@ mg_status mg_graph_create(const int32_t *row_offsets, const int32_t *col_idx, co
 
 /* Replaces ~CsrProblem / ~GraphSlice (GASengine/csr_problem.cuh:217-309). NULL is a no-op. */
 mg_status mg_graph_destroy(mg_graph *g);
+/* Waits for an MG_GRAPH_ASYNC_UPLOAD upload and its validation (no-op otherwise). */
+mg_status mg_graph_sync(mg_graph *g);
 
 /* The CUDA stream (a cudaStream_t) every call on g is issued on, so a caller can
  * order its own work or CUDA events with the engine's. Owned by the graph. */

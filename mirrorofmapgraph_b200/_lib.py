@@ -21,7 +21,7 @@ MG_ERR_NO_DEVICE = 6
 MG_ERR_UNSUPPORTED = 7
 
 MG_DTYPE_NONE, MG_DTYPE_I32, MG_DTYPE_F32 = 0, 1, 2
-MG_GRAPH_SYMMETRIC, MG_GRAPH_NO_CSC, MG_GRAPH_DEVICE_INPUT = 0x1, 0x2, 0x4
+MG_GRAPH_SYMMETRIC, MG_GRAPH_NO_CSC, MG_GRAPH_DEVICE_INPUT, MG_GRAPH_ASYNC_UPLOAD = 0x1, 0x2, 0x4, 0x8
 MG_DIR_AUTO, MG_DIR_PUSH, MG_DIR_PULL = 0, 1, 2
 MG_PR_REFCOMPAT, MG_PR_NORMALIZED = 0, 1
 MG_W_NONE, MG_W_UNIFORM_INT, MG_W_LOGNORMAL = 0, 1, 2
@@ -82,6 +82,7 @@ SIGNATURES = {
     "mg_device_count": (C.c_int32, []),
     "mg_graph_create": (C.c_int, [_P, _P, _P, C.c_int, C.c_int64, C.c_int64, C.c_uint32, C.POINTER(_P)]),
     "mg_graph_destroy": (C.c_int, [_P]),
+    "mg_graph_sync": (C.c_int, [_P]),
     "mg_graph_info": (C.c_int, [_P, _I64P, _I64P, C.POINTER(C.c_uint32), _I32P]),
     "mg_graph_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "mg_graph_device_arrays": (C.c_int, [_P] + [C.POINTER(_P)] * 6),

@@ -53,6 +53,16 @@ cudaError_t mg_malloc_async(void **p, size_t bytes, cudaStream_t s) {
 int32_t debug_barrier_extra() { return g_bar_extra.load(); }
 unsigned long long debug_barrier_limit() { return g_bar_limit.load(); }
 
+extern "C" mg_status mg_graph_sync(mg_graph *g) {
+  if (!g) {
+    mg_set_error("mg_graph_sync: null graph");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return MG_OK;
+}
+
 extern "C" mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count) {
   if (!g || !count || (cap > 0 && !out)) {
     mg_set_error("mg_graph_trace: null argument");
@@ -136,6 +146,21 @@ mg_status ws_reserve(mg_graph *g, Workspace &w, size_t bytes) {
 
 mg_status graph_enter(mg_graph *g) {
   MG_CUDA_TRY(cudaSetDevice(g->device));
+  if (g->pending_validation) {
+    // an asynchronous upload: wait for it and read the validation flags before any
+    // kernel touches the arrays
+    int hbad = 0;
+    const int *bad = reinterpret_cast<const int *>(reinterpret_cast<const char *>(g->ctl) + sizeof(DevCtl));
+    MG_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+    MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    if (hbad) {
+      mg_set_error("mg_graph_create (asynchronous upload): %s",
+                   (hbad & 1) ? "row offsets are not a valid CSR (0..m, non-decreasing)"
+                              : "column index out of range [0, n)");
+      return MG_ERR_ARG;
+    }
+    g->pending_validation = false;
+  }
   return MG_OK;
 }
 
@@ -685,6 +710,20 @@ static mg_status create_impl(const int32_t *row_offsets, const int32_t *col_idx,
   CREATE_TRY(cudaMemsetAsync(bad, 0, sizeof(int) * 2, s));
   mg::validate_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ro, g->ci, n, m, bad);
   CREATE_TRY(cudaGetLastError());
+  if ((flags & MG_GRAPH_ASYNC_UPLOAD) && (flags & (MG_GRAPH_SYMMETRIC | MG_GRAPH_NO_CSC))) {
+    // no CSC to build from unvalidated arrays: return now, check on first use
+    g->pending_validation = true;
+    if (flags & MG_GRAPH_SYMMETRIC) {
+      g->co = g->ro;
+      g->ri = g->ci;
+      g->perm = nullptr;
+      g->cvals = g->vals;
+      g->has_csc = true;
+      g->csc_owned = false;
+    }
+    *out = g;
+    return MG_OK;
+  }
   int hbad[2] = {0, 0};
   CREATE_TRY(cudaMemcpyAsync(hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
   CREATE_TRY(cudaStreamSynchronize(s));

@@ -103,6 +103,7 @@ struct mg_graph {
   void *cvals = nullptr;
   bool has_csc = false, csc_owned = false;
   // cached checks of the edge values
+  bool pending_validation = false;  // MG_GRAPH_ASYNC_UPLOAD: checked before the first use
   bool weights_checked = false;
   int32_t min_weight = 0;
   double mean_weight = 0.0;

@@ -78,9 +78,14 @@ class Graph:
     """
 
     def __init__(self, row_offsets, col_idx, values=None, symmetric: bool = False, build_csc: bool = True,
-                 _handle=None):
+                 async_upload: bool = False, _handle=None):
+        """async_upload (symmetric graphs, or build_csc=False): return as soon as the
+        upload is enqueued, so it overlaps work on other graphs; the input arrays are
+        kept referenced by the graph until it is closed, and an invalid CSR is
+        reported by the first call on the graph (or by sync())."""
         self._lib = L.load()
         self._h = C.c_void_p()
+        self._keep = None
         if _handle is not None:
             self._h = _handle
         else:
@@ -104,8 +109,12 @@ class Graph:
             flags = (L.MG_GRAPH_SYMMETRIC if symmetric else 0) | (0 if build_csc else L.MG_GRAPH_NO_CSC)
             if ro_dev:
                 flags |= L.MG_GRAPH_DEVICE_INPUT
+            if async_upload:
+                flags |= L.MG_GRAPH_ASYNC_UPLOAD
             _check(self._lib.mg_graph_create(ro_p, ci_p, v_p, vt, n, m, flags, C.byref(self._h)),
                    "mg_graph_create")
+            if async_upload:
+                self._keep = (k1, k2, k3)  # the copy may still be reading them
             del k1, k2, k3
         n, m, fl, dev = C.c_int64(), C.c_int64(), C.c_uint32(), C.c_int32()
         _check(self._lib.mg_graph_info(self._h, C.byref(n), C.byref(m), C.byref(fl), C.byref(dev)), "mg_graph_info")
@@ -143,6 +152,10 @@ class Graph:
         return out
 
     # -- lifetime ---------------------------------------------------------------
+    def sync(self) -> None:
+        """Waits for an asynchronous upload and checks it (mg_graph_sync)."""
+        _check(self._lib.mg_graph_sync(self._h), "mg_graph_sync")
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             self._lib.mg_graph_destroy(self._h)

@@ -85,3 +85,31 @@ def test_repeated_runs_are_bit_identical():
         np.testing.assert_array_equal(a, b)
     for a, b in zip(runs[0][3:], runs[1][3:]):
         assert np.abs(a - b).sum() <= 1e-9
+
+
+def test_asynchronous_upload_overlaps_and_validates_on_first_use():
+    h = mg.gen_rmat(13, 16, 77, symmetrize=True)
+    ref = oracle.bfs(h.row_offsets, h.col_idx, [3])
+    g1 = mg.Graph(h.row_offsets, h.col_idx, symmetric=True, async_upload=True)
+    g2 = mg.Graph(h.row_offsets, h.col_idx, symmetric=True, async_upload=True)  # both uploads in flight
+    try:
+        np.testing.assert_array_equal(g1.bfs([3])[0], ref)
+        g2.sync()
+        np.testing.assert_array_equal(g2.bfs([3])[0], ref)
+    finally:
+        g1.close()
+        g2.close()
+    bad = h.col_idx.copy()
+    bad[7] = h.n + 5
+    g3 = mg.Graph(h.row_offsets, bad, symmetric=True, async_upload=True)  # accepted: checked on first use
+    try:
+        with pytest.raises(mg.MapGraphError) as ei:
+            g3.bfs([0])
+        assert ei.value.status == L.MG_ERR_ARG
+        with pytest.raises(mg.MapGraphError):
+            g3.sync()
+    finally:
+        g3.close()
+    # a graph that needs a CSC uploads synchronously whatever the flag
+    with pytest.raises(mg.MapGraphError):
+        mg.Graph(h.row_offsets, bad, async_upload=True)
