@@ -93,9 +93,10 @@ mg_status coo_to_csr(int64_t n, Coo &coo, int32_t wkind, bool canonical, mg_host
   }
   std::vector<int64_t> cnt((size_t)n + 1, 0);
   if (canonical) {
-    std::atomic<int64_t> *acnt = reinterpret_cast<std::atomic<int64_t> *>(cnt.data());
+    // GCC atomic builtins on the plain counters (no std::atomic aliasing).
+    int64_t *acnt = cnt.data();
 #pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < m; e++) acnt[coo.src[e]].fetch_add(1, std::memory_order_relaxed);
+    for (int64_t e = 0; e < m; e++) __atomic_fetch_add(&acnt[coo.src[e]], (int64_t)1, __ATOMIC_RELAXED);
   } else {
     for (int64_t e = 0; e < m; e++) cnt[coo.src[e]]++;
   }
@@ -109,9 +110,9 @@ mg_status coo_to_csr(int64_t n, Coo &coo, int32_t wkind, bool canonical, mg_host
   out->row_offsets[n] = (int32_t)run;
   if (canonical) {
     std::vector<int64_t> slot((size_t)m);
-    std::atomic<int64_t> *cur = reinterpret_cast<std::atomic<int64_t> *>(cnt.data());
+    int64_t *cur = cnt.data();
 #pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < m; e++) slot[e] = cur[coo.src[e]].fetch_add(1, std::memory_order_relaxed);
+    for (int64_t e = 0; e < m; e++) slot[e] = __atomic_fetch_add(&cur[coo.src[e]], (int64_t)1, __ATOMIC_RELAXED);
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < m; e++) {
       out->col_idx[slot[e]] = coo.dst[e];
