@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-scale", type=int, default=CPU_SAMPLE_SCALE,
+                   help="R-MAT scale of the bounded sample the reference's CPU code runs on")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-versus-looped section")
     p.add_argument("--batched-scale", type=int, default=20)
     p.add_argument("--pr-gather", default="auto", choices=["auto", "binned", "cached"],
@@ -339,9 +341,9 @@ def cpu_restatements(hs, src) -> dict:
     return out
 
 
-def cpu_sample_graph():
+def cpu_sample_graph(scale=CPU_SAMPLE_SCALE):
     import mirrorofmapgraph_b200 as mg
-    return mg.gen_rmat(CPU_SAMPLE_SCALE, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
+    return mg.gen_rmat(scale, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
 
 
 def _ref_worker(path, src, steps, warmup, barrier, out):
@@ -379,7 +381,8 @@ def run_reference(args):
         import mirrorofmapgraph_b200 as mg
         if not oracle.have_ref():
             raise RuntimeError("oracle/_ref/libmgref.so missing (reference CPU path not built)")
-        h = cpu_sample_graph()
+        sc = args.cpu_sample_scale
+        h = cpu_sample_graph(sc)
         try:
             ncores = len(os.sched_getaffinity(0))
         except Exception:
@@ -409,12 +412,12 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32",
             "data": "synthetic (seeded R-MAT)",
-            "config": {"workload": f"rmat_s{CPU_SAMPLE_SCALE}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
-                                   "CPUBFS + CPUCC + CPUPR", "scale": CPU_SAMPLE_SCALE, "n": h.n, "m": h.m},
+            "config": {"workload": f"rmat_s{sc}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
+                                   "CPUBFS + CPUCC + CPUPR", "scale": sc, "n": h.n, "m": h.m},
             "host": host_info(),
             "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs, "kind": "reference",
                              "sample": f"{procs} concurrent copies of the reference's serial CPUBFS/CPUCC/CPUPR, "
-                                       f"each {args.steps} step(s) on R-MAT scale {CPU_SAMPLE_SCALE} from its own "
+                                       f"each {args.steps} step(s) on R-MAT scale {sc} from its own "
                                        f"source (CPUPR alone takes ~35 s at scale 22)"},
             "per_algorithm": {k: {"gteps_per_core": v[0] / v[1] / 1e9 if v[1] else None, "core_seconds": v[1]}
                               for k, v in per.items()},
@@ -638,14 +641,14 @@ def run_ours(args):
         try:
             import oracle
             if oracle.have_ref():
-                hs = cpu_sample_graph()
+                hs = cpu_sample_graph(args.cpu_sample_scale)
                 r = cpu_reference_run(hs, sources(hs, 1, SEED + 1)[0])
                 ce = sum(r[k][0] for k in ("bfs", "cc", "pagerank"))
                 cs = sum(r[k][1] for k in ("bfs", "cc", "pagerank"))
                 line["cpu_baseline"] = {
                     "value": ce / cs / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
                     "sample": f"reference CPUBFS + CPUCC + CPUPR (serial, oracle/_ref) once on R-MAT scale "
-                              f"{CPU_SAMPLE_SCALE} (same generator); {cs:.1f} s of CPU work",
+                              f"{args.cpu_sample_scale} (same generator); {cs:.1f} s of CPU work",
                     "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")},
                     "host": host_info(),
                     "sssp": "reference CPUSSSP not run: O(n^2), hours at scale 22 (timed at the 4,096-vertex "
