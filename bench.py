@@ -346,6 +346,32 @@ def cpu_sample_graph(scale=CPU_SAMPLE_SCALE):
     return mg.gen_rmat(scale, 16, SEED, symmetrize=True, weights="int", p0=1, p1=255)
 
 
+def reference_cpu_baseline(scale: int) -> dict:
+    """`cpu_baseline` of the GPU arm: the reference's serial CPUBFS + CPUCC + CPUPR
+    (oracle/_ref) once on the R-MAT sample of the given scale, one core, plus the
+    FP64 / Dijkstra restatements timed beside them."""
+    try:
+        import oracle
+        if not oracle.have_ref():
+            return {"value": None, "unavailable": "oracle/_ref not built"}
+        hs = cpu_sample_graph(scale)
+        src = sources(hs, 1, SEED + 1)[0]
+        r = cpu_reference_run(hs, src)
+        ce = sum(r[k][0] for k in ("bfs", "cc", "pagerank"))
+        cs = sum(r[k][1] for k in ("bfs", "cc", "pagerank"))
+        return {
+            "value": ce / cs / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
+            "sample": f"reference CPUBFS + CPUCC + CPUPR (serial, oracle/_ref) once on R-MAT scale "
+                      f"{scale} (same generator); {cs:.1f} s of CPU work",
+            "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")},
+            "host": host_info(),
+            "sssp": "reference CPUSSSP not run: O(n^2), hours at scale 22 (timed at the 4,096-vertex "
+                    "ER case in the tests); see restatements",
+            "restatements": cpu_restatements(hs, src)}
+    except Exception as e:
+        return {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
+
+
 def _ref_worker(path, src, steps, warmup, barrier, out):
     """One reference process: loads the sample graph, runs the warm-up passes,
     waits for the others, then times `steps` passes of CPUBFS + CPUCC + CPUPR."""
@@ -638,26 +664,7 @@ def run_ours(args):
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            import oracle
-            if oracle.have_ref():
-                hs = cpu_sample_graph(args.cpu_sample_scale)
-                r = cpu_reference_run(hs, sources(hs, 1, SEED + 1)[0])
-                ce = sum(r[k][0] for k in ("bfs", "cc", "pagerank"))
-                cs = sum(r[k][1] for k in ("bfs", "cc", "pagerank"))
-                line["cpu_baseline"] = {
-                    "value": ce / cs / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
-                    "sample": f"reference CPUBFS + CPUCC + CPUPR (serial, oracle/_ref) once on R-MAT scale "
-                              f"{args.cpu_sample_scale} (same generator); {cs:.1f} s of CPU work",
-                    "per_algorithm": {k: r[k][0] / r[k][1] / 1e9 for k in ("bfs", "cc", "pagerank")},
-                    "host": host_info(),
-                    "sssp": "reference CPUSSSP not run: O(n^2), hours at scale 22 (timed at the 4,096-vertex "
-                            "ER case in the tests); see restatements",
-                    "restatements": cpu_restatements(hs, sources(hs, 1, SEED + 1)[0])}
-            else:
-                line["cpu_baseline"] = {"value": None, "unavailable": "oracle/_ref not built"}
-        except Exception as e:
-            line["cpu_baseline"] = {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
+        line["cpu_baseline"] = reference_cpu_baseline(args.cpu_sample_scale)
     g.close()
     if not args.no_batched:
         try:

@@ -44,3 +44,13 @@ def test_reference_arm_prints_one_contract_line():
 def test_reference_arm_is_silent_on_other_ranks():
     assert _run({"RANK": "1", "WORLD_SIZE": "2"}, "--impl", "reference", "--steps", "1", "--warmup", "0",
                 "--cpu-sample-scale", "12") == []
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref not built (reference CPU path)")
+def test_gpu_arm_cpu_baseline_runs_on_the_host():
+    import bench
+    cb = bench.reference_cpu_baseline(12)
+    assert "unavailable" not in cb, cb
+    assert cb["kind"] == "reference" and cb["cores"] == 1 and cb["unit"] == "GTEPS" and cb["value"] > 0
+    assert set(cb["per_algorithm"]) == {"bfs", "cc", "pagerank"}
+    assert {"sssp_dijkstra", "ppr_vector", "pagerank_adjoint"} <= set(cb["restatements"])
