@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--edge-factor", type=int, default=16)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-scale", type=int, default=CPU_SAMPLE_SCALE,
                    help="R-MAT scale of the bounded sample the reference's CPU code runs on")
