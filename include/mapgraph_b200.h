@@ -248,9 +248,17 @@ mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *
  * The same traversal and results as mg_bfs, for callers that must not allocate
  * device memory while they run (memory reserved up front, code running inside
  * an allocator). Frontier queues, visited bitmap, sources and the deferred-hub
- * list live in one static device array of 8.54 MB; nothing is allocated.
- * - depth must be DEVICE memory (n entries); opts->device_output and
- *   opts->use_graph are ignored (the level loop is driven from the host).
+ * list live in one static device array of 8.54 MB; the call allocates nothing.
+ * - The array belongs to the library's device code: every process that loads
+ *   the library holds 8.54 MB of it on each device where the library's kernels
+ *   get loaded, whether or not it calls this function. With CUDA's lazy module
+ *   loading (the default since CUDA 12) that memory is reserved when the module
+ *   first loads on a device, which can be inside the first call here. Make one
+ *   call (or any other engine call) on each device during set-up, before the
+ *   region that must not allocate.
+ * - depth must be DEVICE memory (n entries) of the graph's device; a host
+ *   pointer is rejected with MG_ERR_ARG before anything runs. opts->device_output
+ *   and opts->use_graph are ignored (the level loop is driven from the host).
  * - Graphs of more than MG_BFS_NOALLOC_MAX_VERTICES vertices, or more than
  *   MG_BFS_NOALLOC_MAX_SOURCES sources, are rejected with MG_ERR_ARG.
  * - The first call on a device looks up the array's device address
@@ -258,7 +266,9 @@ mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, const float *
  *   stream capture on the device.
  * - The array is shared by every graph on a device: two calls in flight on the
  *   same device at the same time (other threads or streams) race on it and
- *   corrupt each other's results. Serialise them. */
+ *   corrupt each other's results. Serialise them. Every return, an error
+ *   included, waits for the work the call queued, so serialised calls never
+ *   overlap on the GPU. */
 #define MG_BFS_NOALLOC_MAX_VERTICES (1 << 20)
 #define MG_BFS_NOALLOC_MAX_SOURCES 1024
 mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *depth, const mg_opts *opts,

@@ -533,6 +533,7 @@ extern "C" mg_status mg_bfs_batch(mg_graph *g, const int32_t *srcs, int32_t nsrc
     }
   }
   MG_TRY(graph_enter(g));
+  if (o.device_output) MG_TRY(check_device_ptr(g, depth, "mg_bfs_batch", "depth"));
   const size_t bytes = sizeof(int32_t) * (size_t)nsrc * (size_t)g->n;
   int32_t *out = depth;
   if (!o.device_output) {

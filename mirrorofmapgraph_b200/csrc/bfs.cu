@@ -479,6 +479,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     return MG_ERR_UNSUPPORTED;
   }
   MG_TRY(graph_enter(g));
+  if (o.device_output) MG_TRY(check_device_ptr(g, depth, "mg_bfs", "depth"));
   const int64_t n = g->n;
   int64_t qcap64 = o.queue_sizing > 0 ? (int64_t)std::ceil(o.queue_sizing * (double)n) : n;
   qcap64 = std::max<int64_t>(1, std::min<int64_t>(qcap64, n));
@@ -618,6 +619,12 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_BIG + noalloc_round(sizeof(int32_t) * B
 // writes the queues, sources and hub list before reading them.
 static __device__ __align__(256) uint32_t bfs_noalloc_scratch[NOALLOC_BYTES / sizeof(uint32_t)];
 
+// Waits for a stream when it goes out of scope.
+struct StreamDrain {
+  cudaStream_t s;
+  ~StreamDrain() { cudaStreamSynchronize(s); }
+};
+
 // Device address of the scratch array, resolved once per device (the first call
 // on a device; later calls reuse the cached address).
 static std::mutex noalloc_mu;
@@ -680,6 +687,7 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
     return MG_ERR_UNSUPPORTED;
   }
   MG_TRY(graph_enter(g));
+  MG_TRY(check_device_ptr(g, depth, "mg_bfs_noalloc", "depth"));
   char *scratch = nullptr;
   MG_TRY(noalloc_scratch_of(g->device, &scratch));
   const int64_t n = g->n;
@@ -716,6 +724,10 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   a.bar_limit = a.bar_extra ? debug_barrier_limit() : PERSIST_WAIT;
 
   const int32_t iter_cap = o.iter_num > 0 ? (int32_t)std::min<int64_t>(o.iter_num, n + 1) : (int32_t)(n + 1);
+  // From the first queued copy on, every return (errors included) waits for the
+  // stream: the queued work uses the shared scratch array, and a caller that
+  // serialises its calls must find the array idle when a call returns.
+  StreamDrain drain{s};
   MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
   MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
@@ -811,6 +823,10 @@ extern "C" mg_status mg_bfs_predecessors(mg_graph *g, const int32_t *depth, int3
     return MG_ERR_UNSUPPORTED;
   }
   MG_TRY(graph_enter(g));
+  if (dev_io) {
+    MG_TRY(check_device_ptr(g, depth, "mg_bfs_predecessors", "depth"));
+    MG_TRY(check_device_ptr(g, pred, "mg_bfs_predecessors", "pred"));
+  }
   const int64_t n = g->n;
   cudaStream_t s = g->stream;
   const int32_t *dlabel = depth;

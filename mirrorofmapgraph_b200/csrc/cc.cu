@@ -191,6 +191,7 @@ extern "C" mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_
   std::memset(&o, 0, sizeof(o));
   if (opts) o = *opts;
   MG_TRY(graph_enter(g));
+  if (o.device_output) MG_TRY(check_device_ptr(g, label, "mg_cc", "label"));
   const int64_t n = g->n;
   const size_t need = Carve::need({sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n, 64});
   MG_TRY(ws_reserve(g, g->ws_main, need));

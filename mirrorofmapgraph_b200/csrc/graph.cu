@@ -164,6 +164,28 @@ mg_status graph_enter(mg_graph *g) {
   return MG_OK;
 }
 
+mg_status check_device_ptr(const mg_graph *g, const void *p, const char *fn, const char *what) {
+  if (!p) return MG_OK;
+  cudaPointerAttributes at;
+  const cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    mg_set_error("%s: cannot query %s (%s): it must be device memory", fn, what, cudaGetErrorString(e));
+    return MG_ERR_ARG;
+  }
+  if (at.type == cudaMemoryTypeManaged) return MG_OK;
+  if (at.type != cudaMemoryTypeDevice) {
+    mg_set_error("%s: %s is %s memory; it must be device memory of device %d", fn, what,
+                 at.type == cudaMemoryTypeHost ? "pinned host" : "pageable host", g->device);
+    return MG_ERR_ARG;
+  }
+  if (at.device != g->device) {
+    mg_set_error("%s: %s is memory of device %d, the graph lives on device %d", fn, what, at.device, g->device);
+    return MG_ERR_ARG;
+  }
+  return MG_OK;
+}
+
 mg_status copy_out(mg_graph *g, void *dst, const void *src, size_t bytes, int device_output) {
   if (bytes == 0) return MG_OK;
   MG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, device_output ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,

@@ -184,6 +184,13 @@ struct Carve {
 // Makes the graph's device current; returns MG_ERR_CUDA on failure.
 mg_status graph_enter(mg_graph *g);
 
+// Checks, before any launch, that a caller's pointer that kernels will read or
+// write is device memory of the graph's device (or managed memory): a host
+// pointer passed where device memory is required returns MG_ERR_ARG instead of
+// faulting the GPU. A null pointer passes (callers check their own required
+// arguments). `fn` and `what` name the entry point and the argument in the error.
+mg_status check_device_ptr(const mg_graph *g, const void *p, const char *fn, const char *what);
+
 // Copies a device int32 array into a host or device destination.
 mg_status copy_out(mg_graph *g, void *dst, const void *src, size_t bytes, int device_output);
 #endif  // __CUDACC__

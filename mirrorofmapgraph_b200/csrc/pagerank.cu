@@ -1535,6 +1535,10 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
     return MG_ERR_ARG;
   }
   MG_TRY(graph_enter(g));
+  if (o.device_output) {
+    MG_TRY(check_device_ptr(g, ranks, "mg_pagerank", "ranks"));
+    MG_TRY(check_device_ptr(g, teleport, "mg_pagerank", "teleport"));
+  }
   if (o.mode == MG_PR_REFCOMPAT) {
     if (nvec != 1 || teleport) {
       mg_set_error("mg_pagerank: REFCOMPAT takes no teleport vector and nvec == 1");
@@ -1687,6 +1691,14 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
     return MG_ERR_ARG;
   }
   MG_TRY(graph_enter(g));
+  if (o.device_output) {
+    const char *fn = "mg_pagerank_backward";
+    MG_TRY(check_device_ptr(g, ranks, fn, "ranks"));
+    MG_TRY(check_device_ptr(g, dL_dranks, fn, "dL_dranks"));
+    MG_TRY(check_device_ptr(g, teleport, fn, "teleport"));
+    MG_TRY(check_device_ptr(g, dL_dweights, fn, "dL_dweights"));
+    MG_TRY(check_device_ptr(g, dL_dteleport, fn, "dL_dteleport"));
+  }
   const int64_t n = g->n, m = g->m;
   cudaStream_t s = g->stream;
   // Inputs staged on the device.

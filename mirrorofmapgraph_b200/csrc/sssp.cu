@@ -540,6 +540,7 @@ extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int
   o.directed = 1;
   if (opts) o = *opts;
   MG_TRY(graph_enter(g));
+  if (o.device_output) MG_TRY(check_device_ptr(g, dist, "mg_sssp", "dist"));
   int32_t *out = dist;
   if (!o.device_output) {
     MG_TRY(ws_reserve(g, g->ws_out, sizeof(int32_t) * (size_t)g->n + 256));
@@ -568,6 +569,7 @@ extern "C" mg_status mg_sssp_batch(mg_graph *g, const int32_t *srcs, int32_t nsr
   o.directed = 1;
   if (opts) o = *opts;
   MG_TRY(graph_enter(g));
+  if (o.device_output) MG_TRY(check_device_ptr(g, dist, "mg_sssp_batch", "dist"));
   MG_TRY(sssp_check(g, srcs, nsrc, o, "mg_sssp_batch"));
   const int64_t n = g->n;
   int shift = 0;

@@ -29,7 +29,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "libmgoracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmgref.so")
-REFERENCE_DIR = os.environ.get("MG_REFERENCE_DIR", "/root/reference")
+# The reference checkout: MG_REFERENCE_DIR, else a "reference" directory beside
+# this repository's checkout.
+REFERENCE_DIR = os.environ.get("MG_REFERENCE_DIR",
+                               os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 INT_MAX = 2**31 - 1
 REF_SSSP_UNREACHED = 100000000  # Algorithms/SSSP/sssp.cu:139
 

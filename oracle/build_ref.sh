@@ -18,8 +18,9 @@
 # The reference's GPU engine is not built (CUDA 12 removed texture references and
 # its arch flags stop at sm_35); only this CPU path compiles here.
 set -e
-REF="${MG_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
+# The reference checkout: MG_REFERENCE_DIR, else "reference" beside this repository.
+REF="${MG_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 CUDA="${CUDA_HOME:-/usr/local/cuda}"
 
