@@ -48,7 +48,8 @@ class MgPrOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("directed", C.c_int32), ("max_iter", C.c_int32), ("weighted", C.c_int32),
                 ("alpha", C.c_double), ("tol", C.c_double), ("compensated", C.c_int32),
                 ("device_output", C.c_int32), ("use_graph", C.c_int32), ("gather_kernel", C.c_int32),
-                ("autotune", C.c_int32), ("group_width", C.c_int32)]
+                ("autotune", C.c_int32), ("group_width", C.c_int32), ("seg_hub_edges", C.c_int32),
+                ("seg_block_cols", C.c_int32)]
 
 
 class MgPartLevel(C.Structure):
@@ -127,6 +128,7 @@ SIGNATURES = {
     "mg_graph_trace": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "mg_debug_fail_alloc": (C.c_int, [C.c_int64]),
     "mg_debug_barrier_skew": (C.c_int, [C.c_int32, C.c_int64]),
+    "mg_debug_seg_plan": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

@@ -29,6 +29,7 @@
 #include "expand.cuh"
 #include "pr_binned.cuh"
 #include "pr_gather.cuh"
+#include "pr_segment.cuh"
 #include "ppr.cuh"
 
 namespace mg {
@@ -58,11 +59,19 @@ struct PlanSet {
   BinPlan bcsc, bcsr;
   bool bcsc_ok = false, bcsr_ok = false;
   HubCache hubs;
-  int32_t tuned_cap = -1;  // autotuned column-cache capacity (-1 not tuned, 0 no cache)
+  SegPlan seg;  // column-segmented gather of the hub rows (forward gather)
+  // Autotuned forward gather (-1: not tuned): its gather_kernel variant, column-cache
+  // capacity (0 none), and for the segmented gather its hub threshold and block width.
+  int32_t tuned_variant = -1;
+  int32_t tuned_cap = 0;
+  int32_t tuned_seg_T = 0;
+  int32_t tuned_seg_S = 0;
   int32_t tuned_ppr_w = -1;  // autotuned personalised-PageRank group width (-1 not tuned)
 };
 
 }  // namespace mg
+
+static void seg_plan_release(mg_graph *g, mg::SegPlan &sp);
 
 static mg::PlanSet *plans_of(mg_graph *g) {
   if (!g->plan_csc) g->plan_csc = new mg::PlanSet();
@@ -78,6 +87,7 @@ void pr_release_plans(mg_graph *g) {
   }
   for (mg::BinPlan *b : {&ps->bcsc, &ps->bcsr}) bin_plan_release(g->stream, *b);
   for (void *q : {(void *)ps->hubs.cidx, (void *)ps->hubs.slot, (void *)ps->hubs.hv}) dev_free(g, q);
+  seg_plan_release(g, ps->seg);
   delete ps;
   g->plan_csc = nullptr;
 }
@@ -109,7 +119,8 @@ static mg_status get_plan(mg_graph *g, bool csr, mg::GatherPlan **out) {
 // Degree-binned plan of any row-offset array (n + 1 entries) on stream s: the
 // CSC of a graph (forward gather), its CSR (adjoint, row sums) or the owned rows
 // of a partition slice.
-static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
+static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp,
+                                     int32_t heavy) {
   using namespace mg;
   auto alloc = [&](void **p, size_t bytes) -> mg_status {
     if (mg_malloc_async(p, std::max<size_t>(bytes, 4), s) != cudaSuccess) {
@@ -125,7 +136,7 @@ static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t
   MG_CUDA_TRY(mg_malloc_async((void **)&counts, sizeof(int64_t) * ((nchunks + 2) * (PRB_BINS + 1)), s));
   int64_t *totals = counts + nchunks * (PRB_BINS + 1);
   int64_t *dboff = totals + (PRB_BINS + 1);
-  prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts);
+  prb_count_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, heavy);
   prb_offsets_kernel<<<1, 32, 0, s>>>(counts, nchunks, totals);
   int64_t cnt[PRB_BINS + 1];
   MG_CUDA_TRY(cudaMemcpyAsync(cnt, totals, sizeof(cnt), cudaMemcpyDeviceToHost, s));
@@ -157,7 +168,7 @@ static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t
   MG_CUDA_TRY(cudaMemsetAsync(bp.grab, 0, sizeof(int32_t), s));
   MG_CUDA_TRY(cudaMemsetAsync(bp.hcount, 0, sizeof(int32_t) * std::max<int64_t>(bp.nheavy, 1), s));
   MG_CUDA_TRY(cudaMemcpyAsync(dboff, bp.boff, sizeof(int64_t) * (PRB_BINS + 1), cudaMemcpyHostToDevice, s));
-  prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows);
+  prb_scatter_kernel<<<(unsigned)nchunks, PRB_NT, 0, s>>>(off, n, counts, dboff, bp.rows, bp.hrows, heavy);
   prb_hubs_kernel<<<1, PRB_NT, 0, s>>>(off, bp.hrows, bp.nheavy, bp.hbase);
   MG_CUDA_TRY(cudaGetLastError());
   MG_CUDA_TRY(cudaFreeAsync(counts, s));
@@ -165,9 +176,9 @@ static mg_status bin_plan_build_impl(cudaStream_t s, const int32_t *off, int64_t
 }
 
 // A failed build releases what it had allocated.
-mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp) {
+mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp, int32_t heavy) {
   bp = mg::BinPlan();
-  const mg_status st = bin_plan_build_impl(s, off, n, bp);
+  const mg_status st = bin_plan_build_impl(s, off, n, bp, heavy);
   if (st != MG_OK) bin_plan_release(s, bp);
   return st;
 }
@@ -215,6 +226,7 @@ static mg::PrbArgs prb_args_of(const mg_graph *g, const mg::BinPlan &bp, bool cs
   }
   p.nheavy = bp.nheavy;
   p.grab = nullptr;
+  p.hubs_summed = 0;
   return p;
 }
 
@@ -250,6 +262,7 @@ struct SolveArgs {
   double *part1, *part2;      // per-CTA FP64 partials of the two kernels
   int32_t grid1, grid2;
   const int32_t *hslot;       // shared-memory column cache: slot of each vertex (nullptr: no cache)
+  int32_t gswz;               // 1: x/s of vertex v lives at g[seg_swz(v)] (segmented gather)
   float *gh0, *gh1;           // cached columns' gathered values, ping-pong with g0/g1
   int32_t nhub;               // cached columns
   DevCtl *ctl;
@@ -281,7 +294,7 @@ struct RowUpdate {
       float gv = 0.f;
       if (s > 0.0) gv = (float)(nv / s);
       else red2 += nv;
-      gnew[r] = gv;
+      gnew[a->gswz ? seg_swz(r) : r] = gv;
       if (ghnew) {
         const int32_t sl = __ldg(a->hslot + r);
         if (sl >= 0) ghnew[sl] = gv;
@@ -481,6 +494,24 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
     p.hcontrib[2 * h + 1] = hu.red2;
     __threadfence();
   };
+  if (p.hubs_summed) {
+    // Hub rows of the segmented gather: one warp per hub adds its fragment sums
+    // (lane l takes sums l, l + 32, ...; then a fixed pairing tree) and lane 0
+    // applies the row update, counted in this CTA's partials.
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t)gridDim.x * (PRB_HUB_NT / 32);
+    for (int64_t h = (int64_t)blockIdx.x * (PRB_HUB_NT / 32) + (threadIdx.x >> 5); h < p.nheavy; h += nw) {
+      const int32_t fb = p.hbase[h], nfr = p.hbase[h + 1] - fb;
+      const float2 *parts = reinterpret_cast<const float2 *>(p.hpart) + fb;
+      Comp t{0.f, 0.f};
+      for (int32_t k = lane; k < nfr; k += 32) {
+        const float2 v = parts[k];
+        comp_add(t, Comp{v.x, v.y});
+      }
+      group_comp_reduce<32>(t);
+      if (lane == 0) up(p.hrows[h], t);
+    }
+  }
   prb_run<WEIGHTED, PRB_HUB_ADAPT>(p, [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); }, up,
                     hub);
   const double r = block_sum<PRB_HUB_NT>(up.resid, s_red);
@@ -491,7 +522,41 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
   }
   if (last_block(&c->blocks_done)) {
     if (threadIdx.x == 0 && p.grab) *p.grab = 0;
-    solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.nheavy, s_red);
+    solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.hubs_summed ? 0 : p.nheavy, s_red);
+  }
+}
+
+// Phase 1 of a segmented iteration (pr_segment.cuh): the hub rows' fragments,
+// block by block, out of shared-memory copies of x/s; each fragment's sum goes to
+// its slot in hpart. Phase 2, solve_binned_hub_kernel launched after this kernel
+// (PrbArgs.hubs_summed), finishes the hub rows from those sums, runs the other
+// rows and ends the iteration. One CTA of SEG_NT threads per SM (the plan's ranges
+// are cut for that grid).
+constexpr int SEG_NT = 1024;
+
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(SEG_NT, 1) solve_segment_kernel(SolveArgs a, PrbArgs p, SegArgs sg) {
+  extern __shared__ __align__(128) float s_buf[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int32_t s_next[2];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *__restrict__ gold = cur ? a.g1 : a.g0;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  auto fin = [&](const int2 &e, const Comp &acc) {
+    if (e.x >= 0) p.hpart[e.x] = acc;
+  };
+  uint32_t phase = 0;
+  bool ok = true;
+  seg_phase<WEIGHTED>(sg, gold, s_buf, &s_bar, s_next, phase, ok, fin);
+  if (!ok) {
+    c->status = MG_ERR_TIMEOUT;
+    c->done = 1;
   }
 }
 
@@ -531,7 +596,7 @@ __global__ void hub_slot_kernel(const int32_t *__restrict__ ro, int64_t n, int32
 }
 
 __global__ void hub_remap_kernel(const int32_t *__restrict__ ri, int64_t m, const int32_t *__restrict__ slot,
-                                 int32_t *cidx) {
+                                 int32_t *cidx, int32_t swz = 0) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m + 8; k += (int64_t)gridDim.x * blockDim.x) {
     if (k >= m) {
       cidx[k] = 0;
@@ -539,12 +604,14 @@ __global__ void hub_remap_kernel(const int32_t *__restrict__ ri, int64_t m, cons
     }
     const int32_t c = ri[k];
     const int32_t sl = slot[c];
-    cidx[k] = sl >= 0 ? (int32_t)((uint32_t)sl | 0x80000000u) : c;
+    cidx[k] = sl >= 0 ? (int32_t)((uint32_t)sl | 0x80000000u) : (swz ? seg_swz(c) : c);
   }
 }
 
-__global__ void hub_fill_kernel(const int32_t *__restrict__ hv, int32_t K, const float *__restrict__ g, float *gh) {
-  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) gh[i] = g[hv[i]];
+__global__ void hub_fill_kernel(const int32_t *__restrict__ hv, int32_t K, const float *__restrict__ g, float *gh,
+                                int32_t swz) {
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x)
+    gh[i] = g[swz ? seg_swz(hv[i]) : hv[i]];
 }
 
 struct RowSumStore {
@@ -588,9 +655,10 @@ __global__ void __launch_bounds__(256) solve_init_kernel(SolveArgs a) {
     if (!a.adjoint) {
       const double s = (double)a.srow[i];
       a.v0[i] = (float)t;
-      if (s > 0.0) a.g0[i] = (float)(t / s);
+      const int64_t gi = a.gswz ? seg_swz((int32_t)i) : i;
+      if (s > 0.0) a.g0[gi] = (float)(t / s);
       else {
-        a.g0[i] = 0.f;
+        a.g0[gi] = 0.f;
         acc += (double)(float)t;
       }
     } else {
@@ -680,10 +748,13 @@ struct SolvePlan {
   mg::SolveArgs a;
   GatherLaunch gather;  // merge-path variant (use_tma)
   mg::PrbArgs p;        // degree-binned variant (default)
+  mg::SegArgs sg;       // segmented variant: phase 1's fragments
   bool weighted;
   bool use_tma;
   bool use_hub;         // degree-binned with the shared-memory column cache
-  int32_t hub_bytes;    // its dynamic shared memory
+  bool use_seg;         // segmented hub rows + column cache for the rest
+  int32_t hub_bytes;    // dynamic shared memory of the column-cache kernel
+  int32_t seg_bytes;    // dynamic shared memory of the segmented gather's phase 1 (a column block)
 };
 
 template <bool W>
@@ -693,6 +764,15 @@ static int hub_occupancy(int32_t bytes) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::solve_binned_hub_kernel<W>, mg::PRB_HUB_NT, bytes);
   cudaGetLastError();
   return std::max(1, std::min(occ, PRB_HUB_MINB));
+}
+
+template <bool W>
+static int seg_occupancy(int32_t bytes) {
+  int occ = 0;
+  cudaFuncSetAttribute(mg::solve_segment_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::solve_segment_kernel<W>, mg::SEG_NT, bytes);
+  cudaGetLastError();
+  return occ;
 }
 
 template <bool W>
@@ -753,6 +833,200 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
   return MG_OK;
 }
 
+// ---- segmented gather plan (pr_segment.cuh) ----
+static void seg_plan_release(mg_graph *g, mg::SegPlan &sp) {
+  bin_plan_release(g->stream, sp.bins);
+  for (void *q : {(void *)sp.sidx, (void *)sp.swts, (void *)sp.ent, (void *)sp.gofs, (void *)sp.pidx,
+                  (void *)sp.pwts, (void *)sp.bgrp, (void *)sp.bdense, (void *)sp.cta})
+    dev_free(g, q);
+  sp = mg::SegPlan();
+}
+
+static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted, const mg::HubCache &hc,
+                                mg::SegPlan &sp) {
+  using namespace mg;
+  const int64_t n = g->n, m = g->m;
+  cudaStream_t s = g->stream;
+  const int64_t B = (n + S - 1) / S;
+  if (B > SEG_MAXB || S % 32 != 0) {
+    mg_set_error("segmented gather: %lld column blocks of %d exceed the plan's limit of %d", (long long)B, S,
+                 SEG_MAXB);
+    return MG_ERR_UNSUPPORTED;
+  }
+  sp.T = T;
+  sp.S = S;
+  sp.nblocks = (int32_t)B;
+  sp.grid = g->num_sms;
+  sp.weighted = weighted;
+  MG_TRY(bin_plan_build(s, g->co, n, sp.bins, T));
+  const int64_t nh = sp.bins.nheavy;
+  auto scratch = [&](void **q, size_t bytes) -> mg_status {
+    if (mg_malloc_async(q, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+      cudaGetLastError();
+      *q = nullptr;
+      mg_set_error("segmented gather plan: device allocation of %zu bytes failed", bytes);
+      return MG_ERR_OOM;
+    }
+    return MG_OK;
+  };
+  struct Tmp {  // plan-build scratch, released on every return
+    cudaStream_t s;
+    std::vector<void *> p;
+    ~Tmp() {
+      for (void *q : p)
+        if (q) cudaFreeAsync(q, s);
+    }
+  } tmp{s, {}};
+  int32_t *nfr = nullptr, *lencnt = nullptr;
+  const size_t nkeys = (size_t)B * SEG_FMAX;
+  MG_TRY(scratch((void **)&nfr, sizeof(int32_t) * (size_t)std::max<int64_t>(nh, 1)));
+  tmp.p.push_back(nfr);
+  MG_TRY(scratch((void **)&lencnt, sizeof(int32_t) * nkeys));
+  tmp.p.push_back(lencnt);
+  MG_CUDA_TRY(cudaMemsetAsync(lencnt, 0, sizeof(int32_t) * nkeys, s));
+  const size_t hsm = sizeof(int32_t) * (size_t)B;
+  if (nh > 0) seg_hist_kernel<<<(unsigned)nh, 256, hsm, s>>>(g->co, g->ri, sp.bins.hrows, S, (int32_t)B, nfr, lencnt);
+  seg_scan_kernel<<<1, 256, 0, s>>>(nfr, nh, sp.bins.hbase);
+  MG_CUDA_TRY(cudaGetLastError());
+  std::vector<int32_t> lc(nkeys);
+  int32_t nfrag = 0;
+  MG_CUDA_TRY(cudaMemcpyAsync(lc.data(), lencnt, sizeof(int32_t) * nkeys, cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(&nfrag, sp.bins.hbase + nh, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  sp.nfrag = nfrag;
+  // Slots: per block, fragments longest first, the block's list padded to whole
+  // groups of 32. A group's longest fragment (its first slot) sets its ELL depth.
+  std::vector<int32_t> cursor(nkeys), bgrp((size_t)B + 1);
+  std::vector<int32_t> gdepth;
+  int64_t grp = 0;
+  for (int64_t b = 0; b < B; b++) {
+    bgrp[b] = (int32_t)grp;
+    const int64_t s0 = grp * 32;
+    int64_t k = 0;
+    for (int32_t key = 0; key < SEG_FMAX; key++) {
+      const int32_t len = SEG_FMAX - key, cnt = lc[(size_t)b * SEG_FMAX + key];
+      cursor[(size_t)b * SEG_FMAX + key] = (int32_t)(s0 + k);
+      for (int64_t kk = (k + 31) / 32 * 32; kk < k + cnt; kk += 32) gdepth.push_back(len);
+      k += cnt;
+    }
+    grp += (k + 31) / 32;
+  }
+  if (grp * 32 > INT32_MAX) {
+    mg_set_error("segmented gather plan: %lld fragment slots exceed 2^31", (long long)(grp * 32));
+    return MG_ERR_UNSUPPORTED;
+  }
+  sp.ngroups = grp;
+  bgrp[B] = (int32_t)grp;
+  std::vector<int64_t> gofs((size_t)grp + 1);
+  gofs[0] = 0;
+  for (int64_t gi = 0; gi < grp; gi++) gofs[gi + 1] = gofs[gi] + 32 * (int64_t)gdepth[gi];
+  sp.nell = gofs[grp];
+  const size_t slots = (size_t)std::max<int64_t>(grp * 32, 1);
+  // hub partials count fragments
+  cudaFreeAsync(sp.bins.hpart, s);
+  sp.bins.hpart = nullptr;
+  MG_TRY(scratch((void **)&sp.bins.hpart, sizeof(Comp) * (size_t)std::max<int32_t>(nfrag, 1)));
+  MG_TRY(dev_alloc(g, (void **)&sp.ent, sizeof(int2) * slots));
+  MG_TRY(dev_alloc(g, (void **)&sp.gofs, sizeof(int64_t) * gofs.size()));
+  MG_TRY(dev_alloc(g, (void **)&sp.pidx, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nell, 1)));
+  if (weighted) MG_TRY(dev_alloc(g, (void **)&sp.pwts, sizeof(float) * (size_t)std::max<int64_t>(sp.nell, 1)));
+  MG_TRY(dev_alloc(g, (void **)&sp.bgrp, sizeof(int32_t) * bgrp.size()));
+  MG_TRY(dev_alloc(g, (void **)&sp.bdense, (size_t)std::max<int64_t>(B, 1)));
+  MG_TRY(dev_alloc(g, (void **)&sp.cta, sizeof(int32_t) * (size_t)(sp.grid + 1)));
+  MG_TRY(dev_alloc(g, (void **)&sp.sidx, sizeof(int32_t) * (size_t)(m + 8)));
+  if (weighted) MG_TRY(dev_alloc(g, (void **)&sp.swts, sizeof(float) * (size_t)(m + 8)));
+  int32_t *fsrc = nullptr, *flen = nullptr;
+  MG_TRY(scratch((void **)&fsrc, sizeof(int32_t) * slots));
+  tmp.p.push_back(fsrc);
+  MG_TRY(scratch((void **)&flen, sizeof(int32_t) * slots));
+  tmp.p.push_back(flen);
+  MG_CUDA_TRY(cudaMemsetAsync(sp.ent, 0xff, sizeof(int2) * slots, s));
+  MG_CUDA_TRY(cudaMemsetAsync(sp.pidx, 0xff, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nell, 1), s));
+  if (weighted) MG_CUDA_TRY(cudaMemsetAsync(sp.pwts, 0, sizeof(float) * (size_t)std::max<int64_t>(sp.nell, 1), s));
+  MG_CUDA_TRY(cudaMemcpyAsync(sp.gofs, gofs.data(), sizeof(int64_t) * gofs.size(), cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(sp.bgrp, bgrp.data(), sizeof(int32_t) * bgrp.size(), cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(lencnt, cursor.data(), sizeof(int32_t) * nkeys, cudaMemcpyHostToDevice, s));
+  // sidx: every row's indices with the cached columns flagged, then the hub rows
+  // regrouped by block (plain indices); swts follows sidx's order
+  hub_remap_kernel<<<g->num_sms * 8, 256, 0, s>>>(g->ri, m, hc.slot, sp.sidx, 1);
+  if (weighted) {
+    MG_CUDA_TRY(cudaMemcpyAsync(sp.swts, g->cvals, sizeof(float) * (size_t)m, cudaMemcpyDeviceToDevice, s));
+    MG_CUDA_TRY(cudaMemsetAsync(sp.swts + m, 0, sizeof(float) * 8, s));
+  }
+  if (nh > 0)
+    seg_fill_kernel<<<(unsigned)nh, 32, hsm, s>>>(g->co, g->ri, weighted ? (const float *)g->cvals : nullptr,
+                                                  sp.bins.hrows, sp.bins.hbase, S, (int32_t)B, lencnt, sp.sidx,
+                                                  sp.swts, sp.ent, fsrc, flen);
+  if (grp > 0)
+    seg_sell_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.ent, fsrc, flen, sp.gofs, grp, sp.sidx, sp.swts, sp.pidx,
+                                                   sp.pwts);
+  MG_CUDA_TRY(cudaGetLastError());
+  // Dense blocks are staged in shared memory; phase 1's groups are cut into one
+  // contiguous range per CTA by estimated cost: sliced-ELL entries (a global
+  // gather counting SEG_GLOBAL_FACTOR), a fixed cost per group, and a block load
+  // wherever a CTA's range enters a dense block.
+  std::vector<uint8_t> dense((size_t)std::max<int64_t>(B, 1), 0);
+  std::vector<int32_t> gblock((size_t)grp);
+  for (int64_t b = 0; b < B; b++) {
+    dense[b] = (gofs[bgrp[b + 1]] - gofs[bgrp[b]]) >= SEG_DENSE ? 1 : 0;
+    for (int64_t gi = bgrp[b]; gi < bgrp[b + 1]; gi++) gblock[gi] = (int32_t)b;
+  }
+  auto gcost = [&](int64_t gi) {
+    return 32 * (int64_t)gdepth[gi] * (dense[gblock[gi]] ? 1 : SEG_GLOBAL_FACTOR) + SEG_GROUP_COST;
+  };
+  // Greedy cut for a cost cap per CTA (a range closes before the group that would
+  // pass the cap); the smallest cap that needs at most `grid` ranges is kept.
+  std::vector<int32_t> cta((size_t)sp.grid + 1, (int32_t)grp);
+  auto cut = [&](int64_t cap, bool write) {
+    int64_t acc = 0, start = 0;
+    int32_t used = grp > 0 ? 1 : 0;
+    if (write) cta[0] = 0;
+    for (int64_t gi = 0; gi < grp; gi++) {
+      const bool enters = gi == start || gblock[gi] != gblock[gi - 1];
+      int64_t c = gcost(gi) + ((enters && dense[gblock[gi]]) ? SEG_LOAD_COST : 0);
+      if (acc + c > cap && gi > start) {  // close the range before gi
+        if (write && used < sp.grid) cta[used] = (int32_t)gi;
+        used++;
+        start = gi;
+        acc = 0;
+        c = gcost(gi) + (dense[gblock[gi]] ? SEG_LOAD_COST : 0);
+      }
+      acc += c;
+    }
+    return used;
+  };
+  int64_t lo = 1, hi = 1;
+  for (int64_t gi = 0; gi < grp; gi++) hi += gcost(gi) + SEG_LOAD_COST;
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (cut(mid, false) <= sp.grid) hi = mid;
+    else lo = mid + 1;
+  }
+  cut(lo, true);
+  MG_CUDA_TRY(cudaMemcpyAsync(sp.bdense, dense.data(), dense.size(), cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaMemcpyAsync(sp.cta, cta.data(), sizeof(int32_t) * cta.size(), cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  sp.ok = true;
+  return MG_OK;
+}
+
+// Segmented plan for (T, S), rebuilt when either changes; a failed build leaves
+// nothing behind.
+static mg_status get_seg_plan(mg_graph *g, int32_t T, int32_t S, bool weighted, const mg::HubCache &hc,
+                              mg::SegPlan **out) {
+  mg::SegPlan &sp = plans_of(g)->seg;
+  if (!sp.ok || sp.T != T || sp.S != S || sp.weighted != weighted) {
+    seg_plan_release(g, sp);
+    const mg_status st = seg_plan_build(g, T, S, weighted, hc, sp);
+    if (st != MG_OK) {
+      seg_plan_release(g, sp);
+      return st;
+    }
+  }
+  *out = &sp;
+  return MG_OK;
+}
+
 // Capacity of the column cache: half of an SM's shared memory per CTA (two CTAs
 // of PRB_HUB_NT threads per SM), less the kernel's own static shared memory.
 static int32_t hub_cache_limit(mg_graph *g) {
@@ -766,24 +1040,37 @@ static int32_t hub_cache_limit(mg_graph *g) {
 
 static int32_t hub_cache_capacity(mg_graph *g) { return std::min(PRB_HUB_CAP, hub_cache_limit(g)); }
 
+// Default shape of the segmented gather: hub rows of at least 1024 edges, column
+// blocks as wide as the column cache (the kernel then asks for the cached gather's
+// shared memory, leaving L1 the same room for phase 2's uncached gathers).
+constexpr int32_t SEG_DEFAULT_T = 1024;
+static int32_t seg_block_default(mg_graph *g) { return std::max<int32_t>(1024, hub_cache_capacity(g) & ~1023); }
+
 // Carves the solver's buffers out of ws_main (every per-vertex array padded to
 // n + 8 entries for the widened tile copies), copies the teleport vector and the
 // adjoint right-hand side into padded buffers, computes the row sums s_u and picks
 // the gather variant.
 static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const float *tele_src,
-                             const float *wvec_src, int variant, SolvePlan &sp, int32_t hub_cap = -1) {
+                             const float *wvec_src, int variant, SolvePlan &sp, int32_t hub_cap = -1,
+                             int32_t seg_T = 0, int32_t seg_S = 0) {
   using namespace mg;
   const bool use_tma = variant == 1;
-  const bool use_hub = variant == 2 && !adjoint && g->n > 0;
+  const bool use_seg = variant == 3 && !adjoint && g->n > 0;
+  const bool use_hub = (variant == 2 || use_seg) && !adjoint && g->n > 0;
   GatherPlan *plan = nullptr;
   BinPlan *bins = nullptr, *rbins = nullptr;
   HubCache *hubs = nullptr;
-  if (use_tma) MG_TRY(get_plan(g, adjoint, &plan));
-  else MG_TRY(get_bin_plan(g, adjoint, &bins));
+  SegPlan *seg = nullptr;
   if (use_hub) MG_TRY(get_hub_cache(g, hub_cap > 0 ? hub_cap : hub_cache_capacity(g), &hubs));
+  if (use_tma) MG_TRY(get_plan(g, adjoint, &plan));
+  else if (use_seg) {
+    MG_TRY(get_seg_plan(g, seg_T > 0 ? seg_T : SEG_DEFAULT_T, seg_S > 0 ? seg_S : seg_block_default(g), weighted,
+                        *hubs, &seg));
+    bins = &seg->bins;
+  } else MG_TRY(get_bin_plan(g, adjoint, &bins));
   if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
-  const size_t np = (size_t)n + 8;
+  const size_t np = (size_t)((n + 31) & ~(int64_t)31) + 8;  // whole 32-entry chunks (seg_swz) and a pad
   const int32_t nt = plan ? plan->ntiles : 1;
   const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
   SolveArgs &a = sp.a;
@@ -795,12 +1082,25 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
   a.ri_wvec = adjoint ? nr++ : -1;
   int occ = 0;
   sp.use_tma = use_tma;
-  sp.use_hub = use_hub;
+  sp.use_hub = use_hub && !use_seg;
+  sp.use_seg = use_seg;
   sp.hub_bytes = use_hub ? (int32_t)(sizeof(float) * hubs->K) : 0;
+  sp.seg_bytes = use_seg ? (int32_t)(sizeof(float) * seg->S) : 0;
   sp.weighted = weighted;
   sp.gather = nullptr;
   if (use_tma) sp.gather = gather_variant(weighted, nr, &occ);
-  else if (use_hub) occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
+  else if (use_seg) {
+    occ = weighted ? seg_occupancy<true>(sp.seg_bytes) : seg_occupancy<false>(sp.seg_bytes);
+    if (occ < 1) {
+      mg_set_error("segmented gather: a CTA of %d threads with %d bytes of shared memory does not fit an SM", SEG_NT,
+                   sp.seg_bytes);
+      return MG_ERR_UNSUPPORTED;
+    }
+    // phase 1's ranges are cut for one CTA per SM; phase 2 (the column-cache
+    // kernel) runs one CTA per SM as well
+    occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
+    occ = 1;
+  } else if (use_hub) occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
   else occ = weighted ? binned_occupancy<true>() : binned_occupancy<false>();
   const int g1 = g->num_sms * std::max(1, std::min(occ, 8));
   const int g2 = use_tma ? std::max(1, (nt + PRG_NT - 1) / PRG_NT) : 0;
@@ -864,7 +1164,18 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
 #if PRB_DYNAMIC
     sp.p.grab = bins->grab;  // the solve kernels' last CTA resets it
 #endif
-    if (use_hub) sp.p.idx = hubs->cidx;
+    if (use_seg) {
+      sp.p.idx = seg->sidx;
+      if (weighted) sp.p.wts = seg->swts;
+      sp.p.grab = bins->grab;  // phase 2 always takes items from the counter
+      sp.p.wstart[PRB_BINS] = sp.p.wstart[6];  // hub rows are phase 1's, not work items of phase 2
+      sp.p.hubs_summed = 1;
+      sp.sg = SegArgs{seg->ent,  seg->gofs, seg->pidx, seg->pwts, seg->bgrp, seg->cta,
+                      seg->bdense, (n + 31) & ~(int64_t)31, seg->S, seg->nblocks};
+      a.gswz = 1;
+    } else if (use_hub) {
+      sp.p.idx = hubs->cidx;
+    }
   }
   MG_CUDA_TRY(cudaGetLastError());
   return MG_OK;
@@ -880,16 +1191,17 @@ static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) 
   MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
   solve_init_kernel<<<ginit, 256, 0, s>>>(a);
   solve_init_reduce_kernel<<<1, 256, 0, s>>>(a, ginit);
-  if (sp.use_hub) {
+  if (sp.use_hub || sp.use_seg) {
     const HubCache &hc = plans_of(g)->hubs;
-    hub_fill_kernel<<<g->num_sms, 256, 0, s>>>(hc.hv, hc.K, a.g0, a.gh0);
+    hub_fill_kernel<<<g->num_sms, 256, 0, s>>>(hc.hv, hc.K, a.g0, a.gh0, a.gswz);
   }
   MG_CUDA_TRY(cudaGetLastError());
   struct Sig {
     SolveArgs a;
     GatherLaunch gl;
     PrbArgs p;
-    int w, tma, hub;
+    SegArgs sg;
+    int w, tma, hub, seg;
   } sig;
   std::memset(&sig, 0, sizeof(sig));
   sig.a = a;
@@ -898,18 +1210,31 @@ static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) 
   sig.w = sp.weighted;
   sig.tma = sp.use_tma;
   sig.hub = sp.use_hub;
+  sig.seg = sp.use_seg;
+  if (sp.use_seg) sig.sg = sp.sg;
   const int g1 = a.grid1, g2 = a.grid2;
   const GatherLaunch gl = sp.gather;
   const PrbArgs p = sp.p;
-  const bool tma = sp.use_tma, w = sp.weighted, hub = sp.use_hub;
-  const int32_t hb = sp.hub_bytes;
-  LoopBody body = [a, gl, p, g1, g2, tma, w, hub, hb](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+  const SegArgs sg = sp.sg;
+  const bool tma = sp.use_tma, w = sp.weighted, hub = sp.use_hub, seg = sp.use_seg;
+  const int32_t hb = sp.hub_bytes, sb = sp.seg_bytes;
+  LoopBody body = [a, gl, p, sg, g1, g2, tma, w, hub, seg, hb, sb](cudaStream_t st, cudaGraphConditionalHandle h,
+                                                                  int use_cond) {
     SolveArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
     if (tma) {
       gl(g1, st, b);
       solve_fixup_kernel<<<g2, PRG_NT, 0, st>>>(b);
+    } else if (seg) {
+      // phase 1 (hub fragments), then the other rows and the iteration's end
+      if (w) {
+        solve_segment_kernel<true><<<g1, SEG_NT, sb, st>>>(b, p, sg);
+        solve_binned_hub_kernel<true><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
+      } else {
+        solve_segment_kernel<false><<<g1, SEG_NT, sb, st>>>(b, p, sg);
+        solve_binned_hub_kernel<false><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
+      }
     } else if (hub) {
       if (w) solve_binned_hub_kernel<true><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
       else solve_binned_hub_kernel<false><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
@@ -1216,18 +1541,40 @@ static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opt
   using namespace mg;
   const bool weighted = o.weighted != 0;
   const int32_t limit = hub_cache_limit(g);
+  struct Cand {
+    int variant;
+    int32_t cap, T, S;
+  };
+  std::vector<Cand> cands;
   std::vector<int32_t> caps;
   for (int32_t c : {20480, 32768, PRB_HUB_CAP})
     if (c > 0 && c <= limit && std::find(caps.begin(), caps.end(), c) == caps.end()) caps.push_back(c);
-  caps.push_back(0);  // no cache
+  cands.push_back({0, 0, 0, 0});  // no cache
+  cands.push_back({1, 0, 0, 0});  // merge-path tiles staged by TMA bulk copies
+  for (int32_t c : caps) cands.push_back({2, c, 0, 0});
+  // segmented: hub thresholds, and block widths up to the shared memory a CTA can take
+  const int32_t sdef = seg_block_default(g);
+  std::vector<int32_t> widths{sdef};
+  const int32_t swide = std::min<int32_t>(limit & ~1023, 57344);
+  if (swide > sdef) widths.push_back(swide);
+  if (g->n > 0 && (g->n + sdef - 1) / sdef <= SEG_MAXB)
+    for (int32_t T : {512, 1024, 2048})
+      for (int32_t S : widths) cands.push_back({3, hub_cache_capacity(g), T, S});
   float best = 0.f;
-  int32_t best_cap = 0;
-  for (size_t i = 0; i < caps.size(); i++) {
-    const int32_t c = caps[i];
+  size_t best_i = 0;
+  for (size_t i = 0; i < cands.size(); i++) {
+    const Cand &cd = cands[i];
     float ms = 0.f;
-    for (int rep = 0; rep < 2; rep++) {
+    bool skip = false;
+    for (int rep = 0; rep < 2 && !skip; rep++) {
       SolvePlan sp;
-      MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, c > 0 ? 2 : 0, sp, c > 0 ? c : -1));
+      const mg_status st =
+          solve_setup(g, false, weighted, tele_dev, nullptr, cd.variant, sp, cd.cap > 0 ? cd.cap : -1, cd.T, cd.S);
+      if (st == MG_ERR_UNSUPPORTED) {  // a shape this graph cannot take
+        skip = true;
+        break;
+      }
+      MG_TRY(st);
       SolveArgs &a = sp.a;
       a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
       a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -1240,12 +1587,20 @@ static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opt
       MG_CUDA_TRY(cudaEventSynchronize(g->ev1));
       MG_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
     }
+    if (skip) continue;
     if (i == 0 || ms < best) {
       best = ms;
-      best_cap = c;
+      best_i = i;
     }
   }
-  plans_of(g)->tuned_cap = best_cap;
+  PlanSet *ps = plans_of(g);
+  const Cand &b = cands[best_i];
+  ps->tuned_variant = b.variant;
+  ps->tuned_cap = b.cap;
+  ps->tuned_seg_T = b.variant == 3 ? b.T : 0;
+  ps->tuned_seg_S = b.variant == 3 ? b.S : 0;
+  // keep only the kept variant's segmented plan
+  if (b.variant != 3) seg_plan_release(g, ps->seg);
   return MG_OK;
 }
 
@@ -1262,15 +1617,21 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     return MG_ERR_ARG;
   }
   PlanSet *ps = plans_of(g);
-  if (o.gather_kernel == 0 && o.autotune && ps->tuned_cap < 0) MG_TRY(pr_autotune(g, tele_dev, o));
+  if (o.gather_kernel == 0 && o.autotune && ps->tuned_variant < 0) MG_TRY(pr_autotune(g, tele_dev, o));
   int variant = o.gather_kernel;
-  int32_t cap = -1;
-  if (variant == 0 && ps->tuned_cap > 0) {  // the autotuner chose a column cache
-    variant = 2;
-    cap = ps->tuned_cap;
+  int32_t cap = -1, segT = 0, segS = 0;
+  if (variant == 0 && ps->tuned_variant > 0) {  // the autotuner's pick
+    variant = ps->tuned_variant;
+    cap = ps->tuned_cap > 0 ? ps->tuned_cap : -1;
+    segT = ps->tuned_seg_T;
+    segS = ps->tuned_seg_S;
+  }
+  if (variant == 3) {  // explicit segmented shape
+    if (o.seg_hub_edges > 0) segT = o.seg_hub_edges;
+    if (o.seg_block_cols > 0) segS = o.seg_block_cols;
   }
   SolvePlan sp;
-  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, variant, sp, cap));
+  MG_TRY(solve_setup(g, false, weighted, tele_dev, nullptr, variant, sp, cap, segT, segS));
   SolveArgs &a = sp.a;
   a.tn = g->n > 0 ? 1.0 / (double)g->n : 0.0;
   a.alpha = o.alpha > 0 ? o.alpha : 0.85;
@@ -1300,9 +1661,10 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     stats->kernel_ms = ms;
     // fill + row sums + init + init reduce, then per iteration the gather (merge-path:
     // gather + fix-up), plus the loop guard when the loop runs as a graph
-    const int64_t per_it = o.gather_kernel == 1 ? 2 : 1;
-    stats->status_detail = sp.use_hub ? (int32_t)(sp.hub_bytes / sizeof(float)) : 0;
-    stats->launches = 4 + (sp.use_hub ? 1 : 0) + (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
+    const int64_t per_it = (variant == 1 || sp.use_seg) ? 2 : 1;
+    stats->status_detail = (sp.use_hub || sp.use_seg) ? sp.a.nhub : 0;
+    stats->launches = 4 + ((sp.use_hub || sp.use_seg) ? 1 : 0) +
+                      (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
   }
   return MG_OK;
 }
@@ -1532,6 +1894,14 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
   }
   if (o.alpha < 0 || o.alpha >= 1) {
     mg_set_error("mg_pagerank: alpha must be in [0, 1)");
+    return MG_ERR_ARG;
+  }
+  if (o.gather_kernel < 0 || o.gather_kernel > 3) {
+    mg_set_error("mg_pagerank: gather_kernel must be 0..3");
+    return MG_ERR_ARG;
+  }
+  if (o.seg_hub_edges < 0 || o.seg_block_cols < 0 || o.seg_block_cols % 32 != 0) {
+    mg_set_error("mg_pagerank: seg_hub_edges must be >= 0 and seg_block_cols a multiple of 32");
     return MG_ERR_ARG;
   }
   MG_TRY(graph_enter(g));
@@ -1778,5 +2148,94 @@ extern "C" mg_status mg_pagerank_backward(mg_graph *g, const float *teleport, co
     mg_set_error("mg_pagerank_backward: device status %d", hc.status);
     return (mg_status)hc.status;
   }
+  return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Test hook: host-side check of a segmented gather plan (mg_debug_seg_plan).
+extern "C" mg_status mg_debug_seg_plan(mg_graph *g, int32_t hub_edges, int32_t block_cols, int64_t *out) {
+  using namespace mg;
+  if (!g || !out || hub_edges <= 0 || block_cols <= 0 || block_cols % 32 != 0) {
+    mg_set_error("mg_debug_seg_plan: bad argument");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  HubCache *hubs = nullptr;
+  MG_TRY(get_hub_cache(g, hub_cache_capacity(g), &hubs));
+  SegPlan *sp = nullptr;
+  const bool weighted = plans_of(g)->seg.ok ? plans_of(g)->seg.weighted : false;
+  MG_TRY(get_seg_plan(g, hub_edges, block_cols, weighted, *hubs, &sp));
+  cudaStream_t s = g->stream;
+  const int64_t nh = sp->bins.nheavy, ng = sp->ngroups, m = g->m;
+  auto d2h = [&](void *dst, const void *src, size_t bytes) -> mg_status {
+    if (bytes) MG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    return MG_OK;
+  };
+  std::vector<int32_t> hrows(nh), hbase(nh + 1), hcount(nh), co(g->n + 1), ri(m), bgrp(sp->nblocks + 1),
+      cta(sp->grid + 1), pidx(sp->nell);
+  std::vector<int2> ent((size_t)ng * 32);
+  std::vector<int64_t> gofs(ng + 1);
+  MG_TRY(d2h(hrows.data(), sp->bins.hrows, 4 * nh));
+  MG_TRY(d2h(hbase.data(), sp->bins.hbase, 4 * (nh + 1)));
+  MG_TRY(d2h(hcount.data(), sp->bins.hcount, 4 * nh));
+  MG_TRY(d2h(co.data(), g->co, 4 * (g->n + 1)));
+  MG_TRY(d2h(ri.data(), g->ri, 4 * m));
+  MG_TRY(d2h(bgrp.data(), sp->bgrp, 4 * bgrp.size()));
+  MG_TRY(d2h(cta.data(), sp->cta, 4 * cta.size()));
+  MG_TRY(d2h(pidx.data(), sp->pidx, 4 * pidx.size()));
+  MG_TRY(d2h(ent.data(), sp->ent, sizeof(int2) * ent.size()));
+  MG_TRY(d2h(gofs.data(), sp->gofs, 8 * gofs.size()));
+  MG_CUDA_TRY(cudaStreamSynchronize(s));
+  const int64_t nfrag = nh ? hbase[nh] : 0;
+  std::vector<int32_t> seen(nfrag, 0);
+  // per fragment: its block and the multiset of its (permuted) columns
+  std::vector<std::vector<int32_t>> fcols(nfrag);
+  std::vector<int32_t> fblock(nfrag, -1), fhub(nfrag, -1);
+  for (int64_t b = 0; b < sp->nblocks; b++)
+    for (int64_t gi = bgrp[b]; gi < bgrp[b + 1]; gi++)
+      for (int l = 0; l < 32; l++) {
+        const int2 e = ent[gi * 32 + l];
+        if (e.x < 0) continue;
+        if (e.x >= nfrag) continue;
+        seen[e.x]++;
+        fblock[e.x] = (int32_t)b;
+        fhub[e.x] = e.y;
+        const int64_t depth = (gofs[gi + 1] - gofs[gi]) / 32;
+        for (int64_t i = 0; i < depth; i++) {
+          const int32_t c = pidx[gofs[gi] + 32 * i + l];
+          if (c >= 0) fcols[e.x].push_back(c);
+        }
+      }
+  int64_t once = 0, match = 0;
+  for (int64_t f = 0; f < nfrag; f++) once += seen[f] == 1;
+  // expected: per hub, its edges of each block (permuted), split at SEG_FMAX, in block order
+  for (int64_t h = 0; h < nh; h++) {
+    const int32_t r = hrows[h];
+    std::vector<std::vector<int32_t>> byb(sp->nblocks);
+    for (int32_t k = co[r]; k < co[r + 1]; k++) byb[ri[k] / sp->S].push_back(seg_swz(ri[k]));
+    int64_t f = hbase[h];
+    for (int64_t b = 0; b < sp->nblocks; b++) {
+      for (size_t q = 0; q < byb[b].size(); q += SEG_FMAX, f++) {
+        if (f >= hbase[h + 1]) break;
+        std::vector<int32_t> want(byb[b].begin() + q, byb[b].begin() + std::min(byb[b].size(), q + SEG_FMAX));
+        std::vector<int32_t> got = fcols[f];
+        std::sort(want.begin(), want.end());
+        std::sort(got.begin(), got.end());
+        match += (got == want && fblock[f] == b && fhub[f] == h) ? 1 : 0;
+      }
+    }
+  }
+  int64_t nonzero = 0;
+  for (int32_t c : hcount) nonzero += c != 0;
+  bool cover = cta[0] == 0 && cta[sp->grid] == ng;
+  for (int i = 0; i < sp->grid; i++) cover = cover && cta[i] <= cta[i + 1];
+  out[0] = nh;
+  out[1] = nfrag;
+  out[2] = ng;
+  out[3] = sp->nell;
+  out[4] = once;
+  out[5] = match;
+  out[6] = nonzero;
+  out[7] = cover ? 1 : 0;
   return MG_OK;
 }

@@ -89,20 +89,23 @@ struct BinPlan {
 
 }  // namespace mg
 
-// Host side (pagerank.cu): builds / releases a plan over `off` (n + 1 entries).
-mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp);
+// Host side (pagerank.cu): builds / releases a plan over `off` (n + 1 entries);
+// rows of at least `heavy` edges become hubs.
+mg_status bin_plan_build(cudaStream_t s, const int32_t *off, int64_t n, mg::BinPlan &bp,
+                         int32_t heavy = mg::PRB_HEAVY);
 void bin_plan_release(cudaStream_t s, mg::BinPlan &bp);
 
 namespace mg {
 
-__device__ __forceinline__ int prb_bin_of(int32_t deg) {
+// Bin of a row of `deg` edges; rows of at least `heavy` edges are hubs (bin 6).
+__device__ __forceinline__ int prb_bin_of(int32_t deg, int32_t heavy = PRB_HEAVY) {
+  if (deg >= heavy) return 6;
   if (deg <= 1) return 0;
   if (deg <= 2) return 1;
   if (deg <= 4) return 2;
   if (deg <= 8) return 3;
   if (deg <= 16) return 4;
-  if (deg < PRB_HEAVY) return 5;
-  return 6;
+  return 5;
 }
 
 // Ordered binning. Rows are cut into chunks of PRB_NT * PRB_RPT rows, one per
@@ -115,7 +118,8 @@ constexpr int PRB_CHUNK_ROWS = PRB_NT * PRB_RPT;
 
 #ifndef MG_PRB_NO_PLAN_KERNELS  // plan building runs in pagerank.cu only
 __global__ void __launch_bounds__(PRB_NT) prb_count_kernel(const int32_t *__restrict__ off, int64_t n,
-                                                           int64_t *__restrict__ counts /* [chunk][BINS+1] */) {
+                                                           int64_t *__restrict__ counts /* [chunk][BINS+1] */,
+                                                           int32_t heavy) {
   __shared__ int64_t s[PRB_BINS + 1];
   if (threadIdx.x <= PRB_BINS) s[threadIdx.x] = 0;
   __syncthreads();
@@ -124,7 +128,7 @@ __global__ void __launch_bounds__(PRB_NT) prb_count_kernel(const int32_t *__rest
     const int64_t r = base + (int64_t)threadIdx.x * PRB_RPT + k;
     if (r < n) {
       const int32_t d = off[r + 1] - off[r];
-      const int b = prb_bin_of(d);
+      const int b = prb_bin_of(d, heavy);
       atomicAdd((unsigned long long *)&s[b], 1ull);
       if (b == 6) atomicAdd((unsigned long long *)&s[PRB_BINS], (unsigned long long)((d + PRB_CHUNK - 1) / PRB_CHUNK));
     }
@@ -149,14 +153,14 @@ __global__ void prb_offsets_kernel(int64_t *counts, int64_t nchunks, int64_t *to
 __global__ void __launch_bounds__(PRB_NT) prb_scatter_kernel(const int32_t *__restrict__ off, int64_t n,
                                                              const int64_t *__restrict__ offsets,
                                                              const int64_t *__restrict__ boff, int32_t *rows,
-                                                             int32_t *hrows) {
+                                                             int32_t *hrows, int32_t heavy) {
   __shared__ int32_t red[PRB_NT / 32 + 1];
   const int64_t base = (int64_t)blockIdx.x * PRB_CHUNK_ROWS;
   int bins[PRB_RPT];
 #pragma unroll
   for (int k = 0; k < PRB_RPT; k++) {
     const int64_t r = base + (int64_t)threadIdx.x * PRB_RPT + k;
-    bins[k] = r < n ? prb_bin_of(off[r + 1] - off[r]) : -1;
+    bins[k] = r < n ? prb_bin_of(off[r + 1] - off[r], heavy) : -1;
   }
   for (int b = 0; b < PRB_BINS; b++) {
     int cnt = 0;
@@ -213,6 +217,10 @@ struct PrbArgs {
   int64_t boff[PRB_BINS + 1];
   int64_t wstart[PRB_BINS + 1];
   int64_t nheavy;
+  // 1: the hub rows are not work items of this plan; a previous kernel left each
+  // hub's fragment sums in hpart[hbase[h] .. hbase[h + 1]) (the segmented gather)
+  // and the solve kernel finishes those rows itself.
+  int32_t hubs_summed;
 };
 
 template <bool WEIGHTED>
@@ -300,14 +308,12 @@ __device__ __forceinline__ Comp prb_warp_range(const PrbArgs &p, int32_t b, int3
 // waits for three memory round trips per assignment rather than three per pass.
 // The sum of slot l ends up in lane l, whose row is returned in *my_row (-1 past
 // the bin), so the row updates then run on all lanes at once.
+// prb_ranges32 is the same for 32 edge ranges [mb, me) given per lane (at most G
+// edges each for G < 32): the sum of lane l's range ends up in lane l.
 template <int G, bool WEIGHTED, bool ADAPT, typename Gather>
-__device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa, Gather &gather, int32_t *my_row) {
+__device__ __forceinline__ Comp prb_ranges32(const PrbArgs &p, int32_t mb, int32_t me, Gather &gather) {
   constexpr int RPP = 32 / G;  // rows per pass
   const int lane = threadIdx.x & 31;
-  const int64_t slot = p.boff[bin] + wa * 32 + lane;
-  const int32_t mine_row = slot < p.boff[bin + 1] ? p.rows[slot] : -1;
-  const int32_t mb = mine_row >= 0 ? __ldg(p.off + mine_row) : 0;
-  const int32_t me = mine_row >= 0 ? __ldg(p.off + mine_row + 1) : 0;
   const int gl = lane % G, grp = lane / G;
   Comp mine{0.f, 0.f};
   if (G == 32) {
@@ -346,8 +352,18 @@ __device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa
       }
     }
   }
-  *my_row = mine_row;
   return mine;
+}
+
+template <int G, bool WEIGHTED, bool ADAPT, typename Gather>
+__device__ __forceinline__ Comp prb_rows32(const PrbArgs &p, int bin, int64_t wa, Gather &gather, int32_t *my_row) {
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = p.boff[bin] + wa * 32 + lane;
+  const int32_t mine_row = slot < p.boff[bin + 1] ? p.rows[slot] : -1;
+  const int32_t mb = mine_row >= 0 ? __ldg(p.off + mine_row) : 0;
+  const int32_t me = mine_row >= 0 ? __ldg(p.off + mine_row + 1) : 0;
+  *my_row = mine_row;
+  return prb_ranges32<G, WEIGHTED, ADAPT>(p, mb, me, gather);
 }
 
 // Walks every assignment of the plan with a persistent grid (fixed stride).

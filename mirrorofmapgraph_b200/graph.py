@@ -288,11 +288,13 @@ class Graph:
     @staticmethod
     def _pr_opts(mode="refcompat", directed=1, max_iter=0, weighted=False, alpha=0.85, tol=None,
                  compensated=True, device_output=False, use_graph=True, gather="binned",
-                 autotune=False, group_width=0) -> L.MgPrOpts:
+                 autotune=False, group_width=0, seg_hub_edges=0, seg_block_cols=0) -> L.MgPrOpts:
         o = L.MgPrOpts()
+        o.seg_hub_edges = int(seg_hub_edges)
+        o.seg_block_cols = int(seg_block_cols)
         o.autotune = 1 if autotune else 0
         o.group_width = int(group_width)
-        o.gather_kernel = {"binned": 0, "tma": 1, "cached": 2}[gather]
+        o.gather_kernel = {"binned": 0, "tma": 1, "cached": 2, "segmented": 3}[gather]
         o.mode = {"refcompat": L.MG_PR_REFCOMPAT, "normalized": L.MG_PR_NORMALIZED}[mode]
         o.directed = int(directed)
         o.max_iter = int(max_iter)
@@ -308,7 +310,7 @@ class Graph:
         """struct pagerank (refcompat) or the normalised / personalised power iteration.
 
         Keywords (mg_pr_opts): mode "refcompat" | "normalized", alpha, tol, max_iter,
-        weighted, directed (refcompat), gather "binned" | "cached" | "tma",
+        weighted, directed (refcompat), gather "binned" | "cached" | "tma" | "segmented",
         autotune (time the gathers, or with nvec > 1 the group width, once per
         graph), group_width (nvec > 1: vectors per pass, a multiple of 32 <= 256),
         compensated, use_graph. Returns (ranks, stats); with nvec > 1 the ranks are

@@ -159,7 +159,7 @@ def test_api_pagerank_program(mtx_fixtures):
     assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < cfg.getParameter("tol")
 
 
-@pytest.mark.parametrize("gather", ["binned", "tma", "cached"])
+@pytest.mark.parametrize("gather", ["binned", "tma", "cached", "segmented"])
 @pytest.mark.parametrize("weighted", [False, True])
 def test_gather_kernels_agree_with_fp64(gather, weighted):
     h = mg.gen_rmat(14, 16, 61, symmetrize=False, weights="lognormal" if weighted else None, p0=0, p1=1)
@@ -181,7 +181,7 @@ def test_gather_hub_chunks_binned():
     ro = np.zeros(n + 1, dtype=np.int64)
     np.add.at(ro, src[order] + 1, 1)
     h = mg.HostCsr(np.cumsum(ro).astype(np.int32), dst[order].astype(np.int32))
-    for gather in ("binned", "tma", "cached"):
+    for gather in ("binned", "tma", "cached", "segmented"):
         with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
             x, st = g.pagerank(mode="normalized", gather=gather)
         xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
@@ -218,3 +218,54 @@ def test_gather_autotune_picks_and_keeps_a_variant():
         assert st2["status_detail"] == choice and np.abs(x - x2).sum() <= 1e-9
         xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
         assert np.abs(x - xr).sum() <= L1_TOL
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("sym", [True, False])
+@pytest.mark.parametrize("hub_edges,block_cols", [(64, 4096), (16, 1024), (300, 8192), (1024, 40960)])
+def test_segmented_gather_shapes(weighted, sym, hub_edges, block_cols):
+    """The segmented gather over many column blocks: hub rows cut into fragments of
+    every length class (and split at 1024 edges), phase 1 spread over the CTAs,
+    the other rows through the column cache. Against the FP64 oracle at the same
+    iteration count, and against the binned gather to rounding."""
+    h = mg.gen_rmat(16, 16, 77, symmetrize=sym, weights="lognormal" if weighted else None, p0=0, p1=1)
+    w = h.weights_f32 if weighted else None
+    with mg.Graph(h.row_offsets, h.col_idx, w, symmetric=sym) as g:
+        kw = dict(mode="normalized", weighted=weighted, gather="segmented", seg_hub_edges=hub_edges,
+                  seg_block_cols=block_cols)
+        x, st = g.pagerank(**kw)
+        xh, sth = g.pagerank(use_graph=False, **kw)
+        xb, stb = g.pagerank(mode="normalized", weighted=weighted, gather="binned")
+    assert st["iterations"] == sth["iterations"] == stb["iterations"]
+    assert np.abs(x - xh).sum() <= 1e-9
+    xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, w, 0.85, 0.0, st["iterations"])
+    assert np.abs(x - xr).sum() <= L1_TOL
+    assert np.abs(x - xb).sum() <= L1_TOL
+
+
+def test_segmented_gather_unsorted_rows_and_isolated_vertices():
+    """Rows whose in-edges are not sorted by source (a symmetric CSR is gathered as
+    given) still form one fragment per (row, block): the plan regroups each hub
+    row's edges by block. Vertices without edges and a last block shorter than
+    the rest are covered too."""
+    rng = np.random.default_rng(5)
+    h = mg.gen_rmat(15, 16, 13, symmetrize=True)
+    ro, ci = h.row_offsets.copy(), h.col_idx.copy()
+    for r in range(len(ro) - 1):  # shuffle every row
+        rng.shuffle(ci[ro[r]:ro[r + 1]])
+    with mg.Graph(ro, ci, symmetric=True) as g:
+        x, st = g.pagerank(mode="normalized", gather="segmented", seg_hub_edges=32, seg_block_cols=3072)
+    xr, _, _ = oracle.pr_normalized(ro, ci, None, 0.85, 0.0, st["iterations"])
+    assert np.abs(x - xr).sum() <= L1_TOL
+
+
+def test_segmented_gather_rejects_bad_shapes():
+    h = mg.gen_rmat(12, 16, 3, symmetrize=True)
+    with mg.Graph(h.row_offsets, h.col_idx, symmetric=True) as g:
+        with pytest.raises(mg.MapGraphError):
+            g.pagerank(mode="normalized", gather="segmented", seg_block_cols=100)
+        with pytest.raises(mg.MapGraphError):  # wider than a CTA's shared memory
+            g.pagerank(mode="normalized", gather="segmented", seg_block_cols=1 << 20)
+        x, st = g.pagerank(mode="normalized", gather="segmented")  # the graph is still usable
+    xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, 0.85, 0.0, st["iterations"])
+    assert np.abs(x - xr).sum() <= L1_TOL
