@@ -114,13 +114,14 @@ typedef struct mg_pr_opts {
   int32_t use_graph;     /* as mg_opts.use_graph */
   int32_t gather_kernel; /* NORMALIZED/adjoint gather: 0 degree-binned warps [default]; 1 merge-path tiles
                             staged in shared memory by TMA bulk copies; 2 degree-binned with the most-gathered
-                            columns cached in shared memory; 3 segmented: rows of >= 1024 edges gathered one
+                            columns cached in shared memory; 3 segmented: rows of >= 512 edges gathered one
                             column block at a time from shared-memory copies of the block (TMA bulk copies),
-                            the other rows as 2 (2 and 3 are forward solves; the adjoint uses 0) */
+                            the other rows one lane per row with the column cache of 2 (2 and 3 are forward
+                            solves; the adjoint uses 0) */
   int32_t autotune;      /* NORMALIZED forward with gather_kernel 0: 1 makes the first such solve on a graph
                             time the gathers (degree-binned without and with column caches of 20K, 32K and
-                            40K columns, merge-path, segmented with hub thresholds 512 / 1024 / 2048 edges
-                            and two block widths; 4 iterations each) and keep the fastest for every later
+                            40K columns, merge-path, segmented with hub thresholds 512 / 1024 / 2048 edges;
+                            4 iterations each) and keep the fastest for every later
                             solve;
                             stats->status_detail reports the column-cache size used (0 for none);
                             with nvec > 1 and group_width 0 it picks the group width instead (64, 128
@@ -128,7 +129,7 @@ typedef struct mg_pr_opts {
   int32_t group_width;   /* nvec > 1: vectors iterated together per pass, a multiple of 32 up to 256
                             [0: 256, or the autotuned width]; stats->status_detail reports it */
   int32_t seg_hub_edges; /* gather_kernel 3: rows of at least this many in-edges are gathered column block
-                            by column block [0: 1024, or the autotuned value] */
+                            by column block [0: 512, or the autotuned value] */
   int32_t seg_block_cols;/* gather_kernel 3: columns per block, a multiple of 32 whose values fit one CTA's
                             shared memory [0: the column cache's width, or the autotuned value] */
 } mg_pr_opts;

@@ -226,7 +226,6 @@ static mg::PrbArgs prb_args_of(const mg_graph *g, const mg::BinPlan &bp, bool cs
   }
   p.nheavy = bp.nheavy;
   p.grab = nullptr;
-  p.hubs_summed = 0;
   return p;
 }
 
@@ -263,6 +262,7 @@ struct SolveArgs {
   int32_t grid1, grid2;
   const int32_t *hslot;       // shared-memory column cache: slot of each vertex (nullptr: no cache)
   int32_t gswz;               // 1: x/s of vertex v lives at g[seg_swz(v)] (segmented gather)
+  const int32_t *vpos;        // position of each row's x in v0 / v1 (nullptr: the row itself)
   float *gh0, *gh1;           // cached columns' gathered values, ping-pong with g0/g1
   int32_t nhub;               // cached columns
   DevCtl *ctl;
@@ -494,24 +494,6 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
     p.hcontrib[2 * h + 1] = hu.red2;
     __threadfence();
   };
-  if (p.hubs_summed) {
-    // Hub rows of the segmented gather: one warp per hub adds its fragment sums
-    // (lane l takes sums l, l + 32, ...; then a fixed pairing tree) and lane 0
-    // applies the row update, counted in this CTA's partials.
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = (int64_t)gridDim.x * (PRB_HUB_NT / 32);
-    for (int64_t h = (int64_t)blockIdx.x * (PRB_HUB_NT / 32) + (threadIdx.x >> 5); h < p.nheavy; h += nw) {
-      const int32_t fb = p.hbase[h], nfr = p.hbase[h + 1] - fb;
-      const float2 *parts = reinterpret_cast<const float2 *>(p.hpart) + fb;
-      Comp t{0.f, 0.f};
-      for (int32_t k = lane; k < nfr; k += 32) {
-        const float2 v = parts[k];
-        comp_add(t, Comp{v.x, v.y});
-      }
-      group_comp_reduce<32>(t);
-      if (lane == 0) up(p.hrows[h], t);
-    }
-  }
   prb_run<WEIGHTED, PRB_HUB_ADAPT>(p, [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); }, up,
                     hub);
   const double r = block_sum<PRB_HUB_NT>(up.resid, s_red);
@@ -522,16 +504,16 @@ __global__ void __launch_bounds__(PRB_HUB_NT, PRB_HUB_MINB) solve_binned_hub_ker
   }
   if (last_block(&c->blocks_done)) {
     if (threadIdx.x == 0 && p.grab) *p.grab = 0;
-    solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.hubs_summed ? 0 : p.nheavy, s_red);
+    solve_iteration_end<PRB_HUB_NT>(a, cur, p.hcontrib, p.nheavy, s_red);
   }
 }
 
 // Phase 1 of a segmented iteration (pr_segment.cuh): the hub rows' fragments,
 // block by block, out of shared-memory copies of x/s; each fragment's sum goes to
-// its slot in hpart. Phase 2, solve_binned_hub_kernel launched after this kernel
-// (PrbArgs.hubs_summed), finishes the hub rows from those sums, runs the other
-// rows and ends the iteration. One CTA of SEG_NT threads per SM (the plan's ranges
-// are cut for that grid).
+// its slot in hpart. Phase 2, solve_rows_kernel launched after this kernel,
+// finishes the hub rows from those sums, runs the other rows and ends the
+// iteration. One CTA of SEG_NT threads per SM (the plan's ranges are cut for that
+// grid).
 constexpr int SEG_NT = 1024;
 
 template <bool WEIGHTED>
@@ -557,6 +539,89 @@ __global__ void __launch_bounds__(SEG_NT, 1) solve_segment_kernel(SolveArgs a, P
   if (!ok) {
     c->status = MG_ERR_TIMEOUT;
     c->done = 1;
+  }
+}
+
+// Phase 2 of a segmented iteration: the hub rows from phase 1's fragment sums (a
+// warp per hub: lanes strided over the sums, then a fixed pairing tree), then the
+// other rows from their sliced ELL (a lane per row, groups from a counter), with
+// the most-gathered columns in shared memory. The iterate and the per-row data
+// are in the solve's position order (SegPlan::ppos); the last CTA ends the
+// iteration.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(SEG_NT, 1) solve_rows_kernel(SolveArgs a, PrbArgs p, SegArgs sg) {
+  extern __shared__ __align__(16) float s_hub[];
+  __shared__ double s_red[SEG_NT / 32 + 1];
+  if (solve_skip(a)) return;
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const float *vold = cur ? a.v1 : a.v0;
+  const float *__restrict__ gold = cur ? a.g1 : a.g0;
+  const float *ghold = cur ? a.gh1 : a.gh0;
+  float *vnew = cur ? a.v0 : a.v1, *gnew = cur ? a.g0 : a.g1, *ghnew = cur ? a.gh0 : a.gh1;
+  const int32_t nh4 = a.nhub >> 2;
+  for (int32_t i = threadIdx.x; i < nh4; i += SEG_NT)
+    reinterpret_cast<float4 *>(s_hub)[i] = __ldcg(reinterpret_cast<const float4 *>(ghold) + i);
+  for (int32_t i = 4 * nh4 + threadIdx.x; i < a.nhub; i += SEG_NT) s_hub[i] = __ldcg(ghold + i);
+  __syncthreads();
+  const double scal = vload(&c->dprev[1]);
+  double resid = 0.0, red2 = 0.0;
+  // Row update at position `pos` (row r): x' = alpha (acc + d t) + (1 - alpha) t,
+  // x'/s into the gathered vector (not for dangling rows: never gathered), |dx|
+  // and dangling mass into this thread's partials.
+  auto update = [&](int64_t pos, int32_t r, Comp v) {
+    const double acc = (double)v.hi + (double)v.lo;
+    const double t = sg.pt ? (double)sg.pt[pos] : a.tn;
+    const double s = (double)sg.ps[pos];
+    const double nv = a.alpha * (acc + scal * t) + (1.0 - a.alpha) * t;
+    if (s > 0.0) {
+      const float gv = (float)(nv / s);
+      gnew[seg_swz(r)] = gv;
+      const int32_t sl = sg.pslot[pos];
+      if (sl >= 0) ghnew[sl] = gv;
+    } else {
+      red2 += nv;
+    }
+    const float nf = (float)nv;
+    resid += fabs((double)nf - (double)vold[pos]);
+    vnew[pos] = nf;
+  };
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (SEG_NT / 32);
+  const int64_t hub0 = sg.nrgroups * 32;
+  for (int64_t h = (int64_t)blockIdx.x * (SEG_NT / 32) + (threadIdx.x >> 5); h < p.nheavy; h += nw) {
+    const int32_t fb = p.hbase[h], nfr = p.hbase[h + 1] - fb;
+    const float2 *parts = reinterpret_cast<const float2 *>(p.hpart) + fb;
+    Comp t{0.f, 0.f};
+    for (int32_t k = lane; k < nfr; k += 32) {
+      const float2 v = parts[k];  // written by the previous kernel
+      comp_add(t, Comp{v.x, v.y});
+    }
+    group_comp_reduce<32>(t);
+    if (lane == 0) update(hub0 + h, p.hrows[h], t);
+  }
+  auto gather = [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); };
+  for (;;) {
+    int32_t gi = 0;
+    if (lane == 0) gi = atomicAdd(sg.rgrab, 1);
+    gi = __shfl_sync(FULL, gi, 0);
+    if (gi >= sg.nrgroups) break;
+    const int32_t r = sg.rrow[(int64_t)gi * 32 + lane];
+    const int64_t s0 = sg.rgofs[gi];
+    const int32_t depth = (int32_t)((sg.rgofs[gi + 1] - s0) >> 5);
+    const Comp acc = sell_walk<WEIGHTED, WEIGHTED ? 4 : SEG_U>(sg.ridx + s0 + lane,
+                                                              WEIGHTED ? sg.rwts + s0 + lane : nullptr, depth, gather);
+    if (r >= 0) update((int64_t)gi * 32 + lane, r, acc);
+  }
+  const double rr = block_sum<SEG_NT>(resid, s_red);
+  const double d = block_sum<SEG_NT>(red2, s_red);
+  if (threadIdx.x == 0) {
+    a.part1[2 * blockIdx.x] = rr;
+    a.part1[2 * blockIdx.x + 1] = d;
+  }
+  if (last_block(&c->blocks_done)) {
+    if (threadIdx.x == 0) *sg.rgrab = 0;
+    solve_iteration_end<SEG_NT>(a, cur, nullptr, 0, s_red);
   }
 }
 
@@ -654,7 +719,7 @@ __global__ void __launch_bounds__(256) solve_init_kernel(SolveArgs a) {
     const double t = tele_of(a, i);
     if (!a.adjoint) {
       const double s = (double)a.srow[i];
-      a.v0[i] = (float)t;
+      a.v0[a.vpos ? a.vpos[i] : i] = (float)t;
       const int64_t gi = a.gswz ? seg_swz((int32_t)i) : i;
       if (s > 0.0) a.g0[gi] = (float)(t / s);
       else {
@@ -693,6 +758,28 @@ __global__ void __launch_bounds__(256) solve_init_reduce_kernel(SolveArgs a, int
     c->iter_cap = a.max_iter;
     c->done = a.max_iter <= 0 ? 1 : 0;
   }
+}
+
+// Row sums and teleport entries of a segmented solve in its position order.
+__global__ void seg_pos_rows_kernel(SolveArgs a, const int32_t *__restrict__ prow, int64_t npos, float *ps,
+                                    float *pt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npos; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t r = prow[i];
+    float sv = 0.f, tv = 0.f;
+    if (r >= 0) {
+      sv = a.soff ? (float)(a.off[r + 1] - a.off[r]) : a.srow[r];
+      if (pt) tv = a.tele[r];
+    }
+    ps[i] = sv;
+    if (pt) pt[i] = tv;
+  }
+}
+
+// x in row order from a segmented solve's position order.
+__global__ void seg_unpermute_kernel(const float *__restrict__ v, const int32_t *__restrict__ ppos, int64_t n,
+                                     float *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = v[ppos[i]];
 }
 
 // Row sums s_u of the CSR (outdeg unweighted; sum of weights otherwise, through
@@ -755,6 +842,7 @@ struct SolvePlan {
   bool use_seg;         // segmented hub rows + column cache for the rest
   int32_t hub_bytes;    // dynamic shared memory of the column-cache kernel
   int32_t seg_bytes;    // dynamic shared memory of the segmented gather's phase 1 (a column block)
+  const int32_t *ppos = nullptr;  // segmented: position of each row's x in v0 / v1
 };
 
 template <bool W>
@@ -837,7 +925,9 @@ static mg_status get_hub_cache(mg_graph *g, int32_t cap, mg::HubCache **out) {
 static void seg_plan_release(mg_graph *g, mg::SegPlan &sp) {
   bin_plan_release(g->stream, sp.bins);
   for (void *q : {(void *)sp.sidx, (void *)sp.swts, (void *)sp.ent, (void *)sp.gofs, (void *)sp.pidx,
-                  (void *)sp.pwts, (void *)sp.bgrp, (void *)sp.bdense, (void *)sp.cta})
+                  (void *)sp.pwts, (void *)sp.bgrp, (void *)sp.bdense, (void *)sp.cta, (void *)sp.rrow,
+                  (void *)sp.rgofs, (void *)sp.ridx, (void *)sp.rwts, (void *)sp.rgrab, (void *)sp.ppos,
+                  (void *)sp.prow, (void *)sp.pslot})
     dev_free(g, q);
   sp = mg::SegPlan();
 }
@@ -961,6 +1051,69 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
     seg_sell_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.ent, fsrc, flen, sp.gofs, grp, sp.sidx, sp.swts, sp.pidx,
                                                    sp.pwts);
   MG_CUDA_TRY(cudaGetLastError());
+  // Phase 2's rows (in-degree below T) as sliced ELL, longest first: a counting
+  // sort by degree on the host (rows of one degree in id order). Then the iterate
+  // positions: phase 2's lanes, then the hubs.
+  {
+    std::vector<int32_t> co((size_t)n + 1);
+    MG_CUDA_TRY(cudaMemcpyAsync(co.data(), g->co, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> hrows((size_t)std::max<int64_t>(nh, 1));
+    if (nh > 0)
+      MG_CUDA_TRY(cudaMemcpyAsync(hrows.data(), sp.bins.hrows, sizeof(int32_t) * (size_t)nh, cudaMemcpyDeviceToHost,
+                                  s));
+    MG_CUDA_TRY(cudaStreamSynchronize(s));
+    int32_t dmax = 0;
+    for (int64_t r = 0; r < n; r++) {
+      const int32_t d = co[r + 1] - co[r];
+      if (d < T) dmax = std::max(dmax, d);
+    }
+    std::vector<int64_t> start((size_t)dmax + 2, 0);
+    for (int64_t r = 0; r < n; r++) {
+      const int32_t d = co[r + 1] - co[r];
+      if (d < T) start[dmax - d + 1]++;
+    }
+    for (size_t k = 1; k < start.size(); k++) start[k] += start[k - 1];
+    const int64_t nrows = start.back();
+    sp.nrgroups = (nrows + 31) / 32;
+    std::vector<int32_t> rrow((size_t)std::max<int64_t>(sp.nrgroups * 32, 1), -1);
+    for (int64_t r = 0; r < n; r++) {
+      const int32_t d = co[r + 1] - co[r];
+      if (d < T) rrow[start[dmax - d]++] = (int32_t)r;
+    }
+    std::vector<int64_t> rg((size_t)sp.nrgroups + 1, 0);
+    for (int64_t gi = 0; gi < sp.nrgroups; gi++) {
+      const int32_t r0 = rrow[gi * 32];  // the group's longest row
+      rg[gi + 1] = rg[gi] + 32 * (int64_t)(co[r0 + 1] - co[r0]);
+    }
+    sp.nrell = rg[sp.nrgroups];
+    sp.npos = sp.nrgroups * 32 + nh;
+    std::vector<int32_t> prow((size_t)std::max<int64_t>(sp.npos, 1), -1), ppos((size_t)std::max<int64_t>(n, 1), -1);
+    for (int64_t i = 0; i < sp.nrgroups * 32; i++) prow[i] = rrow[i];
+    for (int64_t h = 0; h < nh; h++) prow[sp.nrgroups * 32 + h] = hrows[h];
+    for (int64_t i = 0; i < sp.npos; i++)
+      if (prow[i] >= 0) ppos[prow[i]] = (int32_t)i;
+    MG_TRY(dev_alloc(g, (void **)&sp.rrow, sizeof(int32_t) * rrow.size()));
+    MG_TRY(dev_alloc(g, (void **)&sp.rgofs, sizeof(int64_t) * rg.size()));
+    MG_TRY(dev_alloc(g, (void **)&sp.ridx, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nrell, 1)));
+    if (weighted) MG_TRY(dev_alloc(g, (void **)&sp.rwts, sizeof(float) * (size_t)std::max<int64_t>(sp.nrell, 1)));
+    MG_TRY(dev_alloc(g, (void **)&sp.rgrab, sizeof(int32_t)));
+    MG_TRY(dev_alloc(g, (void **)&sp.ppos, sizeof(int32_t) * ppos.size()));
+    MG_TRY(dev_alloc(g, (void **)&sp.prow, sizeof(int32_t) * prow.size()));
+    MG_TRY(dev_alloc(g, (void **)&sp.pslot, sizeof(int32_t) * prow.size()));
+    MG_CUDA_TRY(cudaMemsetAsync(sp.rgrab, 0, sizeof(int32_t), s));
+    MG_CUDA_TRY(cudaMemsetAsync(sp.ridx, 0xff, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nrell, 1), s));
+    if (weighted) MG_CUDA_TRY(cudaMemsetAsync(sp.rwts, 0, sizeof(float) * (size_t)std::max<int64_t>(sp.nrell, 1), s));
+    MG_CUDA_TRY(cudaMemcpyAsync(sp.rrow, rrow.data(), sizeof(int32_t) * rrow.size(), cudaMemcpyHostToDevice, s));
+    MG_CUDA_TRY(cudaMemcpyAsync(sp.rgofs, rg.data(), sizeof(int64_t) * rg.size(), cudaMemcpyHostToDevice, s));
+    MG_CUDA_TRY(cudaMemcpyAsync(sp.ppos, ppos.data(), sizeof(int32_t) * ppos.size(), cudaMemcpyHostToDevice, s));
+    MG_CUDA_TRY(cudaMemcpyAsync(sp.prow, prow.data(), sizeof(int32_t) * prow.size(), cudaMemcpyHostToDevice, s));
+    if (sp.nrgroups > 0)
+      seg_rows_fill_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.rrow, sp.rgofs, sp.nrgroups, g->co, sp.sidx, sp.swts,
+                                                          sp.ridx, sp.rwts);
+    if (sp.npos > 0) seg_pos_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(sp.prow, sp.npos, hc.slot, sp.pslot);
+    MG_CUDA_TRY(cudaGetLastError());
+    MG_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  }
   // Dense blocks are staged in shared memory; phase 1's groups are cut into one
   // contiguous range per CTA by estimated cost: sliced-ELL entries (a global
   // gather counting SEG_GLOBAL_FACTOR), a fixed cost per group, and a block load
@@ -1040,10 +1193,10 @@ static int32_t hub_cache_limit(mg_graph *g) {
 
 static int32_t hub_cache_capacity(mg_graph *g) { return std::min(PRB_HUB_CAP, hub_cache_limit(g)); }
 
-// Default shape of the segmented gather: hub rows of at least 1024 edges, column
+// Default shape of the segmented gather: hub rows of at least 512 edges, column
 // blocks as wide as the column cache (the kernel then asks for the cached gather's
 // shared memory, leaving L1 the same room for phase 2's uncached gathers).
-constexpr int32_t SEG_DEFAULT_T = 1024;
+constexpr int32_t SEG_DEFAULT_T = 512;
 static int32_t seg_block_default(mg_graph *g) { return std::max<int32_t>(1024, hub_cache_capacity(g) & ~1023); }
 
 // Carves the solver's buffers out of ws_main (every per-vertex array padded to
@@ -1070,7 +1223,9 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
   } else MG_TRY(get_bin_plan(g, adjoint, &bins));
   if (weighted) MG_TRY(get_bin_plan(g, true, &rbins));
   const int64_t n = g->n;
-  const size_t np = (size_t)((n + 31) & ~(int64_t)31) + 8;  // whole 32-entry chunks (seg_swz) and a pad
+  // whole 32-entry chunks (seg_swz) and a pad; a segmented solve keeps x in its
+  // position order (phase 2's lanes, then the hubs)
+  const size_t np = (size_t)std::max<int64_t>((n + 31) & ~(int64_t)31, seg ? seg->npos : 0) + 8;
   const int32_t nt = plan ? plan->ntiles : 1;
   const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
   SolveArgs &a = sp.a;
@@ -1096,9 +1251,20 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
                    sp.seg_bytes);
       return MG_ERR_UNSUPPORTED;
     }
-    // phase 1's ranges are cut for one CTA per SM; phase 2 (the column-cache
-    // kernel) runs one CTA per SM as well
-    occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
+    // phase 1's ranges are cut for one CTA per SM; phase 2 runs one CTA per SM too
+    int occ2 = 0;
+    if (weighted) {
+      cudaFuncSetAttribute(solve_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp.hub_bytes);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, solve_rows_kernel<true>, SEG_NT, sp.hub_bytes);
+    } else {
+      cudaFuncSetAttribute(solve_rows_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp.hub_bytes);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, solve_rows_kernel<false>, SEG_NT, sp.hub_bytes);
+    }
+    cudaGetLastError();
+    if (occ2 < 1) {
+      mg_set_error("segmented gather: the row kernel does not fit an SM with %d bytes of shared memory", sp.hub_bytes);
+      return MG_ERR_UNSUPPORTED;
+    }
     occ = 1;
   } else if (use_hub) occ = weighted ? hub_occupancy<true>(sp.hub_bytes) : hub_occupancy<false>(sp.hub_bytes);
   else occ = weighted ? binned_occupancy<true>() : binned_occupancy<false>();
@@ -1112,7 +1278,9 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
                                    sizeof(Comp) * (size_t)nt, sizeof(Comp) * (size_t)nt,
                                    sizeof(double) * 2 * (size_t)gp, sizeof(double) * 2 * (size_t)gp,
                                    sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0),
-                                   sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0)});
+                                   sizeof(float) * (size_t)(use_hub ? hubs->K + 8 : 0),
+                                   sizeof(float) * (size_t)(use_seg ? seg->npos + 8 : 0),
+                                   sizeof(float) * (size_t)(use_seg && tele_src ? seg->npos + 8 : 0)});
   MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   a.v0 = cv.take<float>(np);
@@ -1134,6 +1302,8 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
     a.hslot = hubs->slot;
     a.nhub = hubs->K;
   }
+  float *pos_s = use_seg ? cv.take<float>((size_t)seg->npos + 8) : nullptr;
+  float *pos_t = use_seg && tele_src ? cv.take<float>((size_t)seg->npos + 8) : nullptr;
   a.n = n;
   a.srow = srow;
   a.tele = tele_src ? tele : nullptr;
@@ -1169,10 +1339,14 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
       if (weighted) sp.p.wts = seg->swts;
       sp.p.grab = bins->grab;  // phase 2 always takes items from the counter
       sp.p.wstart[PRB_BINS] = sp.p.wstart[6];  // hub rows are phase 1's, not work items of phase 2
-      sp.p.hubs_summed = 1;
-      sp.sg = SegArgs{seg->ent,  seg->gofs, seg->pidx, seg->pwts, seg->bgrp, seg->cta,
-                      seg->bdense, (n + 31) & ~(int64_t)31, seg->S, seg->nblocks};
+      sp.sg = SegArgs{seg->ent,  seg->gofs, seg->pidx,   seg->pwts,  seg->bgrp,  seg->cta,
+                      seg->bdense, (n + 31) & ~(int64_t)31, seg->S, seg->nblocks, seg->rrow, seg->rgofs,
+                      seg->ridx, seg->rwts, seg->rgrab, seg->nrgroups, seg->pslot, pos_s, pos_t};
       a.gswz = 1;
+      a.vpos = seg->ppos;
+      sp.ppos = seg->ppos;
+      if (seg->npos > 0)
+        seg_pos_rows_kernel<<<g->num_sms * 4, 256, 0, s>>>(a, seg->prow, seg->npos, pos_s, pos_t);
     } else if (use_hub) {
       sp.p.idx = hubs->cidx;
     }
@@ -1230,10 +1404,10 @@ static mg_status solve_run(mg_graph *g, SolvePlan &sp, int use_graph, int slot) 
       // phase 1 (hub fragments), then the other rows and the iteration's end
       if (w) {
         solve_segment_kernel<true><<<g1, SEG_NT, sb, st>>>(b, p, sg);
-        solve_binned_hub_kernel<true><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
+        solve_rows_kernel<true><<<g1, SEG_NT, hb, st>>>(b, p, sg);
       } else {
         solve_segment_kernel<false><<<g1, SEG_NT, sb, st>>>(b, p, sg);
-        solve_binned_hub_kernel<false><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
+        solve_rows_kernel<false><<<g1, SEG_NT, hb, st>>>(b, p, sg);
       }
     } else if (hub) {
       if (w) solve_binned_hub_kernel<true><<<g1, PRB_HUB_NT, hb, st>>>(b, p);
@@ -1552,14 +1726,11 @@ static mg_status pr_autotune(mg_graph *g, const float *tele_dev, const mg_pr_opt
   cands.push_back({0, 0, 0, 0});  // no cache
   cands.push_back({1, 0, 0, 0});  // merge-path tiles staged by TMA bulk copies
   for (int32_t c : caps) cands.push_back({2, c, 0, 0});
-  // segmented: hub thresholds, and block widths up to the shared memory a CTA can take
+  // segmented: hub thresholds (blocks as wide as the column cache; wider blocks
+  // measured slower on R-MAT s22, 389 vs 344 us per iteration at T = 512)
   const int32_t sdef = seg_block_default(g);
-  std::vector<int32_t> widths{sdef};
-  const int32_t swide = std::min<int32_t>(limit & ~1023, 57344);
-  if (swide > sdef) widths.push_back(swide);
   if (g->n > 0 && (g->n + sdef - 1) / sdef <= SEG_MAXB)
-    for (int32_t T : {512, 1024, 2048})
-      for (int32_t S : widths) cands.push_back({3, hub_cache_capacity(g), T, S});
+    for (int32_t T : {512, 1024, 2048}) cands.push_back({3, hub_cache_capacity(g), T, sdef});
   float best = 0.f;
   size_t best_i = 0;
   for (size_t i = 0; i < cands.size(); i++) {
@@ -1645,6 +1816,12 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
   MG_TRY(fetch_ctl(g));
   const DevCtl &hc = *g->ctl_host;
   const float *res = hc.cur ? a.v1 : a.v0;
+  if (sp.use_seg && g->n > 0) {  // x is in the solve's position order: back to row order
+    float *rowx = hc.cur ? a.v0 : a.v1;  // the other iterate buffer is free now
+    seg_unpermute_kernel<<<g->num_sms * 4, 256, 0, s>>>(res, sp.ppos, g->n, rowx);
+    MG_CUDA_TRY(cudaGetLastError());
+    res = rowx;
+  }
   MG_CUDA_TRY(cudaMemcpyAsync(ranks_out, res, sizeof(float) * g->n,
                               out_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   MG_CUDA_TRY(cudaStreamSynchronize(s));

@@ -217,10 +217,6 @@ struct PrbArgs {
   int64_t boff[PRB_BINS + 1];
   int64_t wstart[PRB_BINS + 1];
   int64_t nheavy;
-  // 1: the hub rows are not work items of this plan; a previous kernel left each
-  // hub's fragment sums in hpart[hbase[h] .. hbase[h + 1]) (the segmented gather)
-  // and the solve kernel finishes those rows itself.
-  int32_t hubs_summed;
 };
 
 template <bool WEIGHTED>

@@ -21,9 +21,15 @@
 //    sum goes to a fixed slot.
 //  - Phase 2, the next kernel: one warp per hub row adds the row's fragment sums
 //    in a fixed order (lanes strided, then a fixed pairing tree) and applies the
-//    row update; rows below T run through the binned gather with the
-//    shared-memory column cache (dynamic schedule); its last CTA ends the
-//    iteration. Results do not depend on scheduling.
+//    row update. Every row below T (zero-degree rows included) is laid out as
+//    sliced ELL too: rows sorted by degree, longest first, 32 to a group, a lane
+//    per row, index loads one round ahead of the gathers, so no warp walks rows
+//    one after another behind dependent loads. Its gathers take the most-gathered
+//    columns from a shared-memory cache and the rest from global memory. Groups go
+//    to warps from a counter; the last CTA ends the iteration. During a segmented
+//    solve the iterate x, the row sums and the teleport entries are kept in phase
+//    2's lane order, so the row updates read and write them with coalesced
+//    accesses. Results do not depend on scheduling.
 //
 // Bank spreading: a block load copies x/s[block] into shared memory as it lies
 // in global memory, so a column's bank is its position mod 32. R-MAT-like graphs
@@ -87,6 +93,20 @@ struct SegPlan {
   uint8_t *bdense = nullptr; // 1: the block is staged in shared memory; 0: gathered from global
   int32_t *cta = nullptr;    // first group of each CTA, grid + 1 entries
   int64_t ngroups = 0, nfrag = 0, nell = 0;
+  // phase 2: the rows below T as sliced ELL (entries from sidx, -1 past a row's end)
+  int32_t *rrow = nullptr;   // row of every group lane (-1: empty lane), nrgroups * 32
+  int64_t *rgofs = nullptr;  // first entry of each group, nrgroups + 1
+  int32_t *ridx = nullptr;   // column entries
+  float *rwts = nullptr;     // their weights (weighted graphs)
+  int32_t *rgrab = nullptr;  // group counter of phase 2 (zero between launches)
+  int64_t nrgroups = 0, nrell = 0;
+  // Positions of the iterate during a segmented solve: g * 32 + l for phase 2's
+  // group g, lane l, then nrgroups * 32 + h for hub h. Per position: its row (-1
+  // for empty lanes) and the row's cached-column slot.
+  int32_t *ppos = nullptr;   // position of every row, n entries
+  int32_t *prow = nullptr;   // row of every position, npos entries
+  int32_t *pslot = nullptr;  // column-cache slot of every position (-1: not cached)
+  int64_t npos = 0;
   bool weighted = false;
   bool ok = false;
 };
@@ -100,6 +120,15 @@ struct SegArgs {
   const uint8_t *bdense;
   int64_t n32;  // vertices rounded up to whole 32-entry chunks (the permuted x/s extent)
   int32_t S, nblocks;
+  const int32_t *rrow;
+  const int64_t *rgofs;
+  const int32_t *ridx;
+  const float *rwts;
+  int32_t *rgrab;
+  int64_t nrgroups;
+  const int32_t *pslot;  // per position: cached-column slot
+  const float *ps;       // per position: row sum s (0: dangling), filled per solve
+  const float *pt;       // per position: teleport entry (nullptr: uniform), filled per solve
 };
 
 #ifndef MG_PRB_NO_PLAN_KERNELS  // plan building runs in pagerank.cu only
@@ -231,31 +260,79 @@ __global__ void __launch_bounds__(256) seg_sell_kernel(const int2 *__restrict__ 
     }
   }
 }
-#endif  // MG_PRB_NO_PLAN_KERNELS
-
-// U sliced-ELL steps of a lane from q (indices) / qw (weights); CHECK bounds the
-// steps by `left`.
-template <bool WEIGHTED, int U, bool CHECK, typename Gather>
-__device__ __forceinline__ void seg_steps(const int32_t *q, const float *qw, Gather &gather, int32_t left,
-                                          Comp &acc) {
-  int32_t c[U];
-#pragma unroll
-  for (int j = 0; j < U; j++) c[j] = (!CHECK || j < left) ? prb_stream(q + 32 * j) : -1;
-  float v[U];
-#pragma unroll
-  for (int j = 0; j < U; j++) v[j] = c[j] >= 0 ? gather(c[j]) : 0.f;
-#pragma unroll
-  for (int j = 0; j < U; j++) {
-    if (c[j] < 0) continue;
-    if (WEIGHTED) {
-      const float a = prb_stream(qw + 32 * j);
-      const float p = a * v[j];
-      two_sum_add(acc, p);
-      acc.lo += __fmaf_rn(a, v[j], -p);
-    } else {
-      two_sum_add(acc, v[j]);
+// Phase 2's sliced ELL: one warp per group copies lane l's row (sidx / swts over
+// the row's edges, in edge order) into entries rgofs[g] + 32 i + l.
+__global__ void __launch_bounds__(256) seg_rows_fill_kernel(const int32_t *__restrict__ rrow,
+                                                            const int64_t *__restrict__ rgofs, int64_t ngroups,
+                                                            const int32_t *__restrict__ off,
+                                                            const int32_t *__restrict__ sidx,
+                                                            const float *__restrict__ swts, int32_t *__restrict__ ridx,
+                                                            float *__restrict__ rwts) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t gi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < ngroups;
+       gi += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int32_t r = rrow[gi * 32 + lane];
+    if (r < 0) continue;
+    const int32_t b = off[r], d = off[r + 1] - b;
+    const int64_t o = rgofs[gi] + lane;
+    for (int32_t i = 0; i < d; i++) {
+      ridx[o + 32 * (int64_t)i] = sidx[b + i];
+      if (rwts) rwts[o + 32 * (int64_t)i] = swts[b + i];
     }
   }
+}
+
+// Cached-column slot of every iterate position (plan data).
+__global__ void seg_pos_slot_kernel(const int32_t *__restrict__ prow, int64_t npos, const int32_t *__restrict__ slot,
+                                    int32_t *__restrict__ pslot) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npos; i += (int64_t)gridDim.x * blockDim.x)
+    pslot[i] = prow[i] >= 0 ? slot[prow[i]] : -1;
+}
+#endif  // MG_PRB_NO_PLAN_KERNELS
+
+// One lane's row of a sliced-ELL group (a phase-1 fragment or a phase-2 row):
+// `depth` steps from q (qw), index loads one round of U steps ahead of the
+// gathers; -1 entries are padding.
+template <bool WEIGHTED, int U, typename Gather>
+__device__ __forceinline__ Comp sell_walk(const int32_t *q, const float *qw, int32_t depth, Gather &gather) {
+  Comp acc{0.f, 0.f};
+  int32_t c[U];
+  float w[U];
+#pragma unroll
+  for (int j = 0; j < U; j++) {
+    c[j] = j < depth ? prb_stream(q + 32 * j) : -1;
+    w[j] = (WEIGHTED && j < depth) ? prb_stream(qw + 32 * j) : 0.f;
+  }
+  for (int32_t i = 0; i < depth; i += U) {
+    int32_t cn[U];
+    float wn[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      const int32_t k = i + U + j;
+      cn[j] = k < depth ? prb_stream(q + 32 * k) : -1;
+      wn[j] = (WEIGHTED && k < depth) ? prb_stream(qw + 32 * k) : 0.f;
+    }
+    float v[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) v[j] = c[j] != -1 ? gather(c[j]) : 0.f;
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      if (c[j] == -1) continue;
+      if (WEIGHTED) {
+        const float p = w[j] * v[j];
+        two_sum_add(acc, p);
+        acc.lo += __fmaf_rn(w[j], v[j], -p);
+      } else {
+        two_sum_add(acc, v[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      c[j] = cn[j];
+      w[j] = wn[j];
+    }
+  }
+  return acc;
 }
 
 // Phase 1 of a segmented iteration on one CTA: walks the CTA's groups block by
@@ -321,20 +398,9 @@ __device__ __forceinline__ void seg_phase(const SegArgs &sg, const float *gold, 
       const int32_t steps = (int32_t)((sg.gofs[gi + 1] - s0) >> 5);
       const int32_t *q = sg.pidx + s0 + lane;
       const float *qw = WEIGHTED ? sg.pwts + s0 + lane : nullptr;
-      Comp acc{0.f, 0.f};
-      int32_t i = 0;
-      if (dense) {
-        for (; i + SEG_U <= steps; i += SEG_U)
-          seg_steps<WEIGHTED, SEG_U, false>(q + 32 * i, WEIGHTED ? qw + 32 * i : nullptr, from_smem, 0, acc);
-        if (i < steps)
-          seg_steps<WEIGHTED, SEG_U, true>(q + 32 * i, WEIGHTED ? qw + 32 * i : nullptr, from_smem, steps - i, acc);
-      } else {
-        for (; i + SEG_U <= steps; i += SEG_U)
-          seg_steps<WEIGHTED, SEG_U, false>(q + 32 * i, WEIGHTED ? qw + 32 * i : nullptr, from_global, 0, acc);
-        if (i < steps)
-          seg_steps<WEIGHTED, SEG_U, true>(q + 32 * i, WEIGHTED ? qw + 32 * i : nullptr, from_global, steps - i,
-                                           acc);
-      }
+      constexpr int U = WEIGHTED ? 4 : SEG_U;
+      const Comp acc = dense ? sell_walk<WEIGHTED, U>(q, qw, steps, from_smem)
+                             : sell_walk<WEIGHTED, U>(q, qw, steps, from_global);
       fin(e, acc);
     }
     __syncthreads();  // the segment ends for every warp at once
