@@ -11,13 +11,14 @@ one step runs, on the device-resident graph,
                             -> TEPS edges = m * iterations
 
 value = sum of TEPS edges / sum of their device times (GTEPS, CUDA events on the
-engine's stream, L2 flushed between steps). SSSP is timed after the steps and
-reported under "per_algorithm" only: the reference's CPU SSSP is O(n^2) and has no
-CPU baseline at this size.
+engine's stream, L2 flushed between steps). SSSP is timed after the steps, reported
+under "per_algorithm", and folded into "value_all_four" (all four programs per
+step); the headline leaves it out because the reference's CPU SSSP is O(n^2) and
+has no CPU baseline at this size.
 
 --impl reference times the reference's own CPU functions (CPUBFS, CPUCC, CPUPR,
-compiled from the reference tree into oracle/_ref) on the host, on a bounded
-sample of the same workload (the same generator at scale 20).
+compiled from the reference tree into oracle/_ref) on the host, on the same
+scale-22 graph, the driver's passes divided among the host cores.
 
 Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
 torch.distributed.run (one replica per GPU, no data-path collective: every rank
@@ -54,10 +55,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-scale", type=int, default=CPU_SAMPLE_SCALE,
-                   help="R-MAT scale of the bounded sample the reference's CPU code runs on")
+                   help="R-MAT scale of the bounded sample of the GPU arm's one-core cpu_baseline")
+    p.add_argument("--ref-scale", type=int, default=None,
+                   help="R-MAT scale the reference arm runs on (default: --scale, the headline graph)")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-versus-looped section")
     p.add_argument("--batched-scale", type=int, default=20)
-    p.add_argument("--pr-gather", default="auto", choices=["auto", "binned", "cached"],
+    p.add_argument("--pr-gather", default="auto", choices=["auto", "binned", "cached", "tma", "segmented"],
                    help="PageRank gather: autotuned per graph (default) or forced (for profiling one kernel)")
     p.add_argument("--no-extra", action="store_true",
                    help="skip the lattice (BFS/SSSP) and weighted PageRank forward + adjoint sections")
@@ -74,6 +77,29 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+# Kernels of one PageRank iteration per gather variant (mg_stats.variant).
+PR_KERNELS = {0: "solve_binned_kernel", 1: "solve_gather_kernel + solve_fixup_kernel",
+              2: "solve_binned_hub_kernel", 3: "solve_segment_kernel + solve_rows_kernel"}
+
+
+def pagerank_fp64_check(h, x_gpu, iters, weights=None, fixed_point=True):
+    """Error of a GPU PageRank result against the FP64 oracle: L1 at the same
+    number of iterations (the tests' 1e-6 bound), and, when asked, L1 to the FP64
+    fixed point (power iteration to an L1 change below 1e-11). Part of the CPU
+    baseline leg: the oracle is the checker, outside every timed region."""
+    import oracle
+    t0 = time.perf_counter()
+    xr, _, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, weights, ALPHA, 0.0, int(iters))
+    out = {"l1_vs_fp64": float(np.abs(x_gpu.astype(np.float64) - xr).sum()), "iterations": int(iters),
+           "tolerance": PR_TOL}
+    if fixed_point:
+        xf, itf, rf = oracle.pr_normalized(h.row_offsets, h.col_idx, weights, ALPHA, 1e-11, 1000)
+        out["l1_vs_fp64_fixed_point"] = float(np.abs(x_gpu.astype(np.float64) - xf).sum())
+        out["fixed_point_iterations"] = int(itf)
+    out["check_s"] = time.perf_counter() - t0
+    return out
 
 
 def sources(h, k, seed):
@@ -258,10 +284,12 @@ def lattice_section(torch, mg, side=4096):
     return res
 
 
-def adjoint_section(torch, mg, scale=24):
+def adjoint_section(torch, mg, scale=24, keep=None):
     """Weighted PageRank forward + adjoint: R-MAT `scale` ef16 directed, weights
     lognormal(0, 1) (normalised by their row sums), alpha 0.85, forward to L1 <
-    1e-6; backward of L = w . x with w ~ N(0, 1) to relative tolerance 1e-7."""
+    1e-6 (gather autotuned per graph); backward of L = w . x with w ~ N(0, 1) to
+    relative tolerance 1e-7. `keep` (a dict) receives the graph and the forward
+    result for the FP64 check of the CPU baseline leg."""
     h = mg.gen_rmat(scale, 16, SEED + 12, symmetrize=False, weights="lognormal", p0=0, p1=1)
     n, m = h.n, h.m
     g = mg.Graph(h.row_offsets, h.col_idx, h.weights_f32)
@@ -270,13 +298,17 @@ def adjoint_section(torch, mg, scale=24):
     gw = torch.empty(m, dtype=torch.float32, device="cuda")
     gt = torch.empty(n, dtype=torch.float32, device="cuda")
     for _ in range(2):
-        _, sf = g.pagerank(mode="normalized", weighted=True, alpha=ALPHA, tol=PR_TOL, max_iter=200, out=x)
+        _, sf = g.pagerank(mode="normalized", weighted=True, alpha=ALPHA, tol=PR_TOL, max_iter=200, out=x,
+                           autotune=True)
         _, _, sb = g.pagerank_backward(x, wv, weighted=True, alpha=ALPHA, tol=1e-7, max_iter=200,
                                        out_weights=gw, out_teleport=gt)
     g.close()
+    if keep is not None:
+        keep.update(h=h, x=x.cpu().numpy(), iterations=sf["iterations"])
     return {"config": f"R-MAT s{scale} ef16 directed (n={n}, m={m}), lognormal(0,1) weights, alpha {ALPHA}",
             "forward": {"ms": sf["kernel_ms"], "iterations": sf["iterations"],
-                        "gteps": m * sf["iterations"] / sf["kernel_ms"] / 1e6},
+                        "gteps": m * sf["iterations"] / sf["kernel_ms"] / 1e6,
+                        "gather_kernel": PR_KERNELS.get(sf["variant"])},
             "backward": {"ms": sb["kernel_ms"], "iterations": sb["iterations"],
                          "gteps": m * sb["iterations"] / sb["kernel_ms"] / 1e6}}
 
@@ -372,30 +404,33 @@ def reference_cpu_baseline(scale: int) -> dict:
         return {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
 
 
-def _ref_worker(path, src, steps, warmup, barrier, out):
-    """One reference process: loads the sample graph, runs the warm-up passes,
-    waits for the others, then times `steps` passes of CPUBFS + CPUCC + CPUPR."""
+def _ref_worker(path, warm_srcs, timed_srcs, barrier, out):
+    """One reference process: loads the graph, runs its share of the warm-up
+    passes, waits for the others, then times its share of the timed passes of
+    CPUBFS + CPUCC + CPUPR (one BFS source per pass)."""
     import mirrorofmapgraph_b200 as mg
     h = mg.load_csr(path)
-    for _ in range(warmup):
-        cpu_reference_run(h, src)
+    for s_ in warm_srcs:
+        cpu_reference_run(h, s_)
     barrier.wait()
     t0 = time.time()
     per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
-    for _ in range(steps):
-        r = cpu_reference_run(h, src)
+    for s_ in timed_srcs:
+        r = cpu_reference_run(h, s_)
         for k in per:
             per[k][0] += r[k][0]
             per[k][1] += r[k][1]
-    out.put((t0, time.time(), per))
+    out.put((t0, time.time(), per, len(timed_srcs)))
 
 
 def run_reference(args):
     """The reference's own CPU implementation of the path (CPUBFS, CPUCC, CPUPR,
-    compiled from the reference tree into oracle/_ref). The functions are serial,
-    so all host cores are used by running one independent copy per core (up to
-    32), each from its own source, on the bounded sample graph; the value is all
-    copies' TEPS edges over the wall time from the common start to the last finish."""
+    compiled from the reference tree into oracle/_ref), on the GPU arm's graph
+    (R-MAT --scale, same generator and seed). The functions are serial, so the
+    host cores run independent processes; the driver's --warmup and --steps passes
+    are divided among them (pass j goes to process j mod P and uses the GPU arm's
+    BFS source of step j). The value is the timed passes' TEPS edges over the wall
+    time from the common start to the last finish."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -407,21 +442,23 @@ def run_reference(args):
         import mirrorofmapgraph_b200 as mg
         if not oracle.have_ref():
             raise RuntimeError("oracle/_ref/libmgref.so missing (reference CPU path not built)")
-        sc = args.cpu_sample_scale
+        sc = args.ref_scale if args.ref_scale else args.scale
         h = cpu_sample_graph(sc)
         try:
             ncores = len(os.sched_getaffinity(0))
         except Exception:
             ncores = os.cpu_count() or 1
-        procs = max(1, min(32, ncores))
-        srcs = sources(h, procs, SEED + 1)
+        steps = max(1, args.steps)
+        procs = max(1, min(32, ncores, steps))
+        srcs = sources(h, max(steps + args.warmup, 8), SEED + 1)
+        warm = [[srcs[j] for j in range(args.warmup) if j % procs == i] for i in range(procs)]
+        timed = [[srcs[args.warmup + j] for j in range(steps) if j % procs == i] for i in range(procs)]
         tmpdir = tempfile.mkdtemp(prefix="mg_ref_")
-        path = os.path.join(tmpdir, "sample.csr")
+        path = os.path.join(tmpdir, "graph.csr")
         mg.save_csr(path, h)
         ctx = mp.get_context("spawn")
         barrier, out = ctx.Barrier(procs), ctx.Queue()
-        ps = [ctx.Process(target=_ref_worker, args=(path, srcs[i], args.steps, args.warmup, barrier, out))
-              for i in range(procs)]
+        ps = [ctx.Process(target=_ref_worker, args=(path, warm[i], timed[i], barrier, out)) for i in range(procs)]
         for p_ in ps:
             p_.start()
         res = [out.get() for _ in ps]
@@ -429,22 +466,24 @@ def run_reference(args):
             p_.join()
         os.remove(path)
         os.rmdir(tmpdir)
-        wall = max(r[1] for r in res) - min(r[0] for r in res)
+        busy = [r for r in res if r[3] > 0]
+        wall = max(r[1] for r in busy) - min(r[0] for r in busy)
         per = {k: [sum(r[2][k][0] for r in res), sum(r[2][k][1] for r in res)] for k in ("bfs", "cc", "pagerank")}
         edges = sum(v[0] for v in per.values())
         value = edges / wall / 1e9
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32",
             "data": "synthetic (seeded R-MAT)",
-            "config": {"workload": f"rmat_s{sc}_ef16_sym (bounded sample of rmat_s22_ef16_sym): "
-                                   "CPUBFS + CPUCC + CPUPR", "scale": sc, "n": h.n, "m": h.m},
+            "config": {"workload": f"rmat_s{sc}_ef{args.edge_factor}_sym: CPUBFS + CPUCC + CPUPR",
+                       "scale": sc, "edge_factor": 16, "n": h.n, "m": h.m},
             "host": host_info(),
             "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs, "kind": "reference",
-                             "sample": f"{procs} concurrent copies of the reference's serial CPUBFS/CPUCC/CPUPR, "
-                                       f"each {args.steps} step(s) on R-MAT scale {sc} from its own "
-                                       f"source (CPUPR alone takes ~35 s at scale 22)"},
+                             "sample": f"the driver's {steps} timed step(s) (one BFS source each, CC, PageRank) "
+                                       f"on R-MAT scale {sc}, divided among {procs} processes of the "
+                                       f"reference's serial CPUBFS/CPUCC/CPUPR (pass j on process j mod "
+                                       f"{procs}); {args.warmup} warm-up pass(es) divided the same way"},
             "per_algorithm": {k: {"gteps_per_core": v[0] / v[1] / 1e9 if v[1] else None, "core_seconds": v[1]}
                               for k, v in per.items()},
             "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -521,6 +560,8 @@ def run_ours(args):
     launches = 0
     pr_iters = 0
     pr_cache = 0
+    pr_variant = 0
+    pr_last_iters = 0
     pr_ms = 0.0
     bfs_stats = []
     cc_stats = []
@@ -532,11 +573,14 @@ def run_ours(args):
             launches += r[k][2]["launches"]
         pr_iters += r["pagerank"][2]["iterations"]
         pr_cache = r["pagerank"][2]["status_detail"]
+        pr_variant = r["pagerank"][2]["variant"]
+        pr_last_iters = r["pagerank"][2]["iterations"]
         pr_ms += r["pagerank"][1]
         bfs_stats.append(r["bfs"][2])
         cc_stats.append(r["cc"][2])
     torch.cuda.synchronize()
     clock_info = clocks.stop()
+    x_pr = rank_v.cpu().numpy()  # the last step's PageRank, for the FP64 check
     if dist:
         dist.barrier()
     edges = sum(v[0] for v in per.values())
@@ -562,15 +606,15 @@ def run_ours(args):
         sssp_ms += t
         sssp_bytes += st["bytes_compulsory"]
 
-    # Roofline of the dominant kernel: one launch per PageRank iteration of the
-    # gather the autotuner kept -- solve_binned_kernel (degree-binned CSC gather +
-    # row update + residual) or solve_binned_hub_kernel (the same with a column
-    # cache in shared memory). Algorithmic
-    # bytes per launch = offsets 4(n+1) + indices 4m + read x 4n + write x 4n +
-    # write x/s 4n. Its duration is the PageRank call's device time divided by the
-    # iterations (the call also holds two init kernels, so this slightly
-    # understates the kernel's own rate).
-    pr_kernel = "solve_binned_hub_kernel" if pr_cache > 0 else "solve_binned_kernel"
+    # Roofline of the dominant kernel: one PageRank iteration of the gather the
+    # autotuner kept (mg_stats.variant): solve_binned_kernel, solve_binned_hub_kernel
+    # (column cache), or the segmented gather's pair solve_segment_kernel (hub rows
+    # by column block) + solve_rows_kernel (the other rows, hub finishing, row
+    # updates). Algorithmic bytes per iteration = offsets 4(n+1) + indices 4m +
+    # read x 4n + write x 4n + write x/s 4n. Its duration is the PageRank call's
+    # device time divided by the iterations (the call also holds a few init
+    # kernels, so this slightly understates the kernels' own rate).
+    pr_kernel = PR_KERNELS.get(pr_variant, "solve_binned_kernel")
     pr_bytes_iter = 4 * (n + 1) + 4 * m + 12 * n
     pr_s_iter = (pr_ms / max(pr_iters, 1)) * 1e-3
     achieved = pr_bytes_iter / pr_s_iter / 1e9
@@ -594,6 +638,14 @@ def run_ours(args):
     if sssp_ms:
         per_alg["sssp"]["hbm_frac"] = sssp_bytes / (sssp_ms * 1e-3) / 1e9 / peak
     per_alg["pagerank"]["hbm_frac"] = achieved / peak
+    per_alg["pagerank"]["gather_kernel"] = pr_kernel
+    # All four programs per step: the three of the headline plus one SSSP run
+    # (the mean of the SSSP runs above), on the same graph.
+    nss = max(1, min(3, args.steps))
+    value_all_four = None
+    if sssp_ms:
+        value_all_four = ((edges / args.steps + sssp_edges / nss) /
+                          ((ms / args.steps + sssp_ms / nss) * 1e-3) / 1e9 * (world if world > 1 else 1))
 
     # End to end through the public API with host buffers: upload from pinned host
     # memory, run the three programs with outputs in pinned host buffers (read back
@@ -641,7 +693,8 @@ def run_ours(args):
     e2e = e2e_edges / e2e_s / 1e9 * (world if world > 1 else 1) if e2e_s > 0 else None
 
     line = {
-        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "value_all_four": value_all_four, "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32 (BFS/CC), f32 + f64 reductions (PageRank)",
         "data": "synthetic (seeded R-MAT, no vertex permutation)",
@@ -650,7 +703,8 @@ def run_ours(args):
                    "scale": args.scale, "edge_factor": args.edge_factor, "n": n, "m": m,
                    "l2": "256 MiB buffer written between steps; graph (CSR 537 MB) larger than L2",
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": f"{pr_kernel} (one PageRank iteration"
+        "roofline": {"bound": "hbm", "kernel": f"{pr_kernel} (one PageRank iteration per launch pair)"
+                     if pr_variant in (1, 3) else f"{pr_kernel} (one PageRank iteration"
                      + (f", {pr_cache} cached columns)" if pr_cache else ")"),
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -663,7 +717,8 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if cpu_leg:
         line["cpu_baseline"] = reference_cpu_baseline(args.cpu_sample_scale)
     g.close()
     if not args.no_batched:
@@ -671,12 +726,32 @@ def run_ours(args):
             line["batched"] = batched_section(args.batched_scale, torch, mg)
         except Exception as e:
             line["batched"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    adj_keep = {}
     if not args.no_extra:
-        for key, fn in (("lattice", lattice_section), ("pagerank_adjoint", adjoint_section)):
+        for key, fn in (("lattice", lambda t, m_: lattice_section(t, m_)),
+                        ("pagerank_adjoint", lambda t, m_: adjoint_section(t, m_, keep=adj_keep))):
             try:
                 line[key] = fn(torch, mg)
             except Exception as e:
                 line[key] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if cpu_leg:
+        # CPU baseline leg, after every timed region: the PageRank results checked
+        # against the FP64 oracle (the error stated per run)
+        try:
+            chk = pagerank_fp64_check(h, x_pr, pr_last_iters, fixed_point=True)
+            per_alg["pagerank"].update({k: chk[k] for k in ("l1_vs_fp64", "l1_vs_fp64_fixed_point")})
+            line["cpu_baseline"]["pagerank_check"] = chk
+        except Exception as e:
+            per_alg["pagerank"]["l1_vs_fp64"] = f"unavailable: {type(e).__name__}: {e}"
+        if adj_keep and isinstance(line.get("pagerank_adjoint"), dict) and "forward" in line["pagerank_adjoint"]:
+            try:
+                hk = adj_keep["h"]
+                chk = pagerank_fp64_check(hk, adj_keep["x"], adj_keep["iterations"], weights=hk.weights_f32,
+                                          fixed_point=False)
+                line["pagerank_adjoint"]["forward"]["l1_vs_fp64"] = chk["l1_vs_fp64"]
+                line["cpu_baseline"]["pagerank_adjoint_check"] = chk
+            except Exception as e:
+                line["pagerank_adjoint"]["forward"]["l1_vs_fp64"] = f"unavailable: {type(e).__name__}: {e}"
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

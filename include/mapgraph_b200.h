@@ -97,7 +97,8 @@ typedef struct mg_stats {
   double residual;          /* PageRank: last L1 residual (normalised mode) */
   int64_t launches;         /* kernels launched by the call */
   int32_t status_detail;    /* BFS: levels run bottom-up; otherwise detail of a non-OK status */
-  int32_t reserved;
+  int32_t variant;          /* NORMALIZED PageRank (nvec == 1): the gather_kernel that ran (after
+                               autotuning); 0 for the other programs */
 } mg_stats;
 
 /* PageRank options. Zero-initialised fields take the defaults in brackets. */

@@ -38,7 +38,7 @@ class MgOpts(C.Structure):
 class MgStats(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("edges_traversed", C.c_int64), ("edges_inspected", C.c_int64),
                 ("bytes_compulsory", C.c_int64), ("kernel_ms", C.c_double), ("residual", C.c_double),
-                ("launches", C.c_int64), ("status_detail", C.c_int32), ("reserved", C.c_int32)]
+                ("launches", C.c_int64), ("status_detail", C.c_int32), ("variant", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -1840,6 +1840,7 @@ static mg_status pagerank_normalized(mg_graph *g, const float *tele_dev, float *
     // gather + fix-up), plus the loop guard when the loop runs as a graph
     const int64_t per_it = (variant == 1 || sp.use_seg) ? 2 : 1;
     stats->status_detail = (sp.use_hub || sp.use_seg) ? sp.a.nhub : 0;
+    stats->variant = variant;
     stats->launches = 4 + ((sp.use_hub || sp.use_seg) ? 1 : 0) +
                       (o.use_graph >= 0 ? (per_it + 1) * (int64_t)hc.body_iters : per_it * (int64_t)hc.level);
   }
@@ -2133,6 +2134,7 @@ extern "C" mg_status mg_pagerank(mg_graph *g, const float *teleport, int32_t nve
     total.launches += st.launches;
     total.residual = std::max(total.residual, st.residual);
     total.status_detail = st.status_detail;  // cached columns of the gather (same for every vector)
+    total.variant = st.variant;
   }
   if (stats) *stats = total;
   return MG_OK;

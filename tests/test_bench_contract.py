@@ -26,7 +26,7 @@ def _run(env_extra, *args):
 
 @pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref not built (reference CPU path)")
 def test_reference_arm_prints_one_contract_line():
-    lines = _run({}, "--impl", "reference", "--steps", "1", "--warmup", "0", "--cpu-sample-scale", "12")
+    lines = _run({}, "--impl", "reference", "--steps", "1", "--warmup", "0", "--ref-scale", "12")
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert "unavailable" not in d, d
@@ -43,7 +43,39 @@ def test_reference_arm_prints_one_contract_line():
 
 def test_reference_arm_is_silent_on_other_ranks():
     assert _run({"RANK": "1", "WORLD_SIZE": "2"}, "--impl", "reference", "--steps", "1", "--warmup", "0",
-                "--cpu-sample-scale", "12") == []
+                "--ref-scale", "12") == []
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref not built (reference CPU path)")
+def test_reference_arm_divides_the_passes_among_processes():
+    """Three timed passes and two warm-up passes over the processes: every timed
+    pass counted once (one BFS source each), the graph of the GPU arm's scale."""
+    lines = _run({}, "--impl", "reference", "--steps", "3", "--warmup", "2", "--ref-scale", "11")
+    d = json.loads(lines[0])
+    assert "unavailable" not in d, d
+    assert d["config"]["scale"] == 11 and d["steps"] == 3
+    assert 1 <= d["cpu_baseline"]["cores"] <= 3
+    import bench
+    h = bench.cpu_sample_graph(11)
+    assert d["value"] > 0 and h.m == d["config"]["m"]
+    # CC counts m edges per pass: exactly three passes were timed
+    cc = d["per_algorithm"]["cc"]
+    assert abs(cc["gteps_per_core"] * cc["core_seconds"] * 1e9 - 3 * h.m) < 1e-3 * h.m
+
+
+def test_pagerank_fp64_check_measures_the_error():
+    """The CPU baseline leg's PageRank check: an exact FP64 result has no error,
+    a perturbed one shows its L1 distance."""
+    import numpy as np
+    import bench
+    h = bench.cpu_sample_graph(10)
+    x, it, _ = oracle.pr_normalized(h.row_offsets, h.col_idx, None, bench.ALPHA, 0.0, 12)
+    chk = bench.pagerank_fp64_check(h, x.astype(np.float32), 12, fixed_point=True)
+    assert chk["l1_vs_fp64"] < 1e-6 and chk["iterations"] == 12
+    assert chk["fixed_point_iterations"] > 12 and chk["l1_vs_fp64_fixed_point"] > chk["l1_vs_fp64"]
+    y = x.copy()
+    y[0] += 1e-3
+    assert abs(bench.pagerank_fp64_check(h, y, 12, fixed_point=False)["l1_vs_fp64"] - 1e-3) < 1e-9
 
 
 @pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref not built (reference CPU path)")

@@ -80,6 +80,29 @@ def test_bfs_ragged_matches_each_member():
         assert st["edges_traversed"] == etrav
 
 
+def test_bfs_ragged_full_batch_32_graphs():
+    """The batched workload's ragged batch at its stated size: 32 independent
+    R-MAT graphs of scale U{10..18}, edge factor 8, symmetrised (the bench's own
+    seeds), one BFS from vertex 0 each in one device run; every member bit-exact
+    against the oracle's BFS of that graph alone (the reference runs one engine
+    call per source, Algorithms/BFS/bfs.cu:442-456)."""
+    seed = 20140601
+    rng = np.random.default_rng(seed + 10)
+    scales = rng.integers(10, 19, 32)
+    members = [mg.gen_rmat(int(sc), 8, seed + 100 + i, symmetrize=True) for i, sc in enumerate(scales)]
+    assert len(members) == 32 and scales.min() >= 10 and scales.max() <= 18
+    with mg.Graph.ragged(members, symmetric=True) as g:
+        bases = g.ragged_bases()
+        for direction in ("auto", "push"):
+            depth, st = g.bfs_ragged(np.zeros(32, dtype=np.int32), direction=direction)
+            etrav = 0
+            for i, hm in enumerate(members):
+                ref = oracle.bfs(hm.row_offsets, hm.col_idx, [0])
+                np.testing.assert_array_equal(depth[bases[i]:bases[i + 1]], ref)
+                etrav += int(np.diff(hm.row_offsets)[ref >= 0].sum())
+            assert st["edges_traversed"] == etrav
+
+
 def test_bfs_ragged_rejects_bad_sources():
     members = [mg.gen_er(50, 200, 1), mg.gen_er(30, 90, 2)]
     with mg.Graph.ragged(members) as g:
