@@ -375,6 +375,29 @@ typedef struct mg_level_record {
 } mg_level_record;
 mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count);
 
+/* ---- Traversal tuning (per graph) -------------------------------------------
+ * Thresholds and launch shapes of the traversal kernels, read by every later call
+ * on the graph (the reference fixes its equivalents at compile time, e.g. the
+ * expand/contract tile sizes of GASengine/vertex_centric/*_problem_type.cuh).
+ * mg_tuning_defaults fills the defaults; mg_graph_set_tuning checks each field
+ * against its range (MG_ERR_ARG, nothing changed, on a bad value). The Python
+ * package's tuning module times candidate sets on the device for a graph class
+ * and caches the fastest in a JSON file. */
+typedef struct mg_tuning {
+  int32_t sssp_heavy;       /* SSSP round: frontier vertices of at least this many edges are cut into chunks of
+                               256 edges that every warp of the grid relaxes; lighter ones are walked by the warp
+                               that drew them [256; 1 .. 2^30] */
+  int32_t sssp_heavy_small; /* the same for a frontier of fewer vertices than the grid has threads [32; 1 ..
+                               sssp_heavy] */
+  int32_t sssp_ctas_per_sm; /* CTAs of 256 threads per SM of the SSSP round kernels [4; 1 .. 8] */
+  int32_t sssp_chunk_cap;   /* SSSP chunk list capacity in chunks; 0: the bound of the graph's edges (at most
+                               2^23); past it a warp walks its heavy vertices itself [0; 0 .. 2^30] */
+  int32_t reserved[12];
+} mg_tuning;
+void mg_tuning_defaults(mg_tuning *t);
+mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t);
+mg_status mg_graph_get_tuning(mg_graph *g, mg_tuning *t);
+
 /* ---- Test hooks: host-side fault injection ----------------------------------
  * For failure-path tests; nothing here faults, traps or hangs a device.
  * mg_debug_fail_alloc(k): the k-th device allocation from now, and every later

@@ -66,6 +66,14 @@ class MgLevelRecord(C.Structure):
 MG_TRACE_LEVELS = 4096
 
 
+class MgTuning(C.Structure):
+    _fields_ = [("sssp_heavy", C.c_int32), ("sssp_heavy_small", C.c_int32), ("sssp_ctas_per_sm", C.c_int32),
+                ("sssp_chunk_cap", C.c_int32), ("reserved", C.c_int32 * 12)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class MgHostCsr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("row_offsets", C.POINTER(C.c_int32)),
                 ("col_idx", C.POINTER(C.c_int32)), ("weights_i32", C.POINTER(C.c_int32)),
@@ -126,6 +134,9 @@ SIGNATURES = {
     "mg_part_pr_merge": (C.c_int, [_P, _P, C.c_int32, C.c_int64, _P, C.POINTER(MgPartLevel)]),
     "mg_part_pr_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
     "mg_graph_trace": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
+    "mg_tuning_defaults": (None, [C.POINTER(MgTuning)]),
+    "mg_graph_set_tuning": (C.c_int, [_P, C.POINTER(MgTuning)]),
+    "mg_graph_get_tuning": (C.c_int, [_P, C.POINTER(MgTuning)]),
     "mg_debug_fail_alloc": (C.c_int, [C.c_int64]),
     "mg_debug_barrier_skew": (C.c_int, [C.c_int32, C.c_int64]),
     "mg_debug_seg_plan": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),

@@ -63,6 +63,41 @@ extern "C" mg_status mg_graph_sync(mg_graph *g) {
   return MG_OK;
 }
 
+extern "C" void mg_tuning_defaults(mg_tuning *t) {
+  if (t) *t = tuning_defaults();
+}
+
+extern "C" mg_status mg_graph_get_tuning(mg_graph *g, mg_tuning *t) {
+  if (!g || !t) {
+    mg_set_error("mg_graph_get_tuning: null argument");
+    return MG_ERR_ARG;
+  }
+  *t = g->tune;
+  return MG_OK;
+}
+
+extern "C" mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t) {
+  if (!g || !t) {
+    mg_set_error("mg_graph_set_tuning: null argument");
+    return MG_ERR_ARG;
+  }
+  struct Range {
+    const char *name;
+    int32_t v, lo, hi;
+  } const r[] = {{"sssp_heavy", t->sssp_heavy, 1, 1 << 30},
+                 {"sssp_heavy_small", t->sssp_heavy_small, 1, t->sssp_heavy},
+                 {"sssp_ctas_per_sm", t->sssp_ctas_per_sm, 1, 8},
+                 {"sssp_chunk_cap", t->sssp_chunk_cap, 0, 1 << 30}};
+  for (const Range &x : r) {
+    if (x.v < x.lo || x.v > x.hi) {
+      mg_set_error("mg_graph_set_tuning: %s = %d outside [%d, %d]", x.name, x.v, x.lo, x.hi);
+      return MG_ERR_ARG;
+    }
+  }
+  g->tune = *t;
+  return MG_OK;
+}
+
 extern "C" mg_status mg_graph_trace(mg_graph *g, mg_level_record *out, int32_t cap, int32_t *count) {
   if (!g || !count || (cap > 0 && !out)) {
     mg_set_error("mg_graph_trace: null argument");

@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <initializer_list>
 #include <vector>
 
@@ -88,6 +89,16 @@ struct Workspace {
   size_t bytes = 0;
 };
 
+// Default traversal tuning (mg_tuning_defaults).
+inline mg_tuning tuning_defaults() {
+  mg_tuning t;
+  std::memset(&t, 0, sizeof(t));
+  t.sssp_heavy = 256;
+  t.sssp_heavy_small = 32;
+  t.sssp_ctas_per_sm = 4;
+  return t;
+}
+
 struct mg_graph {
   int device = 0;
   int64_t n = 0, m = 0;
@@ -118,6 +129,7 @@ struct mg_graph {
   DevCtl *ctl_host = nullptr;  // pinned host mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   void *cache = nullptr;       // cached executable loop graphs (engine.cu)
+  mg_tuning tune = tuning_defaults();  // traversal thresholds and launch shapes (mg_graph_set_tuning)
 };
 
 // Every device allocation of the library goes through here: cudaMallocAsync on

@@ -26,10 +26,9 @@
 namespace mg {
 
 constexpr int SSSP_NT = 256;
-constexpr int SSSP_CTA_TH = 512;
-#ifndef MG_SSSP_DYNAMIC
-#define MG_SSSP_DYNAMIC 1
-#endif
+constexpr int SSSP_CH = 256;  // edges per chunk of a heavy frontier vertex
+constexpr int SSSP_U = 4;     // edge slots of 32 a warp holds in flight
+constexpr int SSSP_WS = 128;  // next-frontier stage per warp (shared memory)
 
 struct SsspArgs {
   const int32_t *ro, *ci, *w;   // CSR with weights (w == nullptr: unit weights)
@@ -40,17 +39,55 @@ struct SsspArgs {
   int32_t qcap;
   int32_t both;
   int64_t n;
-  int32_t *big_v;  // grid-strided bin (BIG_CAP entries)
+  int2 *chunks;      // {item, first edge | 1 << 31 for a CSC edge} of the heavy vertices' chunks
+  int32_t chunk_cap;
+  int32_t heavy;        // out-degree from which a frontier vertex is cut into chunks
+  int32_t heavy_small;  // the same for a frontier of fewer vertices than the grid has lanes
   int32_t vmask;   // item -> vertex mask: -1 for one instance; batched runs keep the
                    // instance number in the bits above it (item = instance << s | v)
   int32_t delta;   // near-far bucket width (0: plain frontier Bellman-Ford)
-  int32_t stage;   // stage next-frontier appends per CTA (sparse graphs)
   int32_t *far0, *far1;  // far piles (ping-pong)
   uint32_t *infar;       // bit per item: in the current far pile
   DevCtl *ctl;
   cudaGraphConditionalHandle h;
   int32_t use_cond;
 };
+
+// Per-warp staging of next-frontier appends in shared memory: one global atomic
+// per SSSP_WS items instead of one per warp-wide append (a round of R-MAT s22 adds
+// two million vertices to one queue).
+struct WarpStage {
+  int32_t *buf;
+  int32_t n;  // entries held (the same in every lane)
+};
+
+// Every lane of the warp calls it.
+__device__ __forceinline__ void ws_flush(WarpStage &st, int32_t *queue, int32_t *len, int32_t cap,
+                                         int32_t *overflow) {
+  __syncwarp();
+  if (st.n == 0) return;
+  int32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(len, st.n);
+  base = __shfl_sync(FULL, base, 0);
+  for (int32_t i = lane_id(); i < st.n; i += 32) {
+    const int32_t pos = base + i;
+    if (pos < cap) queue[pos] = st.buf[i];
+    else *overflow = 1;
+  }
+  __syncwarp();
+  st.n = 0;
+}
+
+// Appends item where pred; every lane of the warp calls it.
+__device__ __forceinline__ void ws_push(WarpStage &st, bool pred, int32_t item, int32_t *queue, int32_t *len,
+                                        int32_t cap, int32_t *overflow) {
+  const unsigned pm = __ballot_sync(FULL, pred);
+  if (pm == 0) return;
+  const int32_t cnt = __popc(pm);
+  if (st.n + cnt > SSSP_WS) ws_flush(st, queue, len, cap, overflow);
+  if (pred) st.buf[st.n + __popc(pm & lanemask_lt())] = item;
+  st.n += cnt;
+}
 
 struct RelaxCtx {
   int32_t *dist;
@@ -66,36 +103,116 @@ struct RelaxCtx {
   int64_t thr;
   uint32_t *infar;
   int32_t *far_out, *far_len_out;
-  BlockQueue *bq = nullptr;  // staging of the next frontier (nullptr: straight to the queue)
 };
 
-// Relaxes edge (v, u) of weight w, dv = dist[v] as read when v was expanded.
-__device__ __forceinline__ void relax_d(RelaxCtx &x, int32_t dv, int32_t u, int32_t w) {
-  const int64_t nd64 = (int64_t)dv + (int64_t)w;
-  bool push = false, far = false;
-  if (nd64 < (int64_t)vload(x.dist + u)) {
-    const int32_t nd = (int32_t)nd64;
-    const int32_t old = atomicMin(x.dist + u, nd);
-    if (nd < old) {
-      x.updates++;
-      if (old == INT_MAX) x.reach_deg += x.ro[(u & x.vmask) + 1] - x.ro[u & x.vmask];
-      const uint32_t bit = 1u << (u & 31);
-      if (x.delta <= 0 || (int64_t)nd < x.thr) push = !(atomicOr(x.inq_next + (u >> 5), bit) & bit);
-      else far = !(atomicOr(x.infar + (u >> 5), bit) & bit);
-    }
+// Relaxes SSSP_U edges per lane: edge r goes to item u[r] (-1: none) with weight
+// w[r] from a vertex at distance dv[r]. The loads, the atomicMins and the bitmap
+// claims of the SSSP_U edges are each issued together, so a lane waits for one
+// memory round trip per step rather than per edge. Every lane of the warp calls it.
+__device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const int32_t (&u)[SSSP_U],
+                                            const int32_t (&w)[SSSP_U], const int32_t (&dv)[SSSP_U]) {
+  int32_t cd[SSSP_U], nd[SSSP_U], old[SSSP_U];
+  bool tr[SSSP_U];
+#pragma unroll
+  for (int r = 0; r < SSSP_U; r++) cd[r] = u[r] >= 0 ? __ldcg(x.dist + u[r]) : INT_MIN;
+#pragma unroll
+  for (int r = 0; r < SSSP_U; r++) {
+    const int64_t s = (int64_t)dv[r] + (int64_t)w[r];
+    tr[r] = u[r] >= 0 && s < (int64_t)cd[r];
+    nd[r] = (int32_t)min(s, (int64_t)INT_MAX);
   }
-  staged_append(x.bq, push, u, x.qout, x.qlen_out, x.qcap, x.overflow);
-  if (x.delta > 0) warp_append(far, u, x.far_out, x.far_len_out, x.qcap, x.overflow);
-}
-
-__device__ __forceinline__ void relax(RelaxCtx &x, int32_t v, int32_t u, int32_t w) {
-  relax_d(x, vload(x.dist + v), u, w);
+#pragma unroll
+  for (int r = 0; r < SSSP_U; r++) old[r] = tr[r] ? atomicMin(x.dist + u[r], nd[r]) : INT_MIN;
+  uint32_t ob[SSSP_U];
+  bool nearq[SSSP_U];
+#pragma unroll
+  for (int r = 0; r < SSSP_U; r++) {
+    const bool win = tr[r] && nd[r] < old[r];
+    nearq[r] = x.delta <= 0 || (int64_t)nd[r] < x.thr;
+    ob[r] = 0xffffffffu;  // no claim: reads as "already queued"
+    if (win) ob[r] = atomicOr((nearq[r] ? x.inq_next : x.infar) + (u[r] >> 5), 1u << (u[r] & 31));
+  }
+#pragma unroll
+  for (int r = 0; r < SSSP_U; r++) {
+    if (tr[r] && nd[r] < old[r]) {
+      x.updates++;
+      if (old[r] == INT_MAX) x.reach_deg += x.ro[(u[r] & x.vmask) + 1] - x.ro[u[r] & x.vmask];
+    }
+    const bool fresh = u[r] >= 0 && !(ob[r] & (1u << (u[r] & 31)));
+    ws_push(st, fresh && nearq[r], u[r], x.qout, x.qlen_out, x.qcap, x.overflow);
+    if (x.delta > 0) warp_append(fresh && !nearq[r], u[r], x.far_out, x.far_len_out, x.qcap, x.overflow);
+  }
 }
 
 __device__ __forceinline__ RelaxCtx relax_ctx(const SsspArgs &a, DevCtl *c, int cur) {
   const int fc = a.delta > 0 ? vload(&c->far_cur) : 0;
   return RelaxCtx{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap,
                   a.vmask, 0, 0, a.delta, vload(&c->thr), a.infar, fc ? a.far1 : a.far0, &c->far_len[fc]};
+}
+
+// The edges of the warp's 32 vertices (lane l brings vertex item v, its distance
+// dv, its first edge beg and deg edges), concatenated and walked 32 x SSSP_U at a
+// time: edge slot j belongs to the last lane whose exclusive degree prefix is <= j
+// (binary search over the lanes' prefixes by shuffles).
+__device__ __forceinline__ void warp_walk(RelaxCtx &x, WarpStage &st, int32_t v, int32_t dv, int32_t beg,
+                                          int32_t deg, const int32_t *__restrict__ adj,
+                                          const int32_t *__restrict__ wt, int32_t hi) {
+  const int lane = lane_id();
+  const int32_t inc = warp_inclusive_scan(deg);
+  const int32_t tot = __shfl_sync(FULL, inc, 31);
+  const int32_t ex = inc - deg;
+  const int32_t kb = beg - ex;  // edge index of slot j of this lane's vertex: kb + j
+  for (int32_t b0 = 0; b0 < tot; b0 += 32 * SSSP_U) {
+    int32_t u[SSSP_U], w[SSSP_U], d[SSSP_U];
+#pragma unroll
+    for (int r = 0; r < SSSP_U; r++) {
+      const int32_t j = b0 + r * 32 + lane;
+      int l = 0;
+#pragma unroll
+      for (int sft = 16; sft > 0; sft >>= 1)
+        if (__shfl_sync(FULL, ex, l + sft) <= j) l += sft;
+      const int32_t k = __shfl_sync(FULL, kb, l) + j;
+      const int32_t sv = __shfl_sync(FULL, v, l);
+      d[r] = __shfl_sync(FULL, dv, l);
+      const bool ok = j < tot;
+      u[r] = ok ? ((sv & hi) | adj[k]) : -1;
+      w[r] = ok ? (wt ? wt[k] : 1) : 0;
+    }
+    relax_group(x, st, u, w, d);
+  }
+}
+
+// Cuts the lanes' vertices of at least `th` edges into chunks of SSSP_CH edges and
+// appends them to the chunk list ({item, first edge | flag}); returns the number
+// of edges this lane still has to walk itself (0 when chunked). A warp whose chunks
+// do not fit walks all its vertices (the slots it took are marked empty).
+__device__ __forceinline__ int32_t warp_chunks(const SsspArgs &a, int32_t *clen, int32_t v, int32_t beg,
+                                               int32_t deg, int32_t th, int32_t flag) {
+  const int lane = lane_id();
+  const int32_t nch = (v >= 0 && deg >= th) ? (deg + SSSP_CH - 1) / SSSP_CH : 0;
+  const int32_t inc = warp_inclusive_scan(nch);
+  const int32_t tot = __shfl_sync(FULL, inc, 31);
+  if (tot == 0) return deg;
+  int32_t base = 0;
+  if (lane == 0) base = atomicAdd(clen, tot);
+  base = __shfl_sync(FULL, base, 0);
+  const int32_t ex = inc - nch;
+  if (base + tot > a.chunk_cap) {
+    for (int32_t j = base + lane; j < a.chunk_cap; j += 32) a.chunks[j] = make_int2(-1, 0);
+    return deg;
+  }
+  for (int32_t j0 = 0; j0 < tot; j0 += 32) {
+    const int32_t j = j0 + lane;
+    int l = 0;
+#pragma unroll
+    for (int sft = 16; sft > 0; sft >>= 1)
+      if (__shfl_sync(FULL, ex, l + sft) <= j) l += sft;
+    const int32_t sv = __shfl_sync(FULL, v, l);
+    const int32_t sb = __shfl_sync(FULL, beg, l);
+    const int32_t se = __shfl_sync(FULL, ex, l);
+    if (j < tot) a.chunks[base + j] = make_int2(sv, (sb + (j - se) * SSSP_CH) | flag);
+  }
+  return nch ? 0 : deg;
 }
 
 __device__ void sssp_level_end(const SsspArgs &a) {
@@ -125,61 +242,13 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
 }
 
-__global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
-  __shared__ ExpandSmem<SSSP_NT> sm;
-  __shared__ BlockQueue bq;
-  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
-  DevCtl *c = a.ctl;
-  if (vload(&c->done)) {
-    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
-    return;
-  }
-  const int cur = vload(&c->cur);
-  const int32_t nin = vload(&c->qlen[cur]);  // relaxations below read dist[v] once per vertex
-  const int32_t *qin = cur ? a.q1 : a.q0;
-  uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
-  RelaxCtx x = relax_ctx(a, c, cur);
-  bq_init(bq);
-  if (a.stage) x.bq = &bq;
-  const int32_t hi = ~a.vmask;  // instance bits of an item
-  int64_t insp = 0, nexp = 0;
-  const int32_t *ci = a.ci, *w = a.w, *ri = a.ri, *cw = a.cw;
-  const BigList big{a.big_v, &c->big_len, defer_threshold<SSSP_NT>(nin, SSSP_CTA_TH)};
-#if MG_SSSP_DYNAMIC
-  // Tiles of the frontier are handed out one at a time from a counter (reset at
-  // the end of the round), so CTAs that drew light tiles take more.
-  __shared__ int32_t s_tile;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&c->tile_next, 1);
-    __syncthreads();
-    const int64_t tile = (int64_t)s_tile * SSSP_NT;
-    __syncthreads();
-    if (tile >= nin) break;
-#else
-  for (int64_t tile = (int64_t)blockIdx.x * SSSP_NT; tile < nin; tile += (int64_t)gridDim.x * SSSP_NT) {
-#endif
-    const int64_t i = tile + threadIdx.x;
-    const int32_t v = i < nin ? qin[i] : -1;
-    if (v >= 0) {
-      // The whole bitmap of the current frontier is cleared here, one word at a
-      // time: nothing sets bits in it during this level.
-      inq_cur[v >> 5] = 0u;
-      nexp++;
-    }
-    const int32_t dv = v >= 0 ? vload(a.dist + v) : 0;
-    expand_tile_p<SSSP_NT, SSSP_CTA_TH>(sm, a.ro, v, dv, insp, [&](int32_t sv, int32_t d, int32_t k) {
-      relax_d(x, d, (sv & hi) | ci[k], w ? w[k] : 1);
-    }, &big, a.vmask);
-    if (a.both)
-      expand_tile_p<SSSP_NT, SSSP_CTA_TH>(sm, a.co, v, dv, insp, [&](int32_t sv, int32_t d, int32_t k) {
-        relax_d(x, d, (sv & hi) | ri[k], cw ? cw[k] : 1);
-      }, nullptr, a.vmask);
-  }
-  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
-  const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
+// Adds a block's counters to the control block.
+__device__ __forceinline__ void sssp_counters(DevCtl *c, int64_t *s_sum, int64_t reach, int64_t insp, int64_t nexp,
+                                              int64_t upd) {
+  const int64_t b0 = block_sum<SSSP_NT>(reach, s_sum);
   const int64_t b1 = block_sum<SSSP_NT>(insp, s_sum);
   const int64_t b2 = block_sum<SSSP_NT>(nexp, s_sum);
-  const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
+  const int64_t b3 = block_sum<SSSP_NT>(upd, s_sum);
   if (threadIdx.x == 0) {
     if (b0) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b0);
     if (b1) atomicAdd((unsigned long long *)&c->edges_inspected, (unsigned long long)b1);
@@ -188,10 +257,62 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
   }
 }
 
-// Grid-strided bin of a relaxation round; the last CTA closes the round.
-__global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
-  __shared__ BigSmem<SSSP_NT> sm;
-  __shared__ BlockQueue bq;
+// Relaxation round, pass 1: each warp takes 32 frontier items, cuts the heavy ones
+// into chunks for pass 2 and walks the edges of the others itself.
+__global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
+  __shared__ int32_t s_stage[SSSP_NT / 32][SSSP_WS];
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  uint32_t *inq_cur = cur ? a.inq1 : a.inq0;
+  RelaxCtx x = relax_ctx(a, c, cur);
+  WarpStage st{s_stage[warp_id()], 0};
+  const int32_t hi = ~a.vmask;  // instance bits of an item
+  const int64_t nw = (int64_t)gridDim.x * (SSSP_NT / 32);
+  const int64_t gw = (int64_t)blockIdx.x * (SSSP_NT / 32) + warp_id();
+  // A frontier of fewer vertices than the grid has lanes leaves most warps without
+  // a vertex of their own: hand every vertex of heavy_small edges or more to pass 2.
+  const int32_t th = (int64_t)nin < nw * 32 ? a.heavy_small : a.heavy;
+  int64_t insp = 0, nexp = 0;
+  for (int64_t base = gw * 32; base < nin; base += nw * 32) {
+    const int64_t i = base + lane_id();
+    const int32_t v = i < nin ? qin[i] : -1;
+    int32_t beg = 0, deg = 0, dv = 0, cb = 0, cdeg = 0;
+    if (v >= 0) {
+      // The whole bitmap of the current frontier is cleared here, one word at a
+      // time: nothing sets bits in it during this round.
+      inq_cur[v >> 5] = 0u;
+      nexp++;
+      beg = a.ro[v & a.vmask];
+      deg = a.ro[(v & a.vmask) + 1] - beg;
+      dv = vload(a.dist + v);
+      if (a.both) {
+        cb = a.co[v & a.vmask];
+        cdeg = a.co[(v & a.vmask) + 1] - cb;
+      }
+      insp += deg + cdeg;
+    }
+    deg = warp_chunks(a, &c->big_len, v, beg, deg, th, 0);
+    warp_walk(x, st, v, dv, beg, deg, a.ci, a.w, hi);
+    if (a.both) {
+      cdeg = warp_chunks(a, &c->big_len, v, cb, cdeg, th, INT_MIN);
+      warp_walk(x, st, v, dv, cb, cdeg, a.ri, a.cw, hi);
+    }
+  }
+  ws_flush(st, x.qout, x.qlen_out, x.qcap, x.overflow);
+  sssp_counters(c, s_sum, x.reach_deg, insp, nexp, x.updates);
+}
+
+// Pass 2: every warp of the grid relaxes chunks of the heavy vertices' edges; the
+// last CTA closes the round.
+__global__ void __launch_bounds__(SSSP_NT) sssp_chunk_kernel(SsspArgs a) {
+  __shared__ int32_t s_stage[SSSP_NT / 32][SSSP_WS];
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
   if (vload(&c->done)) {
@@ -200,19 +321,37 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_big_kernel(SsspArgs a) {
   }
   const int cur = vload(&c->cur);
   RelaxCtx x = relax_ctx(a, c, cur);
-  bq_init(bq);
-  if (a.stage) x.bq = &bq;
-  const int32_t hi = ~a.vmask;  // instance bits of an item
-  const int32_t *ci = a.ci, *w = a.w;
-  expand_big<SSSP_NT>(sm, a.ro, BigList{a.big_v, &c->big_len},
-                      [&](int32_t sv, int32_t k) { relax(x, sv, (sv & hi) | ci[k], w ? w[k] : 1); }, a.vmask);
-  bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
-  const int64_t b0 = block_sum<SSSP_NT>(x.reach_deg, s_sum);
-  const int64_t b3 = block_sum<SSSP_NT>(x.updates, s_sum);
-  if (threadIdx.x == 0) {
-    if (b0) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b0);
-    if (b3) atomicAdd((unsigned long long *)&c->vertices_updated, (unsigned long long)b3);
+  WarpStage st{s_stage[warp_id()], 0};
+  const int32_t hi = ~a.vmask;
+  const int lane = lane_id();
+  const int32_t nch = min(vload(&c->big_len), a.chunk_cap);
+  const int32_t nw = gridDim.x * (SSSP_NT / 32);
+  for (int32_t ch = blockIdx.x * (SSSP_NT / 32) + warp_id(); ch < nch; ch += nw) {
+    const int2 e = a.chunks[ch];
+    if (e.x < 0) continue;
+    const bool rev = e.y < 0;
+    const int32_t k0 = e.y & INT_MAX;
+    const int32_t *off = rev ? a.co : a.ro;
+    const int32_t *adj = rev ? a.ri : a.ci;
+    const int32_t *wt = rev ? a.cw : a.w;
+    const int32_t end = min(k0 + SSSP_CH, off[(e.x & a.vmask) + 1]);
+    const int32_t dv = vload(a.dist + e.x);
+    const int32_t base = e.x & hi;
+    for (int32_t b = k0; b < end; b += 32 * SSSP_U) {
+      int32_t u[SSSP_U], w[SSSP_U], d[SSSP_U];
+#pragma unroll
+      for (int r = 0; r < SSSP_U; r++) {
+        const int32_t k = b + r * 32 + lane;
+        const bool ok = k < end;
+        u[r] = ok ? (base | adj[k]) : -1;
+        w[r] = ok ? (wt ? wt[k] : 1) : 0;
+        d[r] = dv;
+      }
+      relax_group(x, st, u, w, d);
+    }
   }
+  ws_flush(st, x.qout, x.qlen_out, x.qcap, x.overflow);
+  sssp_counters(c, s_sum, x.reach_deg, 0, 0, x.updates);
   if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
 }
 
@@ -430,25 +569,37 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
     }
   }
   const size_t far_items = delta > 0 ? (size_t)qcap : 0;
+  // Chunk list: a round's heavy vertices hold at most (edges / SSSP_CH + vertices of
+  // heavy_small edges or more) chunks; each instance's frontier holds a vertex once,
+  // so its edges are at most m per direction. Past the capacity a warp walks its
+  // heavy vertices itself.
+  const mg_tuning &tn = g->tune;
+  const int32_t heavy = std::max(1, tn.sssp_heavy);
+  const int32_t heavy_small = std::max(1, std::min(tn.sssp_heavy_small, heavy));
+  const double inst = (double)nitems / (double)std::max<int64_t>(1, n);
+  const double dirs = both ? 2.0 : 1.0;
+  const double cbound = inst * dirs * (double)g->m * (1.0 / SSSP_CH + 1.0 / heavy) + 65536.0;
+  const int32_t chunk_cap = (int32_t)std::max(
+      1.0, std::min(cbound, tn.sssp_chunk_cap > 0 ? (double)tn.sssp_chunk_cap : (double)(1 << 23)));
   const size_t need = Carve::need({sizeof(uint32_t) * (size_t)nwords, sizeof(uint32_t) * (size_t)nwords,
                                    sizeof(int32_t) * (size_t)qcap, sizeof(int32_t) * (size_t)qcap,
-                                   sizeof(int32_t) * (size_t)nseed, sizeof(int32_t) * (size_t)BIG_CAP,
+                                   sizeof(int32_t) * (size_t)nseed, sizeof(int2) * (size_t)chunk_cap,
                                    sizeof(int32_t) * far_items, sizeof(int32_t) * far_items,
                                    sizeof(uint32_t) * (delta > 0 ? (size_t)nwords : 0)});
   MG_TRY(ws_reserve(g, g->ws_main, need));
   Carve cv(g->ws_main.ptr);
   SsspArgs a;
+  std::memset(&a, 0, sizeof(a));  // the loop-graph signature compares its bytes
   a.inq0 = cv.take<uint32_t>(nwords);
   a.inq1 = cv.take<uint32_t>(nwords);
   a.q0 = cv.take<int32_t>(qcap);
   a.q1 = cv.take<int32_t>(qcap);
   int32_t *dsrc = cv.take<int32_t>(nseed);
-  a.big_v = cv.take<int32_t>(BIG_CAP);
+  a.chunks = cv.take<int2>(chunk_cap);
+  a.chunk_cap = chunk_cap;
+  a.heavy = heavy;
+  a.heavy_small = heavy_small;
   a.delta = delta > 0 ? delta : 0;
-  // Per-CTA staging of the next frontier pays on sparse graphs (2048^2 lattice:
-  // 10.4 -> 9.7 ms) and costs on R-MAT (s22: 10.2 -> 11.1 ms, 64-source batch
-  // 413 -> 475 ms), where a CTA's improvements overflow the stage every round.
-  a.stage = g->m <= 8 * g->n ? 1 : 0;
   a.far0 = delta > 0 ? cv.take<int32_t>(far_items) : nullptr;
   a.far1 = delta > 0 ? cv.take<int32_t>(far_items) : nullptr;
   a.infar = delta > 0 ? cv.take<uint32_t>(nwords) : nullptr;
@@ -478,7 +629,7 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   sssp_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(dist, a.inq0, a.inq1, a.infar, nitems);
   sssp_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nseed, iter_cap);
   MG_CUDA_TRY(cudaGetLastError());
-  const int grid = g->num_sms * 4;
+  const int grid = g->num_sms * std::max(1, std::min(tn.sssp_ctas_per_sm, 8));
   struct Sig {
     SsspArgs a;
     int grid;
@@ -491,7 +642,7 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
     b.h = h;
     b.use_cond = use_cond;
     sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
-    sssp_relax_big_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    sssp_chunk_kernel<<<grid, SSSP_NT, 0, st>>>(b);
     if (b.delta > 0) {
       sssp_far_min_kernel<<<grid, SSSP_NT, 0, st>>>(b);
       sssp_far_split_kernel<<<grid, SSSP_NT, 0, st>>>(b);

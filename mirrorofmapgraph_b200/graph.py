@@ -203,6 +203,33 @@ class Graph:
             b["ns"] = b["time_ns"] - a["time_ns"]
         return out
 
+    @staticmethod
+    def default_tuning() -> dict:
+        """The default traversal tuning (mg_tuning_defaults); needs no device."""
+        t = L.MgTuning()
+        L.load().mg_tuning_defaults(C.byref(t))
+        return t.as_dict()
+
+    def tuning(self) -> dict:
+        """The graph's traversal tuning (mg_graph_get_tuning): thresholds and launch
+        shapes the traversal kernels read at every call."""
+        t = L.MgTuning()
+        _check(self._lib.mg_graph_get_tuning(self._h, C.byref(t)), "mg_graph_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, **fields) -> dict:
+        """Changes tuning fields by name (the others keep their values); returns the
+        new tuning. A value outside a field's range raises MapGraphError and
+        changes nothing."""
+        t = L.MgTuning()
+        _check(self._lib.mg_graph_get_tuning(self._h, C.byref(t)), "mg_graph_get_tuning")
+        for k, v in fields.items():
+            if k == "reserved" or k not in dict(L.MgTuning._fields_):
+                raise KeyError(f"unknown tuning field {k!r}")
+            setattr(t, k, int(v))
+        _check(self._lib.mg_graph_set_tuning(self._h, C.byref(t)), "mg_graph_set_tuning")
+        return t.as_dict()
+
     # -- helpers ----------------------------------------------------------------
     def _out(self, out, count, dtype):
         if out is None:

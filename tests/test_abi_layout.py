@@ -18,6 +18,7 @@ STRUCTS = {
     "mg_part_level": L.MgPartLevel,
     "mg_level_record": L.MgLevelRecord,
     "mg_host_csr": L.MgHostCsr,
+    "mg_tuning": L.MgTuning,
 }
 
 

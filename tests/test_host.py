@@ -63,6 +63,9 @@ def test_null_arguments_are_rejected():
     assert lib.mg_part_destroy(None) == L.MG_OK
     cnt = C.c_int32()
     assert lib.mg_graph_trace(None, None, 0, C.byref(cnt)) == L.MG_ERR_ARG
+    t = L.MgTuning()
+    assert lib.mg_graph_get_tuning(None, C.byref(t)) == L.MG_ERR_ARG
+    assert lib.mg_graph_set_tuning(None, C.byref(t)) == L.MG_ERR_ARG
     # fault-injection hooks: argument checks (arming them needs no device)
     assert lib.mg_debug_fail_alloc(-1) == L.MG_ERR_ARG
     assert lib.mg_debug_barrier_skew(-1, 10) == L.MG_ERR_ARG
@@ -232,3 +235,9 @@ def test_binary_csr_cache_round_trip_and_rejects_garbage(tmp_path):
     q.write_bytes(b"not a csr file at all")
     with pytest.raises(RuntimeError):
         mg.load_csr(str(q))
+
+
+def test_tuning_defaults_need_no_device():
+    d = mg.Graph.default_tuning()
+    assert d["sssp_heavy"] == 256 and d["sssp_heavy_small"] == 32 and d["sssp_ctas_per_sm"] == 4
+    assert d["sssp_chunk_cap"] == 0
