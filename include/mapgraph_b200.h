@@ -392,7 +392,9 @@ typedef struct mg_tuning {
   int32_t sssp_ctas_per_sm; /* CTAs of 256 threads per SM of the SSSP round kernels [4; 1 .. 8] */
   int32_t sssp_chunk_cap;   /* SSSP chunk list capacity in chunks; 0: the bound of the graph's edges (at most
                                2^23); past it a warp walks its heavy vertices itself [0; 0 .. 2^30] */
-  int32_t reserved[12];
+  int32_t sssp_batch_heavy; /* mg_sssp_batch (interleaved rows): frontier items of at least this many edges are cut
+                               into chunks of 128 edges for every warp of the grid [32; 1 .. 2^30] */
+  int32_t reserved[11];
 } mg_tuning;
 void mg_tuning_defaults(mg_tuning *t);
 mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t);

@@ -68,7 +68,7 @@ MG_TRACE_LEVELS = 4096
 
 class MgTuning(C.Structure):
     _fields_ = [("sssp_heavy", C.c_int32), ("sssp_heavy_small", C.c_int32), ("sssp_ctas_per_sm", C.c_int32),
-                ("sssp_chunk_cap", C.c_int32), ("reserved", C.c_int32 * 12)]
+                ("sssp_chunk_cap", C.c_int32), ("sssp_batch_heavy", C.c_int32), ("reserved", C.c_int32 * 11)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -33,4 +33,4 @@ mg_status fetch_ctl(mg_graph *g);
 
 // Cache slots.
 enum LoopSlot { SLOT_BFS = 0, SLOT_SSSP, SLOT_CC, SLOT_PR, SLOT_PR_REF, SLOT_ADJ, SLOT_MSBFS, SLOT_BSSSP, SLOT_PPR,
-                SLOT_COUNT };
+                SLOT_MSSSP, SLOT_COUNT };

@@ -87,7 +87,8 @@ extern "C" mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t) {
   } const r[] = {{"sssp_heavy", t->sssp_heavy, 1, 1 << 30},
                  {"sssp_heavy_small", t->sssp_heavy_small, 1, t->sssp_heavy},
                  {"sssp_ctas_per_sm", t->sssp_ctas_per_sm, 1, 8},
-                 {"sssp_chunk_cap", t->sssp_chunk_cap, 0, 1 << 30}};
+                 {"sssp_chunk_cap", t->sssp_chunk_cap, 0, 1 << 30},
+                 {"sssp_batch_heavy", t->sssp_batch_heavy, 1, 1 << 30}};
   for (const Range &x : r) {
     if (x.v < x.lo || x.v > x.hi) {
       mg_set_error("mg_graph_set_tuning: %s = %d outside [%d, %d]", x.name, x.v, x.lo, x.hi);

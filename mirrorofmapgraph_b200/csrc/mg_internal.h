@@ -96,6 +96,7 @@ inline mg_tuning tuning_defaults() {
   t.sssp_heavy = 256;
   t.sssp_heavy_small = 32;
   t.sssp_ctas_per_sm = 4;
+  t.sssp_batch_heavy = 32;
   return t;
 }
 

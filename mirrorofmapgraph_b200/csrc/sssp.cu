@@ -497,6 +497,351 @@ __global__ void min_i32_kernel(const int32_t *__restrict__ v, int64_t m, int *__
   }
 }
 
+// ---- Batched SSSP with interleaved distances -------------------------------
+// Up to 32 instances form a group: a vertex's 32 distances are one 128-byte row
+// (lane i of a warp holds instance i), and a 32-bit mask per row says which
+// instances improved the vertex in the last round. Frontier items are
+// (group, vertex) pairs, item = group << shift | vertex. A warp takes an item and
+// walks its edges once for every instance of the group: the instances active at
+// the item load their distance to the edge's head from one row, lower it with
+// atomicMin, and the warp ORs the ballot of the winners into the head's next mask;
+// the OR that finds the mask empty queues the head. Heavy items are cut into
+// chunks (carrying the mask) that every warp of the grid takes.
+constexpr int MSS_CH = 128;  // edges per chunk of a heavy item
+constexpr int MSS_U = 8;     // edges a warp holds in flight
+
+struct MssArgs {
+  const int32_t *ro, *ci, *w;   // CSR (w == nullptr: unit weights)
+  const int32_t *co, *ri, *cw;  // CSC (directed == 0 on an asymmetric graph)
+  int32_t *D;                   // rows of 32 distances, row (g, v) at g * n + v
+  uint32_t *m0, *m1;            // active-instance masks per row (ping-pong)
+  int32_t *q0, *q1;
+  int32_t qcap;
+  int4 *chunks;                 // {item, first edge | 1 << 31 for a CSC edge, mask, 0}
+  int32_t chunk_cap;
+  int32_t heavy;
+  int64_t n;
+  int32_t shift, vmask;
+  int32_t both;
+  DevCtl *ctl;
+  cudaGraphConditionalHandle h;
+  int32_t use_cond;
+};
+
+// Relaxes edges [k0, k1) of adj/wt from the vertex whose row this lane's instance
+// reads as dv (act: the lane's instance improved that vertex last round). An edge
+// that improves on the distance read before the atomicMin sets the instance's bit
+// in the head's next mask; neither atomic's old value is waited for (the frontier
+// is compacted from the masks after the round), so a warp keeps one memory round
+// trip per MSS_U edges. A bit set by an improvement that a concurrent smaller one
+// overtook only re-expands that vertex once more.
+//
+// The edges are staged MSS_CH at a time in the warp's shared buffer `se` as
+// (head, weight) pairs, read back two per 16-byte broadcast load; slots past the
+// end hold (0, INT_MAX), an edge that can never improve a distance. Inactive lanes
+// compare against 0. Every lane of the warp calls it with the same edge range.
+__device__ __forceinline__ void mss_edges(const MssArgs &a, int2 *se, uint32_t *mnext, int64_t gbase, bool act,
+                                          int32_t dv, const int32_t *__restrict__ adj,
+                                          const int32_t *__restrict__ wt, int32_t k0, int32_t k1, int64_t &updates) {
+  const int lane = lane_id();
+  int32_t *Dl = a.D + (gbase << 5) + lane;  // this lane's column of the group's rows
+  uint32_t *mg = mnext + gbase;
+  for (int32_t b = k0; b < k1; b += MSS_CH) {
+    const int32_t cnt = min(MSS_CH, k1 - b);
+#pragma unroll
+    for (int q = 0; q < MSS_CH / 32; q++) {
+      const int32_t j = q * 32 + lane;
+      se[j] = j < cnt ? make_int2(adj[b + j], wt ? wt[b + j] : 1) : make_int2(0, INT_MAX);
+    }
+    __syncwarp();
+    for (int32_t e0 = 0; e0 < cnt; e0 += MSS_U) {
+      int32_t u[MSS_U], w[MSS_U], cu[MSS_U];
+#pragma unroll
+      for (int r = 0; r < MSS_U; r += 2) {
+        const int4 p = *reinterpret_cast<const int4 *>(se + e0 + r);
+        u[r] = p.x;
+        w[r] = p.y;
+        u[r + 1] = p.z;
+        w[r + 1] = p.w;
+      }
+#pragma unroll
+      for (int r = 0; r < MSS_U; r++) cu[r] = act ? __ldcg(Dl + ((uint32_t)u[r] << 5)) : 0;
+      uint32_t myb = 0;
+      int32_t myv = 0;
+#pragma unroll
+      for (int r = 0; r < MSS_U; r++) {
+        const int32_t nd = (int32_t)min((uint32_t)dv + (uint32_t)w[r], (uint32_t)INT_MAX);
+        const bool tr = nd < cu[r];
+        if (tr) atomicMin(Dl + ((uint32_t)u[r] << 5), nd);
+        const uint32_t bits = __ballot_sync(FULL, tr);
+        if (lane == r) {
+          myb = bits;
+          myv = u[r];
+        }
+      }
+      if (myb) {
+        updates += __popc(myb);
+        atomicOr(mg + myv, myb);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+__device__ void mss_level_end(const MssArgs &a) {
+  DevCtl *c = a.ctl;
+  const int cur = vload(&c->cur);
+  const int32_t nf = vload(&c->qlen[cur ^ 1]);
+  const int lvl = vload(&c->level) + 1;
+  trace_level(c, lvl - 1, MG_DIR_PUSH, vload(&c->qlen[cur]), 0, 0.0);
+  c->level = lvl;
+  c->qlen[cur] = 0;
+  c->cur = cur ^ 1;
+  c->blocks_done = 0;
+  c->big_len = 0;
+  const bool over = vload(&c->overflow) != 0;
+  const bool done = nf == 0 || lvl >= c->iter_cap || over;
+  if (over) c->status = MG_ERR_QUEUE_OVERFLOW;
+  __threadfence();
+  c->done = done ? 1 : 0;
+  if (a.use_cond) cudaGraphSetConditional(a.h, done ? 0u : 1u);
+}
+
+// Pass 1: each warp reads 32 frontier items' headers (one per lane), cuts the
+// heavy ones into chunks and walks the others item by item.
+__global__ void __launch_bounds__(SSSP_NT) mss_relax_kernel(MssArgs a) {
+  __shared__ __align__(16) int2 s_edges[SSSP_NT / 32][MSS_CH + MSS_U];
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const int32_t nin = vload(&c->qlen[cur]);
+  const int32_t *qin = cur ? a.q1 : a.q0;
+  uint32_t *mcur = cur ? a.m1 : a.m0, *mnext = cur ? a.m0 : a.m1;
+  const int lane = lane_id();
+  const int64_t nw = (int64_t)gridDim.x * (SSSP_NT / 32);
+  int64_t insp = 0, nexp = 0, upd = 0;
+  for (int64_t base = ((int64_t)blockIdx.x * (SSSP_NT / 32) + warp_id()) * 32; base < nin; base += nw * 32) {
+    const int64_t i = base + lane;
+    const int32_t it = i < nin ? qin[i] : -1;
+    int64_t row = 0;
+    uint32_t mask = 0;
+    int32_t beg = 0, deg = 0, cb = 0, cdeg = 0;
+    if (it >= 0) {
+      const int32_t v = it & a.vmask;
+      row = (int64_t)(it >> a.shift) * a.n + v;
+      mask = mcur[row];
+      mcur[row] = 0u;  // this array collects the round after next; nothing else writes it now
+      beg = a.ro[v];
+      deg = a.ro[v + 1] - beg;
+      if (a.both) {
+        cb = a.co[v];
+        cdeg = a.co[v + 1] - cb;
+      }
+      insp += deg + cdeg;
+      nexp++;
+    }
+    // heavy items: chunks for pass 2, forward then reverse edges
+    for (int dir = 0; dir < (a.both ? 2 : 1); dir++) {
+      const int32_t db = dir ? cb : beg, dd = dir ? cdeg : deg;
+      const int32_t nch = (it >= 0 && dd >= a.heavy) ? (dd + MSS_CH - 1) / MSS_CH : 0;
+      const int32_t inc = warp_inclusive_scan(nch);
+      const int32_t tot = __shfl_sync(FULL, inc, 31);
+      if (tot == 0) continue;
+      int32_t cbase = 0;
+      if (lane == 0) cbase = atomicAdd(&c->big_len, tot);
+      cbase = __shfl_sync(FULL, cbase, 0);
+      if (cbase + tot > a.chunk_cap) {  // no room: this warp walks its heavy items itself
+        for (int32_t j = cbase + lane; j < a.chunk_cap; j += 32) a.chunks[j] = make_int4(-1, 0, 0, 0);
+        continue;
+      }
+      const int32_t ex = inc - nch;
+      for (int32_t j0 = 0; j0 < tot; j0 += 32) {
+        const int32_t j = j0 + lane;
+        int l = 0;
+#pragma unroll
+        for (int sft = 16; sft > 0; sft >>= 1)
+          if (__shfl_sync(FULL, ex, l + sft) <= j) l += sft;
+        const int32_t sit = __shfl_sync(FULL, it, l);
+        const int32_t sb = __shfl_sync(FULL, db, l);
+        const int32_t se = __shfl_sync(FULL, ex, l);
+        const uint32_t sm = __shfl_sync(FULL, mask, l);
+        if (j < tot) a.chunks[cbase + j] = make_int4(sit, (sb + (j - se) * MSS_CH) | (dir ? INT_MIN : 0), (int)sm, 0);
+      }
+      if (nch) {
+        if (dir) cdeg = 0;
+        else deg = 0;
+      }
+    }
+    // light items, one at a time by the whole warp
+    unsigned todo = __ballot_sync(FULL, deg + cdeg > 0);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int32_t sit = __shfl_sync(FULL, it, j);
+      const int64_t srow = __shfl_sync(FULL, row, j);
+      const uint32_t sm = __shfl_sync(FULL, mask, j);
+      const int64_t gbase = (int64_t)(sit >> a.shift) * a.n;
+      const bool act = (sm >> lane) & 1u;
+      const int32_t dv = act ? __ldcg(a.D + (srow << 5) + lane) : INT_MAX;
+      const int32_t sb = __shfl_sync(FULL, beg, j), sd = __shfl_sync(FULL, deg, j);
+      int2 *se = s_edges[warp_id()];
+      if (sd) mss_edges(a, se, mnext, gbase, act, dv, a.ci, a.w, sb, sb + sd, upd);
+      if (a.both) {
+        const int32_t scb = __shfl_sync(FULL, cb, j), scd = __shfl_sync(FULL, cdeg, j);
+        if (scd) mss_edges(a, se, mnext, gbase, act, dv, a.ri, a.cw, scb, scb + scd, upd);
+      }
+    }
+  }
+  sssp_counters(c, s_sum, 0, insp, nexp, upd);
+}
+
+// Pass 2: chunks of the heavy items, a warp per chunk.
+__global__ void __launch_bounds__(SSSP_NT) mss_chunk_kernel(MssArgs a) {
+  __shared__ __align__(16) int2 s_edges[SSSP_NT / 32][MSS_CH + MSS_U];
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  uint32_t *mnext = cur ? a.m0 : a.m1;
+  const int lane = lane_id();
+  int64_t upd = 0;
+  const int32_t nch = min(vload(&c->big_len), a.chunk_cap);
+  const int32_t nw = gridDim.x * (SSSP_NT / 32);
+  for (int32_t ch = blockIdx.x * (SSSP_NT / 32) + warp_id(); ch < nch; ch += nw) {
+    const int4 e = a.chunks[ch];
+    if (e.x < 0) continue;
+    const bool rev = e.y < 0;
+    const int32_t k0 = e.y & INT_MAX;
+    const int32_t v = e.x & a.vmask;
+    const int64_t gbase = (int64_t)(e.x >> a.shift) * a.n;
+    const int32_t *off = rev ? a.co : a.ro;
+    const int32_t end = min(k0 + MSS_CH, off[v + 1]);
+    const bool act = ((uint32_t)e.z >> lane) & 1u;
+    const int32_t dv = act ? __ldcg(a.D + ((gbase + v) << 5) + lane) : INT_MAX;
+    mss_edges(a, s_edges[warp_id()], mnext, gbase, act, dv, rev ? a.ri : a.ci, rev ? a.cw : a.w, k0, end, upd);
+  }
+  sssp_counters(c, s_sum, 0, 0, 0, upd);
+}
+
+// Pass 3: the next frontier, compacted in row order from the masks the round set
+// (rows of MSS_CT consecutive masks per tile, one queue atomic per tile); the last
+// CTA ends the round.
+constexpr int MSS_CT = SSSP_NT * 4;
+__global__ void __launch_bounds__(SSSP_NT) mss_compact_kernel(MssArgs a, int64_t rows) {
+  __shared__ int32_t s_red[SSSP_NT / 32 + 1];
+  __shared__ int32_t s_base;
+  DevCtl *c = a.ctl;
+  if (vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  const uint32_t *mnext = cur ? a.m0 : a.m1;
+  int32_t *qout = cur ? a.q0 : a.q1;
+  int32_t *qlen = &c->qlen[cur ^ 1];
+  for (int64_t t0 = (int64_t)blockIdx.x * MSS_CT; t0 < rows; t0 += (int64_t)gridDim.x * MSS_CT) {
+    const int64_t r0 = t0 + (int64_t)threadIdx.x * 4;
+    uint32_t mk[4] = {0u, 0u, 0u, 0u};
+    if (r0 + 3 < rows) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(mnext + r0);
+      mk[0] = q.x;
+      mk[1] = q.y;
+      mk[2] = q.z;
+      mk[3] = q.w;
+    } else {
+      for (int k = 0; k < 4; k++)
+        if (r0 + k < rows) mk[k] = mnext[r0 + k];
+    }
+    const int32_t cnt = (mk[0] != 0u) + (mk[1] != 0u) + (mk[2] != 0u) + (mk[3] != 0u);
+    int32_t tot;
+    int32_t ex = block_exclusive_scan<SSSP_NT>(cnt, s_red, &tot);
+    if (threadIdx.x == 0) s_base = tot ? atomicAdd(qlen, tot) : 0;
+    __syncthreads();
+    ex += s_base;
+    for (int k = 0; k < 4; k++) {
+      if (mk[k] == 0u) continue;
+      const int64_t row = r0 + k;
+      const int32_t g = (int32_t)(row / a.n);
+      const int32_t v = (int32_t)(row - (int64_t)g * a.n);
+      if (ex < a.qcap) qout[ex] = (g << a.shift) | v;
+      else c->overflow = 1;
+      ex++;
+    }
+    __syncthreads();
+  }
+  if (last_block(&c->blocks_done) && threadIdx.x == 0) mss_level_end(a);
+}
+
+// Rows := INT_MAX, masks := 0.
+__global__ void mss_clear_kernel(MssArgs a, int64_t rows) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows * 32; i += stride) {
+    a.D[i] = INT_MAX;
+    if (i < rows) {
+      a.m0[i] = 0u;
+      a.m1[i] = 0u;
+    }
+  }
+}
+
+// Instance i (group i / 32, lane i % 32) starts at srcs[i]; items of equal
+// (group, vertex) share a queue entry.
+__global__ void mss_seed_kernel(MssArgs a, const int32_t *srcs, int32_t nsrc, int32_t iter_cap) {
+  DevCtl *c = a.ctl;
+  for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
+    const int32_t s = srcs[i];
+    const int32_t g = i >> 5;
+    const int64_t row = (int64_t)g * a.n + s;
+    a.D[(row << 5) + (i & 31)] = 0;
+    if (atomicOr(a.m0 + row, 1u << (i & 31)) == 0u) {
+      const int pos = atomicAdd(&c->qlen[0], 1);
+      if (pos < a.qcap) a.q0[pos] = (g << a.shift) | s;
+      else c->overflow = 1;
+    }
+  }
+  if (threadIdx.x == 0) {
+    c->iter_cap = iter_cap;
+    c->done = c->overflow ? 1 : 0;
+    if (c->overflow) c->status = MG_ERR_QUEUE_OVERFLOW;
+  }
+}
+
+// Rows -> nsrc x n distance rows (a 32 x 32 transpose per block of 32 vertices
+// and one group), and the TEPS numerator: out-degrees of every instance's reached
+// vertices.
+__global__ void __launch_bounds__(1024) mss_unpack_kernel(MssArgs a, int32_t *dist, int32_t nsrc, int32_t groups) {
+  __shared__ int32_t t[32][33];
+  __shared__ int64_t s_sum[1024 / 32 + 1];
+  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+  const int64_t vtiles = (a.n + 31) >> 5;
+  int64_t reach = 0;
+  for (int64_t tile = blockIdx.x; tile < vtiles * groups; tile += gridDim.x) {
+    const int32_t g = (int32_t)(tile / vtiles);
+    const int64_t v0 = (tile % vtiles) << 5;
+    const int64_t v = v0 + wy;
+    __syncthreads();
+    t[wy][lane] = v < a.n ? a.D[(((int64_t)g * a.n + v) << 5) + lane] : INT_MAX;
+    __syncthreads();
+    // thread (wy, lane): instance g * 32 + wy, vertex v0 + lane
+    const int32_t inst = g * 32 + wy;
+    const int64_t vv = v0 + lane;
+    if (inst < nsrc && vv < a.n) {
+      const int32_t d = t[lane][wy];
+      dist[(int64_t)inst * a.n + vv] = d;
+      if (d != INT_MAX) reach += a.ro[vv + 1] - a.ro[vv];
+    }
+  }
+  const int64_t b = block_sum<1024>(reach, s_sum);
+  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&a.ctl->visited_deg, (unsigned long long)b);
+}
+
 }  // namespace mg
 
 // Checks once per graph that int32 weights are non-negative (cached).
@@ -705,6 +1050,108 @@ extern "C" mg_status mg_sssp(mg_graph *g, const int32_t *srcs, int32_t nsrc, int
   return MG_OK;
 }
 
+// Batched plain Bellman-Ford over interleaved distance rows (mss_* kernels) into
+// `dist` (device, nsrc x n).
+static mg_status msssp_run(mg_graph *g, const int32_t *srcs, int32_t nsrc, int32_t *dist, const mg_opts &o,
+                           mg_stats *stats) {
+  using namespace mg;
+  const bool symmetric = (g->flags & MG_GRAPH_SYMMETRIC) != 0;
+  const bool both = o.directed == 0 && !symmetric;
+  const int64_t n = g->n;
+  const int32_t groups = (nsrc + 31) / 32;
+  int shift = 0;
+  while ((int64_t(1) << shift) < n) shift++;
+  if ((int64_t)groups << shift > (int64_t)INT_MAX + 1) {
+    mg_set_error("mg_sssp_batch: %d groups of 32 sources over %lld vertices exceed 2^31 frontier items; split the "
+                 "sources", groups, (long long)n);
+    return MG_ERR_ARG;
+  }
+  const int64_t rows = (int64_t)groups * n;
+  const mg_tuning &tn = g->tune;
+  const int32_t heavy = std::max(1, tn.sssp_batch_heavy);
+  const double cbound = groups * (both ? 2.0 : 1.0) * (double)g->m * (1.0 / MSS_CH + 1.0 / heavy) + 65536.0;
+  const int32_t chunk_cap = (int32_t)std::max(
+      1.0, std::min(cbound, tn.sssp_chunk_cap > 0 ? (double)tn.sssp_chunk_cap : (double)(1 << 23)));
+  const size_t need = Carve::need({sizeof(int32_t) * 32 * (size_t)rows, sizeof(uint32_t) * (size_t)rows,
+                                   sizeof(uint32_t) * (size_t)rows, sizeof(int32_t) * (size_t)rows,
+                                   sizeof(int32_t) * (size_t)rows, sizeof(int4) * (size_t)chunk_cap,
+                                   sizeof(int32_t) * (size_t)nsrc});
+  MG_TRY(ws_reserve(g, g->ws_main, need));
+  Carve cv(g->ws_main.ptr);
+  MssArgs a;
+  std::memset(&a, 0, sizeof(a));  // the loop-graph signature compares its bytes
+  a.D = cv.take<int32_t>(32 * (size_t)rows);
+  a.m0 = cv.take<uint32_t>(rows);
+  a.m1 = cv.take<uint32_t>(rows);
+  a.q0 = cv.take<int32_t>(rows);
+  a.q1 = cv.take<int32_t>(rows);
+  a.chunks = cv.take<int4>(chunk_cap);
+  int32_t *dsrc = cv.take<int32_t>(nsrc);
+  a.qcap = (int32_t)std::min<int64_t>(rows, INT_MAX);
+  a.chunk_cap = chunk_cap;
+  a.heavy = heavy;
+  a.ro = g->ro;
+  a.ci = g->ci;
+  a.w = g->vtype == MG_DTYPE_I32 ? (const int32_t *)g->vals : nullptr;
+  a.co = g->has_csc ? g->co : g->ro;
+  a.ri = g->has_csc ? g->ri : g->ci;
+  a.cw = g->vtype == MG_DTYPE_I32 ? (const int32_t *)(g->has_csc ? g->cvals : g->vals) : nullptr;
+  a.n = n;
+  a.shift = shift;
+  a.vmask = (int32_t)((int64_t(1) << shift) - 1);
+  a.both = both ? 1 : 0;
+  a.ctl = g->ctl;
+  cudaStream_t s = g->stream;
+  MG_CUDA_TRY(cudaMemcpyAsync(dsrc, srcs, sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  MG_CUDA_TRY(cudaEventRecord(g->ev0, s));
+  MG_CUDA_TRY(cudaMemsetAsync(g->ctl, 0, sizeof(DevCtl), s));
+  mss_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(a, rows);
+  mss_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, (int32_t)std::min<int64_t>(n + 1, INT_MAX));
+  MG_CUDA_TRY(cudaGetLastError());
+  const int grid = g->num_sms * std::max(1, std::min(tn.sssp_ctas_per_sm, 8));
+  struct Sig {
+    MssArgs a;
+    int grid;
+  } sig;
+  std::memset(&sig, 0, sizeof(sig));
+  sig.a = a;
+  sig.grid = grid;
+  const int cgrid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + MSS_CT - 1) / MSS_CT, g->num_sms * 8));
+  LoopBody body = [a, grid, cgrid, rows](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+    MssArgs b = a;
+    b.h = h;
+    b.use_cond = use_cond;
+    mss_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    mss_chunk_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    mss_compact_kernel<<<cgrid, SSSP_NT, 0, st>>>(b, rows);
+  };
+  MG_TRY(run_loop(g, SLOT_MSSSP, &sig, sizeof(sig), o.use_graph >= 0, body, n + 3));
+  mss_unpack_kernel<<<g->num_sms * 2, 1024, 0, s>>>(a, dist, nsrc, groups);
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
+  MG_TRY(fetch_ctl(g));
+  const DevCtl &hc = *g->ctl_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->iterations = hc.level;
+    stats->edges_traversed = hc.visited_deg;
+    stats->edges_inspected = hc.edges_inspected;
+    // per inspected edge: its index and weight, one row read; per expanded item:
+    // its mask and offsets; the rows written back once
+    stats->bytes_compulsory = (a.w ? 8 : 4) * hc.edges_inspected + 16 * hc.vertices_expanded +
+                              128 * hc.vertices_expanded + 4 * (int64_t)nsrc * n;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->kernel_ms = ms;
+    stats->launches = 3 + (o.use_graph >= 0 ? 4 * (int64_t)hc.body_iters : 3 * (int64_t)hc.level);
+  }
+  if (hc.status != 0) {
+    mg_set_error("mg_sssp_batch: device status %d", hc.status);
+    return (mg_status)hc.status;
+  }
+  return MG_OK;
+}
+
 // nsrc independent single-source runs in one device run (no reference
 // counterpart; the reference loops the engine per source,
 // Algorithms/BFS/bfs.cu:442-456). Instance i relaxes items i << s | v, with
@@ -723,6 +1170,23 @@ extern "C" mg_status mg_sssp_batch(mg_graph *g, const int32_t *srcs, int32_t nsr
   if (o.device_output) MG_TRY(check_device_ptr(g, dist, "mg_sssp_batch", "dist"));
   MG_TRY(sssp_check(g, srcs, nsrc, o, "mg_sssp_batch"));
   const int64_t n = g->n;
+  // Plain unbounded rounds on graphs where a single run would take them too (mean
+  // out-degree above 8, or delta < 0): interleaved distance rows, one edge read for
+  // up to 32 instances. Near-far and capped runs: one item per instance and vertex.
+  const bool interleaved = o.iter_num <= 0 && n > 0 && (o.delta < 0 || (o.delta == 0 && g->m > 8 * n));
+  if (interleaved) {
+    int32_t *out = dist;
+    if (!o.device_output) {
+      MG_TRY(ws_reserve(g, g->ws_out, sizeof(int32_t) * (size_t)nsrc * (size_t)n + 256));
+      out = (int32_t *)g->ws_out.ptr;
+    }
+    MG_TRY(msssp_run(g, srcs, nsrc, out, o, stats));
+    if (!o.device_output) {
+      MG_TRY(copy_out(g, dist, out, sizeof(int32_t) * (size_t)nsrc * (size_t)n, 0));
+      MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    return MG_OK;
+  }
   int shift = 0;
   while ((int64_t(1) << shift) < n) shift++;
   const int64_t stride = int64_t(1) << shift;

@@ -153,6 +153,38 @@ def test_sssp_batch_power_of_two_device_output(rmat14):
     np.testing.assert_array_equal(dev.cpu().numpy().reshape(3, h.n), host)
 
 
+@pytest.mark.parametrize("nsrc", [1, 31, 33, 70])
+def test_sssp_batch_interleaved_rows(nsrc):
+    """Mean out-degree above 8: the batch runs on interleaved distance rows (32
+    instances per row, groups of 32). Every row equals the oracle's single-source
+    distances, out- and in-edges, with repeated sources and zero weights."""
+    torch = pytest.importorskip("torch")
+    h = mg.gen_rmat(12, 16, 123, symmetrize=False, weights="int", p0=0, p1=40)
+    assert h.m > 8 * h.n
+    rng = np.random.default_rng(nsrc)
+    srcs = rng.integers(0, h.n, nsrc).astype(np.int32)
+    if nsrc > 3:
+        srcs[1] = srcs[2]
+    deg = np.diff(h.row_offsets).astype(np.int64)
+    with mg.Graph(h.row_offsets, h.col_idx, h.weights_i32) as g:
+        for directed in (1, 0):
+            dist, st = g.sssp_batch(srcs, directed=directed)
+            etrav = 0
+            for i, s_ in enumerate(srcs):
+                ref = oracle.sssp(h.row_offsets, h.col_idx, h.weights_i32, [int(s_)], directed)
+                np.testing.assert_array_equal(dist[i], ref)
+                etrav += int(deg[ref < 2**31 - 1].sum())
+            assert st["edges_traversed"] == etrav
+            dev = torch.empty(nsrc * h.n, dtype=torch.int32, device="cuda")
+            g.sssp_batch(srcs, out=dev, directed=directed, use_graph=False)
+            np.testing.assert_array_equal(dev.cpu().numpy().reshape(nsrc, h.n), dist)
+    with mg.Graph(h.row_offsets, h.col_idx) as g:  # unit weights: distance = BFS depth
+        dist, _ = g.sssp_batch(srcs[:5])
+        for i in range(min(5, nsrc)):
+            bd = oracle.bfs(h.row_offsets, h.col_idx, [int(srcs[i])])
+            np.testing.assert_array_equal(dist[i], np.where(bd < 0, 2**31 - 1, bd))
+
+
 def _sparse_teleports(n, nvec, seed):
     return mg.sparse_teleports(n, nvec, seed)
 

@@ -18,6 +18,9 @@ SSSP_SETTINGS = [
     dict(sssp_heavy=32, sssp_chunk_cap=100),
     dict(sssp_ctas_per_sm=1),
     dict(sssp_ctas_per_sm=8, sssp_heavy=128),
+    dict(sssp_batch_heavy=1),          # every batch item cut into chunks
+    dict(sssp_batch_heavy=1 << 30),    # every batch item walked by its warp
+    dict(sssp_batch_heavy=16, sssp_chunk_cap=3),
 ]
 
 
@@ -50,7 +53,9 @@ def test_sssp_tuning_settings_are_exact(rmat13, setting):
         g.set_tuning(**mg.Graph.default_tuning())
 
 
-@pytest.mark.parametrize("setting", SSSP_SETTINGS[:4], ids=["defaults", "all-chunks", "all-walked", "cap-1"])
+@pytest.mark.parametrize("setting", SSSP_SETTINGS[:4] + SSSP_SETTINGS[-3:],
+                         ids=["defaults", "all-chunks", "all-walked", "cap-1", "batch-chunks", "batch-walked",
+                              "batch-cap-3"])
 def test_sssp_tuning_both_directions(setting):
     # directed graph read both ways: chunks of CSC edges carry the reverse flag
     h = mg.gen_rmat(12, 16, 31, symmetrize=False, weights="int", p0=0, p1=40)
@@ -59,6 +64,10 @@ def test_sssp_tuning_both_directions(setting):
         for directed in (1, 0):
             d, _ = g.sssp([0, 5], directed=directed)
             np.testing.assert_array_equal(d, oracle.sssp(h.row_offsets, h.col_idx, h.weights_i32, [0, 5], directed))
+            db, _ = g.sssp_batch([0, 5, 77], directed=directed)
+            for i, s_ in enumerate([0, 5, 77]):
+                np.testing.assert_array_equal(db[i], oracle.sssp(h.row_offsets, h.col_idx, h.weights_i32, [s_],
+                                                                 directed))
 
 
 def test_tuning_ranges(rmat13):
@@ -66,7 +75,7 @@ def test_tuning_ranges(rmat13):
     before = g.tuning()
     assert before == mg.Graph.default_tuning()
     for bad in (dict(sssp_heavy=0), dict(sssp_heavy_small=before["sssp_heavy"] + 1), dict(sssp_ctas_per_sm=9),
-                dict(sssp_ctas_per_sm=0), dict(sssp_chunk_cap=-1)):
+                dict(sssp_ctas_per_sm=0), dict(sssp_chunk_cap=-1), dict(sssp_batch_heavy=0)):
         with pytest.raises(mg.MapGraphError) as ex:
             g.set_tuning(**bad)
         assert ex.value.status == L.MG_ERR_ARG
