@@ -121,6 +121,22 @@ __device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const in
     tr[r] = u[r] >= 0 && s < (int64_t)cd[r];
     nd[r] = (int32_t)min(s, (int64_t)INT_MAX);
   }
+  if (x.delta <= 0) {
+    // Plain rounds: an edge that improves on the distance read before the
+    // atomicMin marks its head in the next-frontier bitmap, and neither atomic's
+    // old value is waited for (the frontier is compacted from the bitmap after the
+    // round). A mark from an improvement that a concurrent smaller one overtook
+    // only expands that vertex once more.
+#pragma unroll
+    for (int r = 0; r < SSSP_U; r++) {
+      if (tr[r]) {
+        atomicMin(x.dist + u[r], nd[r]);
+        atomicOr(x.inq_next + (u[r] >> 5), 1u << (u[r] & 31));
+        x.updates++;
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < SSSP_U; r++) old[r] = tr[r] ? atomicMin(x.dist + u[r], nd[r]) : INT_MIN;
   uint32_t ob[SSSP_U];
@@ -128,7 +144,7 @@ __device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const in
 #pragma unroll
   for (int r = 0; r < SSSP_U; r++) {
     const bool win = tr[r] && nd[r] < old[r];
-    nearq[r] = x.delta <= 0 || (int64_t)nd[r] < x.thr;
+    nearq[r] = (int64_t)nd[r] < x.thr;
     ob[r] = 0xffffffffu;  // no claim: reads as "already queued"
     if (win) ob[r] = atomicOr((nearq[r] ? x.inq_next : x.infar) + (u[r] >> 5), 1u << (u[r] & 31));
   }
@@ -140,13 +156,14 @@ __device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const in
     }
     const bool fresh = u[r] >= 0 && !(ob[r] & (1u << (u[r] & 31)));
     ws_push(st, fresh && nearq[r], u[r], x.qout, x.qlen_out, x.qcap, x.overflow);
-    if (x.delta > 0) warp_append(fresh && !nearq[r], u[r], x.far_out, x.far_len_out, x.qcap, x.overflow);
+    warp_append(fresh && !nearq[r], u[r], x.far_out, x.far_len_out, x.qcap, x.overflow);
   }
 }
 
 __device__ __forceinline__ RelaxCtx relax_ctx(const SsspArgs &a, DevCtl *c, int cur) {
   const int fc = a.delta > 0 ? vload(&c->far_cur) : 0;
-  return RelaxCtx{a.dist, cur ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1], &c->overflow, a.qcap,
+  return RelaxCtx{a.dist, (cur || a.delta <= 0) ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1],
+                  &c->overflow, a.qcap,
                   a.vmask, 0, 0, a.delta, vload(&c->thr), a.infar, fc ? a.far1 : a.far0, &c->far_len[fc]};
 }
 
@@ -221,7 +238,6 @@ __device__ void sssp_level_end(const SsspArgs &a) {
   const int32_t nf = vload(&c->qlen[cur ^ 1]);
   const int lvl = vload(&c->level) + 1;
   trace_level(c, lvl - 1, MG_DIR_PUSH, vload(&c->qlen[cur]), vload(&c->mf_next), 0.0);
-  c->visited_deg = vload(&c->visited_deg) + vload(&c->mf_next);
   c->mf_next = 0;
   c->level = lvl;
   c->qlen[cur] = 0;
@@ -285,9 +301,10 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
     const int32_t v = i < nin ? qin[i] : -1;
     int32_t beg = 0, deg = 0, dv = 0, cb = 0, cdeg = 0;
     if (v >= 0) {
-      // The whole bitmap of the current frontier is cleared here, one word at a
-      // time: nothing sets bits in it during this round.
-      inq_cur[v >> 5] = 0u;
+      // Near-far rounds: the whole bitmap of the current frontier is cleared here,
+      // one word at a time (nothing sets bits in it during this round). Plain
+      // rounds have one bitmap, cleared by the compaction.
+      if (a.delta > 0) inq_cur[v >> 5] = 0u;
       nexp++;
       beg = a.ro[v & a.vmask];
       deg = a.ro[(v & a.vmask) + 1] - beg;
@@ -352,7 +369,84 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_chunk_kernel(SsspArgs a) {
   }
   ws_flush(st, x.qout, x.qlen_out, x.qcap, x.overflow);
   sssp_counters(c, s_sum, x.reach_deg, 0, 0, x.updates);
+  if (a.delta > 0 && last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
+}
+
+// Plain rounds, pass 3: the next frontier, compacted in item order from the
+// bitmap the round marked (SSSP_CW words per tile, one queue atomic per tile),
+// the words cleared for the next round, the frontier's out-edges summed for the
+// trace; the last CTA ends the round. Near-far rounds append to the queue as they
+// relax and end in pass 2.
+constexpr int SSSP_CW = SSSP_NT * 4;
+__global__ void __launch_bounds__(SSSP_NT) sssp_compact_kernel(SsspArgs a) {
+  __shared__ int32_t s_red[SSSP_NT / 32 + 1];
+  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
+  __shared__ int32_t s_base;
+  DevCtl *c = a.ctl;
+  if (a.delta > 0 || vload(&c->done)) {
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0 && vload(&c->done)) cudaGraphSetConditional(a.h, 0u);
+    return;
+  }
+  const int cur = vload(&c->cur);
+  int32_t *qout = cur ? a.q0 : a.q1;
+  int32_t *qlen = &c->qlen[cur ^ 1];
+  uint32_t *bm = a.inq0;
+  const int64_t nwords = (a.n + 31) >> 5;
+  int64_t fdeg = 0;
+  for (int64_t t0 = (int64_t)blockIdx.x * SSSP_CW; t0 < nwords; t0 += (int64_t)gridDim.x * SSSP_CW) {
+    const int64_t w0 = t0 + (int64_t)threadIdx.x * 4;
+    uint32_t wd[4] = {0u, 0u, 0u, 0u};
+    if (w0 + 3 < nwords) {
+      uint4 *p = reinterpret_cast<uint4 *>(bm + w0);
+      const uint4 q = *p;
+      wd[0] = q.x;
+      wd[1] = q.y;
+      wd[2] = q.z;
+      wd[3] = q.w;
+      if (q.x | q.y | q.z | q.w) *p = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+      for (int k = 0; k < 4; k++) {
+        if (w0 + k < nwords) {
+          wd[k] = bm[w0 + k];
+          if (wd[k]) bm[w0 + k] = 0u;
+        }
+      }
+    }
+    const int32_t cnt = __popc(wd[0]) + __popc(wd[1]) + __popc(wd[2]) + __popc(wd[3]);
+    int32_t tot;
+    int32_t pos = block_exclusive_scan<SSSP_NT>(cnt, s_red, &tot);
+    if (threadIdx.x == 0) s_base = tot ? atomicAdd(qlen, tot) : 0;
+    __syncthreads();
+    pos += s_base;
+    for (int k = 0; k < 4; k++) {
+      uint32_t m = wd[k];
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        const int32_t it = (int32_t)((w0 + k) * 32 + b);
+        const int32_t v = it & a.vmask;
+        fdeg += a.ro[v + 1] - a.ro[v];
+        if (pos < a.qcap) qout[pos] = it;
+        else c->overflow = 1;
+        pos++;
+      }
+    }
+    __syncthreads();
+  }
+  const int64_t b = block_sum<SSSP_NT>(fdeg, s_sum);
+  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b);
   if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
+}
+
+// The TEPS numerator of a run: out-degrees of every reached item's vertex.
+__global__ void sssp_reach_kernel(const int32_t *__restrict__ dist, int64_t nitems, int32_t vmask,
+                                  const int32_t *__restrict__ ro, DevCtl *c) {
+  __shared__ int64_t s_sum[256 / 32 + 1];
+  int64_t t = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += (int64_t)gridDim.x * blockDim.x)
+    if (dist[i] != INT_MAX) t += ro[(i & vmask) + 1] - ro[i & vmask];
+  const int64_t b = block_sum<256>(t, s_sum);
+  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&c->visited_deg, (unsigned long long)b);
 }
 
 // Near-far split, pass 1: the smallest distance still waiting at or above the
@@ -461,7 +555,9 @@ __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, 
   for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
     const int32_t s = srcs[i];
     const uint32_t bit = 1u << (s & 31);
-    if (!(atomicOr(&a.inq0[s >> 5], bit) & bit)) {
+    // duplicates: near-far rounds clear this bitmap as they expand the seeds; plain
+    // rounds mark the next frontier in inq0 and leave inq1 to the seeds
+    if (!(atomicOr(&(a.delta > 0 ? a.inq0 : a.inq1)[s >> 5], bit) & bit)) {
       a.dist[s] = 0;
       deg += a.ro[(s & a.vmask) + 1] - a.ro[s & a.vmask];
       const int pos = atomicAdd(&c->qlen[0], 1);
@@ -471,7 +567,7 @@ __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, 
   }
   const int64_t t = block_sum<1024>(deg, s_sum);
   if (threadIdx.x == 0) {
-    c->visited_deg = t;
+    if (a.delta > 0) c->mf_next = t;  // near-far: reached vertices' out-edges, seeds first
     c->iter_cap = iter_cap;
     c->thr = a.delta > 0 ? (int64_t)a.delta : INT64_MAX;
     c->far_min = INT_MAX;
@@ -982,12 +1078,16 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   std::memset(&sig, 0, sizeof(sig));
   sig.a = a;
   sig.grid = grid;
-  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+  const int64_t nwords_all = (nitems + 31) / 32;
+  const int cgrid =
+      (int)std::max<int64_t>(1, std::min<int64_t>((nwords_all + SSSP_CW - 1) / SSSP_CW, g->num_sms * 8));
+  LoopBody body = [a, grid, cgrid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
     SsspArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
     sssp_relax_kernel<<<grid, SSSP_NT, 0, st>>>(b);
     sssp_chunk_kernel<<<grid, SSSP_NT, 0, st>>>(b);
+    if (b.delta <= 0) sssp_compact_kernel<<<cgrid, SSSP_NT, 0, st>>>(b);
     if (b.delta > 0) {
       sssp_far_min_kernel<<<grid, SSSP_NT, 0, st>>>(b);
       sssp_far_split_kernel<<<grid, SSSP_NT, 0, st>>>(b);
@@ -995,6 +1095,8 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   };
   MG_TRY(run_loop(g, vmask == -1 ? SLOT_SSSP : SLOT_BSSSP, &sig, sizeof(sig), o.use_graph >= 0, body,
                   (int64_t)iter_cap + 2));
+  sssp_reach_kernel<<<g->num_sms * 4, 256, 0, s>>>(dist, nitems, vmask, g->ro, g->ctl);
+  MG_CUDA_TRY(cudaGetLastError());
   MG_CUDA_TRY(cudaEventRecord(g->ev1, s));
   MG_TRY(fetch_ctl(g));
   const DevCtl &hc = *g->ctl_host;
@@ -1007,8 +1109,8 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
-    const int64_t per = a.delta > 0 ? 4 : 2;
-    stats->launches = 2 + (o.use_graph >= 0 ? (per + 1) * (int64_t)hc.body_iters : per * (int64_t)hc.level);
+    const int64_t per = a.delta > 0 ? 4 : 3;
+    stats->launches = 3 + (o.use_graph >= 0 ? (per + 1) * (int64_t)hc.body_iters : per * (int64_t)hc.level);
     stats->status_detail = a.delta > 0 ? a.delta : 0;
   }
   if (hc.status != 0) {
