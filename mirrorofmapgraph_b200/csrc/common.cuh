@@ -204,4 +204,13 @@ __device__ __forceinline__ void staged_append(BlockQueue *bq, bool pred, int32_t
 
 __device__ __forceinline__ int32_t ld_nc(const int32_t *p) { return __ldg(p); }
 
+// Reductions whose old value nobody waits for (PTX red): the issuing warp does
+// not stall on them, unlike atomics whose result is used.
+__device__ __forceinline__ void red_min(int32_t *p, int32_t v) {
+  asm volatile("red.relaxed.gpu.global.min.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_or(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 }  // namespace mg

@@ -130,8 +130,8 @@ __device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const in
 #pragma unroll
     for (int r = 0; r < SSSP_U; r++) {
       if (tr[r]) {
-        atomicMin(x.dist + u[r], nd[r]);
-        atomicOr(x.inq_next + (u[r] >> 5), 1u << (u[r] & 31));
+        red_min(x.dist + u[r], nd[r]);
+        red_or(x.inq_next + (u[r] >> 5), 1u << (u[r] & 31));
         x.updates++;
       }
     }
@@ -275,7 +275,7 @@ __device__ __forceinline__ void sssp_counters(DevCtl *c, int64_t *s_sum, int64_t
 
 // Relaxation round, pass 1: each warp takes 32 frontier items, cuts the heavy ones
 // into chunks for pass 2 and walks the edges of the others itself.
-__global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
+__global__ void __launch_bounds__(SSSP_NT, 4) sssp_relax_kernel(SsspArgs a) {
   __shared__ int32_t s_stage[SSSP_NT / 32][SSSP_WS];
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_relax_kernel(SsspArgs a) {
 
 // Pass 2: every warp of the grid relaxes chunks of the heavy vertices' edges; the
 // last CTA closes the round.
-__global__ void __launch_bounds__(SSSP_NT) sssp_chunk_kernel(SsspArgs a) {
+__global__ void __launch_bounds__(SSSP_NT, 4) sssp_chunk_kernel(SsspArgs a) {
   __shared__ int32_t s_stage[SSSP_NT / 32][SSSP_WS];
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
@@ -668,7 +668,7 @@ __device__ __forceinline__ void mss_edges(const MssArgs &a, int2 *se, uint32_t *
       for (int r = 0; r < MSS_U; r++) {
         const int32_t nd = (int32_t)min((uint32_t)dv + (uint32_t)w[r], (uint32_t)INT_MAX);
         const bool tr = nd < cu[r];
-        if (tr) atomicMin(Dl + ((uint32_t)u[r] << 5), nd);
+        if (tr) red_min(Dl + ((uint32_t)u[r] << 5), nd);
         const uint32_t bits = __ballot_sync(FULL, tr);
         if (lane == r) {
           myb = bits;
@@ -677,7 +677,7 @@ __device__ __forceinline__ void mss_edges(const MssArgs &a, int2 *se, uint32_t *
       }
       if (myb) {
         updates += __popc(myb);
-        atomicOr(mg + myv, myb);
+        red_or(mg + myv, myb);
       }
     }
     __syncwarp();
@@ -705,7 +705,7 @@ __device__ void mss_level_end(const MssArgs &a) {
 
 // Pass 1: each warp reads 32 frontier items' headers (one per lane), cuts the
 // heavy ones into chunks and walks the others item by item.
-__global__ void __launch_bounds__(SSSP_NT) mss_relax_kernel(MssArgs a) {
+__global__ void __launch_bounds__(SSSP_NT, 4) mss_relax_kernel(MssArgs a) {
   __shared__ __align__(16) int2 s_edges[SSSP_NT / 32][MSS_CH + MSS_U];
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(SSSP_NT) mss_relax_kernel(MssArgs a) {
 }
 
 // Pass 2: chunks of the heavy items, a warp per chunk.
-__global__ void __launch_bounds__(SSSP_NT) mss_chunk_kernel(MssArgs a) {
+__global__ void __launch_bounds__(SSSP_NT, 4) mss_chunk_kernel(MssArgs a) {
   __shared__ __align__(16) int2 s_edges[SSSP_NT / 32][MSS_CH + MSS_U];
   __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   DevCtl *c = a.ctl;
