@@ -164,6 +164,11 @@ mg_status mg_graph_stream(const mg_graph *g, void **stream);
 /* Sizes and flags of a graph (CsrProblem::nodes/edges, csr_problem.cuh:312-314). */
 mg_status mg_graph_info(const mg_graph *g, int64_t *n, int64_t *m, uint32_t *flags, int32_t *device);
 
+/* Out-degree statistics of a graph, computed on the device (synchronises the
+ * graph's stream): the largest out-degree and the number of vertices without
+ * out-edges. Either pointer may be NULL. */
+mg_status mg_graph_degree_stats(mg_graph *g, int64_t *max_out_degree, int64_t *no_out_edges);
+
 /* Device arrays of a graph, as GraphSlice exposes them (csr_problem.cuh:154-163):
  * row_offsets, column_indices, edge_values (NULL without values), column_offsets,
  * row_indices and the CSC->CSR edge permutation (the last three NULL without CSC;
@@ -394,7 +399,22 @@ typedef struct mg_tuning {
                                2^23); past it a warp walks its heavy vertices itself [0; 0 .. 2^30] */
   int32_t sssp_batch_heavy; /* mg_sssp_batch (interleaved rows): frontier items of at least this many edges are cut
                                into chunks of 128 edges for every warp of the grid [32; 1 .. 2^30] */
-  int32_t reserved[11];
+  int32_t bfs_cta_th;       /* BFS push levels: out-degree from which the whole CTA expands a frontier vertex
+                               [512; 32 .. 2^30] */
+  int32_t bfs_grid_th;      /* out-degree from which a vertex of a large frontier is spread over the whole grid
+                               [4096; 32 .. 2^30] */
+  int32_t bfs_defer_warp;   /* 1: a frontier filling under an eighth of the grid's threads sends every vertex of
+                               32+ edges to the grid-wide pass; 0: only those of bfs_cta_th+ edges [1; 0 .. 1] */
+  int32_t bfs_persist_max;  /* push levels of at most this many frontier vertices ... [65536; 0 .. 2^30] */
+  int32_t bfs_persist_edges;/* ... and at most this many frontier out-edges run in one persistent cooperative
+                               launch (0: never) [131072; 0 .. 2^30] */
+  int32_t bfs_alpha;        /* direction rule: pull once the frontier's out-edges exceed the unvisited vertices'
+                               out-edges / alpha [14; 1 .. 2^20] */
+  int32_t bfs_beta;         /* ... and back to push when the frontier holds fewer than n / beta vertices
+                               [24; 1 .. 2^20] */
+  int32_t bfs_sparse_degree;/* MG_DIR_AUTO stays top-down on graphs of mean out-degree <= this [8; 0 .. 2^20] */
+  int32_t bfs_ctas_per_sm;  /* CTAs of 256 threads per SM of the BFS level kernels [4; 1 .. 8] */
+  int32_t reserved[18];
 } mg_tuning;
 void mg_tuning_defaults(mg_tuning *t);
 mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t);

@@ -68,7 +68,10 @@ MG_TRACE_LEVELS = 4096
 
 class MgTuning(C.Structure):
     _fields_ = [("sssp_heavy", C.c_int32), ("sssp_heavy_small", C.c_int32), ("sssp_ctas_per_sm", C.c_int32),
-                ("sssp_chunk_cap", C.c_int32), ("sssp_batch_heavy", C.c_int32), ("reserved", C.c_int32 * 11)]
+                ("sssp_chunk_cap", C.c_int32), ("sssp_batch_heavy", C.c_int32), ("bfs_cta_th", C.c_int32),
+                ("bfs_grid_th", C.c_int32), ("bfs_defer_warp", C.c_int32), ("bfs_persist_max", C.c_int32),
+                ("bfs_persist_edges", C.c_int32), ("bfs_alpha", C.c_int32), ("bfs_beta", C.c_int32),
+                ("bfs_sparse_degree", C.c_int32), ("bfs_ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 18)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -135,6 +138,7 @@ SIGNATURES = {
     "mg_part_pr_result": (C.c_int, [_P, _P, C.c_int32, C.POINTER(MgStats)]),
     "mg_graph_trace": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "mg_tuning_defaults": (None, [C.POINTER(MgTuning)]),
+    "mg_graph_degree_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mg_graph_set_tuning": (C.c_int, [_P, C.POINTER(MgTuning)]),
     "mg_graph_get_tuning": (C.c_int, [_P, C.POINTER(MgTuning)]),
     "mg_debug_fail_alloc": (C.c_int, [C.c_int64]),

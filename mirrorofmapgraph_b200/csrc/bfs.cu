@@ -40,11 +40,10 @@ namespace mg {
 constexpr int BFS_NT = 256;
 constexpr int BFS_CTA_TH = 512;   // out-degree at or above which a CTA expands the vertex
 constexpr int PULL_SERIAL = 8;    // in-edges a lane scans alone before the warp helps
-constexpr int64_t BEAMER_ALPHA = 14, BEAMER_BETA = 24;
-#ifndef MG_BFS_GRID_MULT
-#define MG_BFS_GRID_MULT 4
-#endif
-constexpr int64_t BFS_SPARSE_DEGREE = 8;  // mean out-degree at or below which AUTO runs top-down only
+// Beamer's direction rule (mg_tuning.bfs_alpha / bfs_beta, defaults 14 and 24):
+// pull when the frontier's out-edges exceed the unvisited vertices' out-edges /
+// alpha, back to push when the frontier holds fewer than n / beta vertices. AUTO
+// runs top-down only on graphs of mean out-degree <= bfs_sparse_degree (8).
 
 struct BfsArgs {
   const int32_t *ro, *ci;  // out-edges (CSR)
@@ -64,7 +63,24 @@ struct BfsArgs {
   int32_t use_cond;
   uint32_t bar_extra;            // test hook (mg_debug_barrier_skew): a barrier that cannot complete
   unsigned long long bar_limit;  // barrier polls before MG_ERR_TIMEOUT
+  // tuned thresholds (mg_tuning): CTA-bin and grid-bin out-degrees, the warp-bin
+  // deferral rule, the persistent kernel's frontier limits, Beamer's constants
+  int32_t cta_th, grid_th, defer_warp;
+  int32_t persist_max;
+  int64_t persist_edges;
+  int64_t alpha, beta;
 };
+
+// The graph's tuned BFS thresholds into the kernel arguments.
+inline void bfs_tuning(BfsArgs &a, const mg_tuning &t) {
+  a.cta_th = t.bfs_cta_th;
+  a.grid_th = t.bfs_grid_th;
+  a.defer_warp = t.bfs_defer_warp;
+  a.persist_max = t.bfs_persist_max;
+  a.persist_edges = t.bfs_persist_edges;
+  a.alpha = t.bfs_alpha;
+  a.beta = t.bfs_beta;
+}
 
 __device__ void bfs_level_end(const BfsArgs &a) {
   DevCtl *c = a.ctl;
@@ -92,9 +108,9 @@ __device__ void bfs_level_end(const BfsArgs &a) {
     } else if (a.mode == MG_DIR_PUSH || !a.can_pull) {
       dir = 0;
     } else if (dir == 0) {
-      if (mf > (a.m_total - vdeg) / BEAMER_ALPHA) dir = 1;
+      if (mf > (a.m_total - vdeg) / a.alpha) dir = 1;
     } else {
-      if ((int64_t)nf * BEAMER_BETA < a.n) dir = 0;
+      if ((int64_t)nf * a.beta < a.n) dir = 0;
     }
   }
   if (dir == 1 && !done) c->levels_pull += 1;
@@ -160,15 +176,17 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
   bq_init(bq);
   x.bq = &bq;
   int64_t insp = 0, nexp = 0;
-  const BigList big{a.big_v, &c->big_len, defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
+  const BigList big{a.big_v, &c->big_len, defer_threshold<BFS_NT>(nin, a.cta_th, a.grid_th, a.defer_warp)};
   for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
     const int64_t i = tile + threadIdx.x;
     const int32_t v = i < nin ? qin[i] : -1;
     nexp += v >= 0;
     const int32_t *ci = a.ci, *ri = a.ri;
-    expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big);
+    expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big, -1,
+                                    a.cta_th);
     if (a.both)
-      expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
+      expand_tile<BFS_NT, BFS_CTA_TH>(sm, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); }, nullptr,
+                                      -1, a.cta_th);
   }
   bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
   const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
@@ -185,19 +203,11 @@ __global__ void __launch_bounds__(BFS_NT) bfs_push_kernel(BfsArgs a) {
 // lattices, where a BFS has thousands of levels of a few thousand vertices and
 // per-level launches dominate). One cooperative launch runs level after level,
 // with a grid barrier between the expansion and the level end, while the level is
-// a push level with at most PERSIST_MAX frontier vertices and PERSIST_EDGES
+// a push level with at most bfs_persist_max frontier vertices and bfs_persist_edges
 // frontier out-edges; it then returns and the per-level kernels continue from the
 // same control block. Vertices of GRID_TH or more edges are deferred as in the
 // per-level push and expanded by the whole grid after a second barrier, which
 // only levels that deferred one take.
-#ifndef MG_PERSIST_MAX
-#define MG_PERSIST_MAX (1 << 16)
-#endif
-#ifndef MG_PERSIST_EDGES
-#define MG_PERSIST_EDGES (1 << 17)
-#endif
-constexpr int32_t PERSIST_MAX = MG_PERSIST_MAX;
-constexpr int64_t PERSIST_EDGES = MG_PERSIST_EDGES;  // frontier out-edges
 constexpr unsigned long long PERSIST_WAIT = 1ull << 22;  // barrier polls (seconds at most) before giving up
 
 __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
@@ -216,7 +226,7 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
   int32_t nin = vload(&c->qlen[sel]);
   int64_t mf = vload(&c->mf_front), vdeg = vload(&c->visited_deg);
   const int32_t iter_cap = vload(&c->iter_cap);
-  if (vload(&c->done) || vload(&c->dir) != 0 || nin > PERSIST_MAX || mf > PERSIST_EDGES) return;
+  if (vload(&c->done) || vload(&c->dir) != 0 || nin > a.persist_max || mf > a.persist_edges) return;
   bq_init(bq);
   for (;;) {
     // Per-level counters rotate over three slots: this level appends to `out`;
@@ -230,16 +240,18 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
     const int32_t *qin = sel ? a.q1 : a.q0;
     PushCtx x{a.label, a.vis, a.ro, sel ? a.q0 : a.q1, &c->pq[out], &c->overflow, a.qcap, lvl, 0};
     x.bq = &bq;
-    const BigList big{a.big_v, &c->pb[out], defer_threshold<BFS_NT>(nin, BFS_CTA_TH)};
+    const BigList big{a.big_v, &c->pb[out], defer_threshold<BFS_NT>(nin, a.cta_th, a.grid_th, a.defer_warp)};
     const int32_t *ci = a.ci, *ri = a.ri;
     int64_t insp = 0, nexp = 0;
     for (int64_t tile = (int64_t)blockIdx.x * BFS_NT; tile < nin; tile += (int64_t)gridDim.x * BFS_NT) {
       const int64_t i = tile + threadIdx.x;
       const int32_t v = i < nin ? qin[i] : -1;
       nexp += v >= 0;
-      expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big);
+      expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.ro, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ci[k]); }, &big,
+                                      -1, a.cta_th);
       if (a.both)
-        expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); });
+        expand_tile<BFS_NT, BFS_CTA_TH>(sm.e, a.co, v, insp, [&](int32_t, int32_t k) { bfs_visit(x, ri[k]); },
+                                        nullptr, -1, a.cta_th);
     }
     bq_flush(bq, x.qout, x.qlen_out, x.qcap, x.overflow);
     const int64_t bmf = block_sum<BFS_NT>(x.mf, s_sum);
@@ -283,8 +295,8 @@ __global__ void __launch_bounds__(BFS_NT) bfs_persist_kernel(BfsArgs a) {
     const bool done = nf == 0 || lvl >= iter_cap || over;
     int dir = 0;
     if (a.mode == MG_DIR_PULL) dir = a.can_pull ? 1 : 0;
-    else if (a.mode == MG_DIR_AUTO && a.can_pull && mf > (a.m_total - vdeg) / BEAMER_ALPHA) dir = 1;
-    if (done || dir != 0 || nf > PERSIST_MAX || mf > PERSIST_EDGES) {
+    else if (a.mode == MG_DIR_AUTO && a.can_pull && mf > (a.m_total - vdeg) / a.alpha) dir = 1;
+    if (done || dir != 0 || nf > a.persist_max || mf > a.persist_edges) {
       // Hand over to the per-level kernels (or finish) with their control state.
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         c->level = lvl;
@@ -500,6 +512,8 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   cudaStream_t s = g->stream;
 
   BfsArgs a;
+  std::memset(&a, 0, sizeof(a));  // the loop-graph signature compares its bytes
+  bfs_tuning(a, g->tune);
   a.ro = g->ro;
   a.ci = g->ci;
   a.co = g->has_csc ? g->co : g->ro;
@@ -513,7 +527,8 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   // top-down: a bottom-up level scans every unvisited vertex and, far from a thin
   // wavefront, finds no early exit (4096^2 lattice: 7.8 ms with Beamer's rule,
   // 6.7 ms top-down only).
-  a.mode = (o.direction == MG_DIR_AUTO && g->m <= BFS_SPARSE_DEGREE * g->n) ? MG_DIR_PUSH : o.direction;
+  a.mode = (o.direction == MG_DIR_AUTO && g->m <= (int64_t)g->tune.bfs_sparse_degree * g->n) ? MG_DIR_PUSH
+                                                                                           : o.direction;
   a.can_pull = g->has_csc && !undirected;
   a.both = undirected ? 1 : 0;
   a.n = n;
@@ -545,7 +560,7 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     cudaGetLastError();
   }
 
-  const int grid = g->num_sms * MG_BFS_GRID_MULT;
+  const int grid = g->num_sms * g->tune.bfs_ctas_per_sm;
   const bool use_graph = o.use_graph >= 0;
   struct Sig {
     BfsArgs a;
@@ -698,6 +713,8 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   cudaStream_t s = g->stream;
 
   BfsArgs a;
+  std::memset(&a, 0, sizeof(a));  // the loop-graph signature compares its bytes
+  bfs_tuning(a, g->tune);
   a.ro = g->ro;
   a.ci = g->ci;
   a.co = g->has_csc ? g->co : g->ro;
@@ -711,7 +728,8 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   // top-down: a bottom-up level scans every unvisited vertex and, far from a thin
   // wavefront, finds no early exit (4096^2 lattice: 7.8 ms with Beamer's rule,
   // 6.7 ms top-down only).
-  a.mode = (o.direction == MG_DIR_AUTO && g->m <= BFS_SPARSE_DEGREE * g->n) ? MG_DIR_PUSH : o.direction;
+  a.mode = (o.direction == MG_DIR_AUTO && g->m <= (int64_t)g->tune.bfs_sparse_degree * g->n) ? MG_DIR_PUSH
+                                                                                           : o.direction;
   a.can_pull = g->has_csc && !undirected;
   a.both = undirected ? 1 : 0;
   a.n = n;
@@ -734,7 +752,7 @@ extern "C" mg_status mg_bfs_noalloc(mg_graph *g, const int32_t *srcs, int32_t ns
   bfs_clear_kernel<<<g->num_sms * 8, 256, 0, s>>>(depth, a.vis, n);
   bfs_seed_kernel<<<1, 1024, 0, s>>>(a, dsrc, nsrc, iter_cap, 0);
   MG_CUDA_TRY(cudaGetLastError());
-  const int grid = g->num_sms * MG_BFS_GRID_MULT;
+  const int grid = g->num_sms * g->tune.bfs_ctas_per_sm;
   LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle, int) {
     bfs_push_kernel<<<grid, BFS_NT, 0, st>>>(a);
     bfs_push_big_kernel<<<grid, BFS_NT, 0, st>>>(a);

@@ -41,10 +41,13 @@ __device__ __forceinline__ bool defer_big(const BigList &big, int32_t v, int32_t
 // `vmask` maps a frontier item to the vertex whose offsets it uses (item & vmask);
 // -1 (every bit) is the identity. Batched runs pack an instance number into the
 // item's high bits and pass the low-bit mask.
+//
+// `cta_th` (default CTA_TH) is the out-degree from which the whole CTA expands a
+// vertex; callers with a tuned threshold pass it at run time.
 template <int NT, int CTA_TH, typename P, typename Visit>
 __device__ __forceinline__ void expand_tile_p(ExpandSmem<NT, P> &sm, const int32_t *__restrict__ off, int32_t v,
                                               P pay, int64_t &insp, Visit &&visit, const BigList *big = nullptr,
-                                              int32_t vmask = -1) {
+                                              int32_t vmask = -1, int32_t cta_th = CTA_TH) {
   const int tid = threadIdx.x, lane = lane_id();
   int32_t beg = 0, deg = 0;
   if (v >= 0) {
@@ -55,8 +58,8 @@ __device__ __forceinline__ void expand_tile_p(ExpandSmem<NT, P> &sm, const int32
   // Vertices for the grid-strided bin are expanded by a later kernel.
   if (big && defer_big(*big, v, deg)) deg = 0;
   // CTA bin.
-  while (__syncthreads_or(deg >= CTA_TH)) {
-    if (deg >= CTA_TH) sm.cta[0] = tid;
+  while (__syncthreads_or(deg >= cta_th)) {
+    if (deg >= cta_th) sm.cta[0] = tid;
     __syncthreads();
     if (sm.cta[0] == tid) {
       sm.cta[1] = beg;
@@ -105,9 +108,9 @@ __device__ __forceinline__ void expand_tile_p(ExpandSmem<NT, P> &sm, const int32
 template <int NT, int CTA_TH, typename Visit>
 __device__ __forceinline__ void expand_tile(ExpandSmem<NT> &sm, const int32_t *__restrict__ off, int32_t v,
                                             int64_t &insp, Visit &&visit, const BigList *big = nullptr,
-                                            int32_t vmask = -1) {
+                                            int32_t vmask = -1, int32_t cta_th = CTA_TH) {
   expand_tile_p<NT, CTA_TH>(sm, off, v, (int32_t)0, insp, [&](int32_t sv, int32_t, int32_t k) { visit(sv, k); },
-                            big, vmask);
+                            big, vmask, cta_th);
 }
 
 template <typename T>
@@ -138,10 +141,14 @@ struct BigList {
 // grid-wide pass instead; when it fills under an eighth of them, so does every
 // vertex the warp bin would take (32 edges or more). R-MAT s22 BFS, mean of 13
 // sources: 0.54 ms with the CTA-bin rule alone, 0.42 ms with both.
+//
+// grid_th and defer_warp (the warp-bin rule on or off) default to GRID_TH and
+// MG_DEFER_WARP; callers with tuned values pass them at run time.
 template <int NT>
-__device__ __forceinline__ int32_t defer_threshold(int64_t nin, int32_t cta_th) {
-  if (MG_DEFER_WARP && nin * 8 < (int64_t)gridDim.x * NT) return 32;
-  return nin < (int64_t)gridDim.x * NT ? cta_th : GRID_TH;
+__device__ __forceinline__ int32_t defer_threshold(int64_t nin, int32_t cta_th, int32_t grid_th = GRID_TH,
+                                                   int32_t defer_warp = MG_DEFER_WARP) {
+  if (defer_warp && nin * 8 < (int64_t)gridDim.x * NT) return 32;
+  return nin < (int64_t)gridDim.x * NT ? cta_th : grid_th;
 }
 
 // Returns true (and records v) when v goes to the grid bin.

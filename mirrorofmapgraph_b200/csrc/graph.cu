@@ -88,7 +88,16 @@ extern "C" mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t) {
                  {"sssp_heavy_small", t->sssp_heavy_small, 1, t->sssp_heavy},
                  {"sssp_ctas_per_sm", t->sssp_ctas_per_sm, 1, 8},
                  {"sssp_chunk_cap", t->sssp_chunk_cap, 0, 1 << 30},
-                 {"sssp_batch_heavy", t->sssp_batch_heavy, 1, 1 << 30}};
+                 {"sssp_batch_heavy", t->sssp_batch_heavy, 1, 1 << 30},
+                 {"bfs_cta_th", t->bfs_cta_th, 32, 1 << 30},
+                 {"bfs_grid_th", t->bfs_grid_th, 32, 1 << 30},
+                 {"bfs_defer_warp", t->bfs_defer_warp, 0, 1},
+                 {"bfs_persist_max", t->bfs_persist_max, 0, 1 << 30},
+                 {"bfs_persist_edges", t->bfs_persist_edges, 0, 1 << 30},
+                 {"bfs_alpha", t->bfs_alpha, 1, 1 << 20},
+                 {"bfs_beta", t->bfs_beta, 1, 1 << 20},
+                 {"bfs_sparse_degree", t->bfs_sparse_degree, 0, 1 << 20},
+                 {"bfs_ctas_per_sm", t->bfs_ctas_per_sm, 1, 8}};
   for (const Range &x : r) {
     if (x.v < x.lo || x.v > x.hi) {
       mg_set_error("mg_graph_set_tuning: %s = %d outside [%d, %d]", x.name, x.v, x.lo, x.hi);
@@ -843,6 +852,44 @@ mg_status mg_graph_info(const mg_graph *g, int64_t *n, int64_t *m, uint32_t *fla
   if (m) *m = g->m;
   if (flags) *flags = g->flags;
   if (device) *device = g->device;
+  return MG_OK;
+}
+
+namespace {
+// out[0] = max out-degree, out[1] = vertices without out-edges.
+__global__ void degree_stats_kernel(const int32_t *__restrict__ ro, int64_t n, unsigned long long *out) {
+  int32_t mx = 0;
+  unsigned long long zero = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = ro[i + 1] - ro[i];
+    mx = max(mx, d);
+    zero += d == 0;
+  }
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  for (int o = 16; o > 0; o >>= 1) zero += __shfl_xor_sync(0xffffffffu, zero, o);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, (unsigned long long)mx);
+    if (zero) atomicAdd(out + 1, zero);
+  }
+}
+}  // namespace
+
+mg_status mg_graph_degree_stats(mg_graph *g, int64_t *max_out_degree, int64_t *no_out_edges) {
+  if (!g) {
+    mg_set_error("mg_graph_degree_stats: graph is NULL");
+    return MG_ERR_ARG;
+  }
+  MG_TRY(graph_enter(g));
+  // two counters in the control block's spare bytes behind the DevCtl
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(g->ctl) + sizeof(DevCtl));
+  unsigned long long h[2] = {0, 0};
+  MG_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+  if (g->n > 0) degree_stats_kernel<<<g->num_sms * 4, 256, 0, g->stream>>>(g->ro, g->n, d);
+  MG_CUDA_TRY(cudaGetLastError());
+  MG_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+  MG_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  if (max_out_degree) *max_out_degree = (int64_t)h[0];
+  if (no_out_edges) *no_out_edges = (int64_t)h[1];
   return MG_OK;
 }
 

@@ -97,6 +97,15 @@ inline mg_tuning tuning_defaults() {
   t.sssp_heavy_small = 32;
   t.sssp_ctas_per_sm = 4;
   t.sssp_batch_heavy = 32;
+  t.bfs_cta_th = 512;
+  t.bfs_grid_th = 4096;
+  t.bfs_defer_warp = 1;
+  t.bfs_persist_max = 1 << 16;
+  t.bfs_persist_edges = 1 << 17;
+  t.bfs_alpha = 14;
+  t.bfs_beta = 24;
+  t.bfs_sparse_degree = 8;
+  t.bfs_ctas_per_sm = 4;
   return t;
 }
 

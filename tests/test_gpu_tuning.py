@@ -82,3 +82,86 @@ def test_tuning_ranges(rmat13):
         assert g.tuning() == before
     with pytest.raises(KeyError):
         g.set_tuning(no_such_field=1)
+
+
+BFS_SETTINGS = [
+    dict(bfs_cta_th=32, bfs_grid_th=64),                                 # CTA and grid bins take nearly all
+    dict(bfs_cta_th=1 << 30, bfs_grid_th=1 << 30, bfs_defer_warp=0),     # warp and thread bins only
+    dict(bfs_persist_max=0),                                             # no persistent levels
+    dict(bfs_persist_max=1 << 30, bfs_persist_edges=1 << 30),            # every push level persistent
+    dict(bfs_alpha=1, bfs_beta=1 << 20),
+    dict(bfs_alpha=1 << 20, bfs_beta=1),
+    dict(bfs_sparse_degree=1 << 20),                                     # AUTO stays top-down
+    dict(bfs_ctas_per_sm=1),
+    dict(bfs_ctas_per_sm=8),
+]
+
+
+@pytest.mark.parametrize("setting", BFS_SETTINGS, ids=lambda d: ",".join(f"{k}={v}" for k, v in d.items()))
+def test_bfs_tuning_settings_are_exact(rmat13, setting):
+    h, g = rmat13
+    g.set_tuning(**{**mg.Graph.default_tuning(), **setting})
+    try:
+        for s in (0, 99, h.n - 1):
+            ref = oracle.bfs(h.row_offsets, h.col_idx, [s])
+            for direction in ("auto", "push", "pull"):
+                for use_graph in (True, False):
+                    d, st = g.bfs([s], direction=direction, use_graph=use_graph)
+                    np.testing.assert_array_equal(d, ref)
+                    assert st["edges_traversed"] == int(np.diff(h.row_offsets)[ref >= 0].sum())
+    finally:
+        g.set_tuning(**mg.Graph.default_tuning())
+
+
+def test_bfs_tuning_both_directions():
+    h = mg.gen_rmat(12, 16, 44, symmetrize=False)
+    with mg.Graph(h.row_offsets, h.col_idx) as g:
+        for setting in BFS_SETTINGS[:4]:
+            g.set_tuning(**{**mg.Graph.default_tuning(), **setting})
+            for directed in (1, 0):
+                d, _ = g.bfs([3], directed=directed)
+                np.testing.assert_array_equal(d, oracle.bfs(h.row_offsets, h.col_idx, [3], directed=directed))
+
+
+def test_autotune_caches_per_graph_class(tmp_path):
+    from mirrorofmapgraph_b200 import tuning
+    cache = str(tmp_path / "tuning.json")
+    h = mg.gen_rmat(14, 16, 1001, symmetrize=True, weights="int", p0=1, p1=255)
+    with mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True) as g:
+        ent = tuning.tune(g, programs=("bfs", "sssp"), cache=cache, reps=1)
+        assert not ent["cached"] and ent["class"] == tuning.graph_class(g)
+        assert ent["class"].split("|")[1:] == ["n2^14", "deg2^5", ent["class"].split("|")[3], "sym", "w"]
+        got = g.tuning()
+        for prog in ("bfs", "sssp"):
+            assert ent["times_ms"][prog][0] <= ent["times_ms"][prog][1]
+            for f, vals in tuning.CANDIDATES[prog].items():
+                assert got[f] in vals + [mg.Graph.default_tuning()[f]]
+                assert ent["tuning"][f] == got[f]
+        db = tuning.load_cache(cache)
+        assert set(db[ent["class"]]["programs"]) == {"bfs", "sssp"}
+        # the tuned graph is exact
+        for s in (0, 5):
+            np.testing.assert_array_equal(g.bfs([s])[0], oracle.bfs(h.row_offsets, h.col_idx, [s]))
+            np.testing.assert_array_equal(g.sssp([s])[0], oracle.sssp(h.row_offsets, h.col_idx, h.weights_i32, [s]))
+    # another graph of the same class takes the cached setting without timing
+    h2 = mg.gen_rmat(14, 16, 1002, symmetrize=True, weights="int", p0=1, p1=255)
+    with mg.Graph(h2.row_offsets, h2.col_idx, h2.weights_i32, symmetric=True) as g2:
+        if tuning.graph_class(g2) == ent["class"]:
+            e2 = tuning.tune(g2, programs=("bfs",), cache=cache)
+            assert e2["cached"] and all(g2.tuning()[f] == ent["tuning"][f] for f in ent["tuning"])
+        g2.set_tuning(**mg.Graph.default_tuning())
+        assert tuning.apply_cached(g2, cache) == (tuning.graph_class(g2) in db)
+    # a batch program extends the class's entry
+    with mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True) as g:
+        e3 = tuning.tune(g, programs=("sssp_batch",), sources=[0, 1, 2, 3, 4, 5, 6, 7], cache=cache, reps=1)
+        assert not e3["cached"] and set(e3["programs"]) == {"bfs", "sssp", "sssp_batch"}
+        assert g.tuning()["sssp_batch_heavy"] in tuning.CANDIDATES["sssp_batch"]["sssp_batch_heavy"]
+
+
+def test_degree_stats(rmat13):
+    import ctypes as C
+    h, g = rmat13
+    mx, iso = C.c_int64(), C.c_int64()
+    assert g._lib.mg_graph_degree_stats(g._h, C.byref(mx), C.byref(iso)) == L.MG_OK
+    deg = np.diff(h.row_offsets)
+    assert mx.value == deg.max() and iso.value == int((deg == 0).sum())

@@ -241,3 +241,32 @@ def test_tuning_defaults_need_no_device():
     d = mg.Graph.default_tuning()
     assert d["sssp_heavy"] == 256 and d["sssp_heavy_small"] == 32 and d["sssp_ctas_per_sm"] == 4
     assert d["sssp_chunk_cap"] == 0 and d["sssp_batch_heavy"] == 32
+
+
+def test_tuning_search_and_cache(tmp_path):
+    """The autotuner's search (coordinate descent with a minimum gain) and its JSON
+    cache, with a synthetic cost in place of device timing."""
+    from mirrorofmapgraph_b200 import tuning
+    start = mg.Graph.default_tuning()
+    # cost: bfs fastest at cta_th 1024 and 8 CTAs/SM; sssp at heavy 128; a 1% gain is noise
+    def measure(prog, s):
+        if prog == "bfs":
+            return 10.0 + abs(s["bfs_cta_th"] - 1024) / 256 + (0 if s["bfs_ctas_per_sm"] == 8 else 1) \
+                + (0.05 if s["bfs_alpha"] != 14 else 0.0)
+        return 5.0 + abs(s["sssp_heavy"] - 128) / 64 + (0.001 if s["sssp_heavy_small"] == 16 else 0.0)
+    valid = lambda s: s["sssp_heavy_small"] <= s["sssp_heavy"]  # noqa: E731
+    best, times = tuning.search(start, ["bfs", "sssp"], measure, 0.02, valid)
+    assert best["bfs_cta_th"] == 1024 and best["bfs_ctas_per_sm"] == 8 and best["sssp_heavy"] == 128
+    assert best["bfs_alpha"] == 14 and best["sssp_heavy_small"] == start["sssp_heavy_small"]
+    assert times["bfs"][0] < times["bfs"][1] and times["sssp"][0] < times["sssp"][1]
+    k1 = tuning.class_key(1 << 20, 16 << 20, 40000, True, True, gpu="B200")
+    assert k1 == tuning.class_key(1 << 20, 16 << 20, 40000, True, True, gpu="B200")
+    assert k1 != tuning.class_key(1 << 20, 16 << 20, 64, True, True, gpu="B200")  # skew differs
+    assert k1.startswith("B200|n2^20|deg2^4|")
+    p = str(tmp_path / "sub" / "tuning.json")
+    assert tuning.load_cache(p) == {}
+    tuning.save_cache({k1: {"tuning": {"bfs_cta_th": 1024}}}, p)
+    assert tuning.load_cache(p)[k1]["tuning"]["bfs_cta_th"] == 1024
+    with open(p, "w") as f:
+        f.write("not json")
+    assert tuning.load_cache(p) == {}
