@@ -59,6 +59,9 @@ def parse():
     p.add_argument("--ref-scale", type=int, default=None,
                    help="R-MAT scale the reference arm runs on (default: --scale, the headline graph)")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-versus-looped section")
+    p.add_argument("--no-tune", action="store_true",
+                   help="keep the default traversal tuning (otherwise the BFS/SSSP thresholds are tuned on "
+                        "the device for the graph's class before the warm-up, or taken from the JSON cache)")
     p.add_argument("--batched-scale", type=int, default=20)
     p.add_argument("--pr-gather", default="auto", choices=["auto", "binned", "cached", "tma", "segmented"],
                    help="PageRank gather: autotuned per graph (default) or forced (for profiling one kernel)")
@@ -123,7 +126,17 @@ class Clocks:
         self.path = os.path.join(log_dir, f"clocks_rank{device_index}.csv") if log_dir and os.path.isdir(log_dir) \
             else f"/tmp/mg_clocks_{os.getpid()}_{device_index}.csv"
 
+    def _lines(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for ln in f if ln.endswith("\n"))
+        except OSError:
+            return 0
+
     def start(self):
+        """Starts sampling every 50 ms and waits (up to 5 s) for the first sample,
+        so that the sampler is running when the timed region begins."""
+        self.mark_at = 0
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
@@ -131,10 +144,22 @@ class Clocks:
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while self._lines() == 0 and time.time() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+
+    def mark(self):
+        """The timed region starts: samples from here on are the region's."""
+        self.mark_at = self._lines()
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # a region shorter than the sampling period still gets the first sample after it began
+        t0 = time.time()
+        while self._lines() <= self.mark_at and time.time() - t0 < 1.0 and self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -143,7 +168,9 @@ class Clocks:
         self.f.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for i, line in enumerate(open(self.path)):
+            if i < self.mark_at:
+                continue
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -159,7 +186,7 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def batched_section(scale, torch, mg):
+def batched_section(scale, torch, mg, tune=True):
     """Batched workload against looping the plain engine once per instance, on
     the same GPU: 64 BFS and 64 SSSP sources (half top-1% degree, half median
     degree), 256 personalised PageRank vectors (supports of U{1..32} vertices)
@@ -174,6 +201,12 @@ def batched_section(scale, torch, mg):
     out = torch.empty(64 * n, dtype=torch.int32, device="cuda")
     one = torch.empty(n, dtype=torch.int32, device="cuda")
     res = {}
+    if tune:
+        # both arms on the tuned setting: single-source BFS/SSSP (looped) and the batch
+        from mirrorofmapgraph_b200 import tuning
+        tuning.tune(g, programs=("bfs", "sssp"), sources=[int(s_) for s_ in srcs[:8]], reps=2)
+        ent = tuning.tune(g, programs=("sssp_batch",), sources=[int(s_) for s_ in srcs], reps=2)
+        res["tuning"] = {"class": ent["class"], "cached": ent["cached"], "tuning": ent["tuning"]}
 
     def pair(name, batched, looped, reps=2):
         # both arms warmed up once (plans, executable graphs), then timed
@@ -515,6 +548,14 @@ def run_ours(args):
     n, m = h.n, h.m
     srcs = sources(h, max(args.steps + args.warmup, 8), SEED + 1)
     g = mg.Graph(h.row_offsets, h.col_idx, h.weights_i32, symmetric=True)
+    tune_info = None
+    if not args.no_tune:
+        # mirrorofmapgraph_b200.tuning: device-timed choice of the BFS/SSSP thresholds
+        # for this graph's class (or the cached one), before anything is timed
+        from mirrorofmapgraph_b200 import tuning
+        ent = tuning.tune(g, programs=("bfs", "sssp"), sources=[int(s_) for s_ in srcs[:4]], reps=3)
+        tune_info = {"class": ent["class"], "cached": ent["cached"], "tuning": ent["tuning"],
+                     "times_ms_tuned_vs_default": ent["times_ms"]}
     stream = torch.cuda.ExternalStream(g.stream_ptr)
     depth = torch.empty(n, dtype=torch.int32, device="cuda")
     label = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -549,13 +590,14 @@ def run_ours(args):
         return {"bfs": (st_b["edges_traversed"], tb, st_b), "cc": (m, tc, st_c),
                 "pagerank": (m * st_p["iterations"], tp, st_p)}
 
+    clocks = Clocks(local)
+    clocks.start()  # running before the timed region starts (its first sample can take a while)
     for i in range(args.warmup):
         step(i)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
-    clocks.start()
+    clocks.mark()
     per = {"bfs": [0, 0.0], "cc": [0, 0.0], "pagerank": [0, 0.0]}
     launches = 0
     pr_iters = 0
@@ -665,11 +707,19 @@ def run_ours(args):
     # timed step still holds one full upload and the three read-backs.
     e2e_serial_s = 0.0
     if args.e2e_steps > 0:
-        ge = mg.Graph(ro_pin, ci_pin, symmetric=True, async_upload=True)
+        tuned = g.tuning() if tune_info else None
+
+        def new_graph(**kw):
+            gr = mg.Graph(ro_pin, ci_pin, symmetric=True, **kw)
+            if tuned:
+                gr.set_tuning(**tuned)
+            return gr
+
+        ge = new_graph(async_upload=True)
         for i in range(-1, args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            nxt = mg.Graph(ro_pin, ci_pin, symmetric=True, async_upload=True)
+            nxt = new_graph(async_upload=True)
             _, sb = ge.bfs([srcs[i % len(srcs)]], out=depth_pin)
             _, sc = ge.cc(out=label_pin)
             _, sp = ge.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT, out=rank_pin)
@@ -684,7 +734,7 @@ def run_ours(args):
         for i in range(-1, args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            with mg.Graph(ro_pin, ci_pin, symmetric=True) as gs:
+            with new_graph() as gs:
                 gs.bfs([srcs[i % len(srcs)]], out=depth_pin)
                 gs.cc(out=label_pin)
                 gs.pagerank(mode="normalized", alpha=ALPHA, tol=PR_TOL, max_iter=PR_MAX_IT, out=rank_pin)
@@ -716,6 +766,7 @@ def run_ours(args):
                                  if e2e_serial_s > 0 else None)},
         "gpu_launches": int(launches),
         "clocks": clock_info,
+        "tuning": tune_info,
     }
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
     if cpu_leg:
@@ -723,7 +774,7 @@ def run_ours(args):
     g.close()
     if not args.no_batched:
         try:
-            line["batched"] = batched_section(args.batched_scale, torch, mg)
+            line["batched"] = batched_section(args.batched_scale, torch, mg, tune=not args.no_tune)
         except Exception as e:
             line["batched"] = {"unavailable": f"{type(e).__name__}: {e}"}
     adj_keep = {}
