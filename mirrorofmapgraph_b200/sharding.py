@@ -90,3 +90,90 @@ def pagerank_sharded(graph, teleport: np.ndarray, group=None, **kw) -> np.ndarra
         x, _ = graph.pagerank(teleport=np.ascontiguousarray(teleport[lo:hi]), nvec=hi - lo, **kw)
         local = np.asarray(x).reshape(hi - lo, graph.n)
     return gather_rows(local, nvec, group)
+
+
+def ragged_partition(sizes, world: int) -> list[list[int]]:
+    """Member indices per rank for a ragged batch: longest first, each to the
+    least-loaded rank (ties to the lower rank), so the largest per-rank load is
+    within one member of the best split; each rank's list is in member order.
+    Deterministic, so every rank computes the same partition without talking."""
+    if world <= 0:
+        raise ValueError(f"world of {world}")
+    sizes = [int(s) for s in sizes]
+    load = [0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
+def _all_gather_1d(local: np.ndarray, lengths: list[int], group=None) -> list[np.ndarray]:
+    """All-gathers one 1-D int32 array per rank (rank r's has lengths[r] entries,
+    known to every rank) padded to the longest; returns the unpadded arrays."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    most = max(1, max(lengths))
+    on_gpu = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    pad = torch.zeros(most, dtype=torch.int32, device=dev)
+    if local.size:
+        pad[: local.size] = torch.from_numpy(np.ascontiguousarray(local, dtype=np.int32)).to(dev)
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return [parts[r][: lengths[r]].cpu().numpy() for r in range(world)]
+
+
+def bfs_ragged_sharded(members, srcs, group=None, symmetric: bool = False, make_graph=None, **kw):
+    """BFS of every member graph of a ragged batch from its source srcs[i], the
+    members split over the ranks (ragged_partition by vertices + edges): each rank
+    uploads only its members as one ragged graph (Graph.ragged, or
+    make_graph(members, symmetric=...)) and runs one mg_bfs_ragged; one
+    all-gather assembles every member's depth array on every rank. Returns
+    (depths, stats): depths[i] is member i's depth array, stats holds the summed
+    edges_traversed, the largest per-rank kernel_ms, and members_per_rank."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    srcs = np.asarray(srcs, dtype=np.int32)
+    if srcs.size != len(members):
+        raise ValueError(f"{srcs.size} sources for {len(members)} member graphs")
+    nv = [int(np.asarray(m.row_offsets).size) - 1 for m in members]
+    parts = ragged_partition([nv[i] + int(np.asarray(members[i].col_idx).size) for i in range(len(members))], world)
+    mine = parts[rank]
+    edges, ms = 0.0, 0.0
+    local = np.zeros(0, np.int32)
+    if mine:
+        if make_graph is None:
+            from .graph import Graph
+            make_graph = Graph.ragged
+        g = make_graph([members[i] for i in mine], symmetric=symmetric)
+        try:
+            depth, st = g.bfs_ragged(srcs[mine], **kw)
+        finally:
+            g.close()
+        local = np.asarray(depth, dtype=np.int32)
+        edges, ms = float(st["edges_traversed"]), float(st["kernel_ms"])
+    lengths = [sum(nv[i] for i in parts[r]) for r in range(world)]
+    if local.size != lengths[rank]:
+        raise ValueError(f"rank {rank}: ragged BFS returned {local.size} depths for {lengths[rank]} vertices")
+    chunks = _all_gather_1d(local, lengths, group)
+    depths: list = [None] * len(members)
+    for r in range(world):
+        off = 0
+        for i in parts[r]:
+            depths[i] = chunks[r][off:off + nv[i]]
+            off += nv[i]
+    on_gpu = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    t = torch.tensor([edges], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, group=group)
+    tm = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX, group=group)
+    return depths, {"edges_traversed": float(t.item()), "kernel_ms": float(tm.item()),
+                    "members_per_rank": [len(p) for p in parts]}
