@@ -363,8 +363,8 @@ mg_status mg_part_pr_result(mg_part *p, float *ranks, int32_t device_output, mg_
  * on a graph, for the first MG_TRACE_LEVELS levels. One record per level:
  *   BFS:      frontier = vertices expanded, frontier_edges = their out-edges,
  *             direction = MG_DIR_PUSH / MG_DIR_PULL;
- *   SSSP:     frontier = vertices relaxed, frontier_edges = out-edges of the
- *             vertices this round improved;
+ *   SSSP:     frontier = vertices relaxed, frontier_edges = their out-edges (the
+ *             edges the round inspects; both directions with directed = 0);
  *   PageRank: frontier = n, value = the iteration's L1 change;
  *   every record: time_ns, the device clock at the level's end.
  * *count = records written (min(levels, cap, MG_TRACE_LEVELS)). */

@@ -96,7 +96,6 @@ struct RelaxCtx {
   int32_t *qout, *qlen_out, *overflow;
   int32_t qcap;
   int32_t vmask;
-  int64_t reach_deg;  // out-degrees of vertices reached for the first time
   int64_t updates;
   // near-far: improvements to a distance >= thr go to the far pile instead
   int32_t delta;
@@ -150,10 +149,7 @@ __device__ __forceinline__ void relax_group(RelaxCtx &x, WarpStage &st, const in
   }
 #pragma unroll
   for (int r = 0; r < SSSP_U; r++) {
-    if (tr[r] && nd[r] < old[r]) {
-      x.updates++;
-      if (old[r] == INT_MAX) x.reach_deg += x.ro[(u[r] & x.vmask) + 1] - x.ro[u[r] & x.vmask];
-    }
+    if (tr[r] && nd[r] < old[r]) x.updates++;
     const bool fresh = u[r] >= 0 && !(ob[r] & (1u << (u[r] & 31)));
     ws_push(st, fresh && nearq[r], u[r], x.qout, x.qlen_out, x.qcap, x.overflow);
     warp_append(fresh && !nearq[r], u[r], x.far_out, x.far_len_out, x.qcap, x.overflow);
@@ -164,7 +160,7 @@ __device__ __forceinline__ RelaxCtx relax_ctx(const SsspArgs &a, DevCtl *c, int 
   const int fc = a.delta > 0 ? vload(&c->far_cur) : 0;
   return RelaxCtx{a.dist, (cur || a.delta <= 0) ? a.inq0 : a.inq1, a.ro, cur ? a.q0 : a.q1, &c->qlen[cur ^ 1],
                   &c->overflow, a.qcap,
-                  a.vmask, 0, 0, a.delta, vload(&c->thr), a.infar, fc ? a.far1 : a.far0, &c->far_len[fc]};
+                  a.vmask, 0, a.delta, vload(&c->thr), a.infar, fc ? a.far1 : a.far0, &c->far_len[fc]};
 }
 
 // The edges of the warp's 32 vertices (lane l brings vertex item v, its distance
@@ -323,7 +319,8 @@ __global__ void __launch_bounds__(SSSP_NT, 4) sssp_relax_kernel(SsspArgs a) {
     }
   }
   ws_flush(st, x.qout, x.qlen_out, x.qcap, x.overflow);
-  sssp_counters(c, s_sum, x.reach_deg, insp, nexp, x.updates);
+  // the round's frontier out-edges (its inspected edges) go to the trace record
+  sssp_counters(c, s_sum, insp, insp, nexp, x.updates);
 }
 
 // Pass 2: every warp of the grid relaxes chunks of the heavy vertices' edges; the
@@ -368,19 +365,16 @@ __global__ void __launch_bounds__(SSSP_NT, 4) sssp_chunk_kernel(SsspArgs a) {
     }
   }
   ws_flush(st, x.qout, x.qlen_out, x.qcap, x.overflow);
-  sssp_counters(c, s_sum, x.reach_deg, 0, 0, x.updates);
+  sssp_counters(c, s_sum, 0, 0, 0, x.updates);
   if (a.delta > 0 && last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
 }
 
 // Plain rounds, pass 3: the next frontier, compacted in item order from the
-// bitmap the round marked (SSSP_CW words per tile, one queue atomic per tile),
-// the words cleared for the next round, the frontier's out-edges summed for the
-// trace; the last CTA ends the round. Near-far rounds append to the queue as they
-// relax and end in pass 2.
-constexpr int SSSP_CW = SSSP_NT * 4;
+// bitmap the round marked (one word per thread, one queue atomic per CTA), the
+// words cleared for the next round; the last CTA ends the round. Near-far rounds
+// append to the queue as they relax and end in pass 2.
 __global__ void __launch_bounds__(SSSP_NT) sssp_compact_kernel(SsspArgs a) {
   __shared__ int32_t s_red[SSSP_NT / 32 + 1];
-  __shared__ int64_t s_sum[SSSP_NT / 32 + 1];
   __shared__ int32_t s_base;
   DevCtl *c = a.ctl;
   if (a.delta > 0 || vload(&c->done)) {
@@ -392,49 +386,27 @@ __global__ void __launch_bounds__(SSSP_NT) sssp_compact_kernel(SsspArgs a) {
   int32_t *qlen = &c->qlen[cur ^ 1];
   uint32_t *bm = a.inq0;
   const int64_t nwords = (a.n + 31) >> 5;
-  int64_t fdeg = 0;
-  for (int64_t t0 = (int64_t)blockIdx.x * SSSP_CW; t0 < nwords; t0 += (int64_t)gridDim.x * SSSP_CW) {
-    const int64_t w0 = t0 + (int64_t)threadIdx.x * 4;
-    uint32_t wd[4] = {0u, 0u, 0u, 0u};
-    if (w0 + 3 < nwords) {
-      uint4 *p = reinterpret_cast<uint4 *>(bm + w0);
-      const uint4 q = *p;
-      wd[0] = q.x;
-      wd[1] = q.y;
-      wd[2] = q.z;
-      wd[3] = q.w;
-      if (q.x | q.y | q.z | q.w) *p = make_uint4(0u, 0u, 0u, 0u);
-    } else {
-      for (int k = 0; k < 4; k++) {
-        if (w0 + k < nwords) {
-          wd[k] = bm[w0 + k];
-          if (wd[k]) bm[w0 + k] = 0u;
-        }
-      }
+  for (int64_t t0 = (int64_t)blockIdx.x * SSSP_NT; t0 < nwords; t0 += (int64_t)gridDim.x * SSSP_NT) {
+    const int64_t w = t0 + threadIdx.x;
+    uint32_t m = 0u;
+    if (w < nwords) {
+      m = bm[w];
+      if (m) bm[w] = 0u;
     }
-    const int32_t cnt = __popc(wd[0]) + __popc(wd[1]) + __popc(wd[2]) + __popc(wd[3]);
     int32_t tot;
-    int32_t pos = block_exclusive_scan<SSSP_NT>(cnt, s_red, &tot);
+    int32_t pos = block_exclusive_scan<SSSP_NT>((int32_t)__popc(m), s_red, &tot);
     if (threadIdx.x == 0) s_base = tot ? atomicAdd(qlen, tot) : 0;
     __syncthreads();
     pos += s_base;
-    for (int k = 0; k < 4; k++) {
-      uint32_t m = wd[k];
-      while (m) {
-        const int b = __ffs(m) - 1;
-        m &= m - 1;
-        const int32_t it = (int32_t)((w0 + k) * 32 + b);
-        const int32_t v = it & a.vmask;
-        fdeg += a.ro[v + 1] - a.ro[v];
-        if (pos < a.qcap) qout[pos] = it;
-        else c->overflow = 1;
-        pos++;
-      }
+    while (m) {
+      const int b = __ffs(m) - 1;
+      m &= m - 1;
+      if (pos < a.qcap) qout[pos] = (int32_t)(w * 32 + b);
+      else c->overflow = 1;
+      pos++;
     }
     __syncthreads();
   }
-  const int64_t b = block_sum<SSSP_NT>(fdeg, s_sum);
-  if (threadIdx.x == 0 && b) atomicAdd((unsigned long long *)&c->mf_next, (unsigned long long)b);
   if (last_block(&c->blocks_done) && threadIdx.x == 0) sssp_level_end(a);
 }
 
@@ -549,9 +521,7 @@ __global__ void sssp_clear_kernel(int32_t *dist, uint32_t *b0, uint32_t *b1, uin
 }
 
 __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, int32_t iter_cap) {
-  __shared__ int64_t s_sum[1024 / 32 + 1];
   DevCtl *c = a.ctl;
-  int64_t deg = 0;
   for (int i = threadIdx.x; i < nsrc; i += blockDim.x) {
     const int32_t s = srcs[i];
     const uint32_t bit = 1u << (s & 31);
@@ -559,15 +529,13 @@ __global__ void sssp_seed_kernel(SsspArgs a, const int32_t *srcs, int32_t nsrc, 
     // rounds mark the next frontier in inq0 and leave inq1 to the seeds
     if (!(atomicOr(&(a.delta > 0 ? a.inq0 : a.inq1)[s >> 5], bit) & bit)) {
       a.dist[s] = 0;
-      deg += a.ro[(s & a.vmask) + 1] - a.ro[s & a.vmask];
       const int pos = atomicAdd(&c->qlen[0], 1);
       if (pos < a.qcap) a.q0[pos] = s;
       else c->overflow = 1;
     }
   }
-  const int64_t t = block_sum<1024>(deg, s_sum);
+  __syncthreads();
   if (threadIdx.x == 0) {
-    if (a.delta > 0) c->mf_next = t;  // near-far: reached vertices' out-edges, seeds first
     c->iter_cap = iter_cap;
     c->thr = a.delta > 0 ? (int64_t)a.delta : INT64_MAX;
     c->far_min = INT_MAX;
@@ -1080,7 +1048,7 @@ static mg_status sssp_core(mg_graph *g, const int32_t *seeds, int32_t nseed, int
   sig.grid = grid;
   const int64_t nwords_all = (nitems + 31) / 32;
   const int cgrid =
-      (int)std::max<int64_t>(1, std::min<int64_t>((nwords_all + SSSP_CW - 1) / SSSP_CW, g->num_sms * 8));
+      (int)std::max<int64_t>(1, std::min<int64_t>((nwords_all + SSSP_NT - 1) / SSSP_NT, g->num_sms * 8));
   LoopBody body = [a, grid, cgrid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
     SsspArgs b = a;
     b.h = h;
