@@ -600,12 +600,20 @@ __global__ void __launch_bounds__(SEG_NT, 1) solve_rows_kernel(SolveArgs a, PrbA
     group_comp_reduce<32>(t);
     if (lane == 0) update(hub0 + h, p.hrows[h], t);
   }
+  // Rows without in-edges (the last groups of the degree order) take only the
+  // teleport and dangling terms: one coalesced pass over their positions, outside
+  // the group counter.
+  for (int64_t pos = sg.nrgroups_e * 32 + (int64_t)blockIdx.x * SEG_NT + threadIdx.x; pos < sg.nrgroups * 32;
+       pos += (int64_t)gridDim.x * SEG_NT) {
+    const int32_t r = sg.rrow[pos];
+    if (r >= 0) update(pos, r, Comp{0.f, 0.f});
+  }
   auto gather = [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); };
   for (;;) {
     int32_t gi = 0;
     if (lane == 0) gi = atomicAdd(sg.rgrab, 1);
     gi = __shfl_sync(FULL, gi, 0);
-    if (gi >= sg.nrgroups) break;
+    if (gi >= sg.nrgroups_e) break;
     const int32_t r = sg.rrow[(int64_t)gi * 32 + lane];
     const int64_t s0 = sg.rgofs[gi];
     const int32_t depth = (int32_t)((sg.rgofs[gi + 1] - s0) >> 5);
@@ -1081,9 +1089,11 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
       if (d < T) rrow[start[dmax - d]++] = (int32_t)r;
     }
     std::vector<int64_t> rg((size_t)sp.nrgroups + 1, 0);
+    sp.nrgroups_e = 0;
     for (int64_t gi = 0; gi < sp.nrgroups; gi++) {
       const int32_t r0 = rrow[gi * 32];  // the group's longest row
       rg[gi + 1] = rg[gi] + 32 * (int64_t)(co[r0 + 1] - co[r0]);
+      if (co[r0 + 1] > co[r0]) sp.nrgroups_e = gi + 1;
     }
     sp.nrell = rg[sp.nrgroups];
     sp.npos = sp.nrgroups * 32 + nh;
@@ -1341,7 +1351,8 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
       sp.p.wstart[PRB_BINS] = sp.p.wstart[6];  // hub rows are phase 1's, not work items of phase 2
       sp.sg = SegArgs{seg->ent,  seg->gofs, seg->pidx,   seg->pwts,  seg->bgrp,  seg->cta,
                       seg->bdense, (n + 31) & ~(int64_t)31, seg->S, seg->nblocks, seg->rrow, seg->rgofs,
-                      seg->ridx, seg->rwts, seg->rgrab, seg->nrgroups, seg->pslot, pos_s, pos_t};
+                      seg->ridx, seg->rwts, seg->rgrab, seg->nrgroups, seg->nrgroups_e, seg->pslot, pos_s,
+                      pos_t};
       a.gswz = 1;
       a.vpos = seg->ppos;
       sp.ppos = seg->ppos;

@@ -100,6 +100,7 @@ struct SegPlan {
   float *rwts = nullptr;     // their weights (weighted graphs)
   int32_t *rgrab = nullptr;  // group counter of phase 2 (zero between launches)
   int64_t nrgroups = 0, nrell = 0;
+  int64_t nrgroups_e = 0;    // groups holding an edge (the rest, last in the order, hold rows without edges)
   // Positions of the iterate during a segmented solve: g * 32 + l for phase 2's
   // group g, lane l, then nrgroups * 32 + h for hub h. Per position: its row (-1
   // for empty lanes) and the row's cached-column slot.
@@ -126,6 +127,7 @@ struct SegArgs {
   const float *rwts;
   int32_t *rgrab;
   int64_t nrgroups;
+  int64_t nrgroups_e;    // groups with an edge; positions from nrgroups_e * 32 on are rows without one
   const int32_t *pslot;  // per position: cached-column slot
   const float *ps;       // per position: row sum s (0: dangling), filled per solve
   const float *pt;       // per position: teleport entry (nullptr: uniform), filled per solve
