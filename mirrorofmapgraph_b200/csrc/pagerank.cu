@@ -609,11 +609,30 @@ __global__ void __launch_bounds__(SEG_NT, 1) solve_rows_kernel(SolveArgs a, PrbA
     if (r >= 0) update(pos, r, Comp{0.f, 0.f});
   }
   auto gather = [&](int32_t col) { return col < 0 ? s_hub[col & 0x7fffffff] : __ldg(gold + col); };
+  // Short groups (depth <= SEG_SHORT; rows of a few edges, most of the groups that
+  // hold an edge): a fixed share per warp, two groups at a time with their loads
+  // issued together, no counter and no header round trip in between.
+  {
+    const int64_t wg = (int64_t)blockIdx.x * (SEG_NT / 32) + (threadIdx.x >> 5);
+    for (int64_t ga = sg.nrgroups_l + 2 * wg; ga < sg.nrgroups_e; ga += 2 * nw) {
+      const int64_t gb = ga + 1 < sg.nrgroups_e ? ga + 1 : -1;
+      const int64_t pa = ga * 32 + lane, pb = gb * 32 + lane;
+      const int32_t ra = sg.rrow[pa], rb = gb >= 0 ? sg.rrow[pb] : -1;
+      const int64_t a0 = sg.rgofs[ga], a1 = sg.rgofs[ga + 1];
+      const int64_t b0 = gb >= 0 ? sg.rgofs[gb] : 0, b1 = gb >= 0 ? sg.rgofs[gb + 1] : 0;
+      Comp va, vb;
+      sell_short2<WEIGHTED>(sg.ridx + a0 + lane, WEIGHTED ? sg.rwts + a0 + lane : nullptr, (int32_t)((a1 - a0) >> 5),
+                            sg.ridx + b0 + lane, WEIGHTED ? sg.rwts + b0 + lane : nullptr, (int32_t)((b1 - b0) >> 5),
+                            gather, va, vb);
+      if (ra >= 0) update(pa, ra, va);
+      if (rb >= 0) update(pb, rb, vb);
+    }
+  }
   for (;;) {
     int32_t gi = 0;
     if (lane == 0) gi = atomicAdd(sg.rgrab, 1);
     gi = __shfl_sync(FULL, gi, 0);
-    if (gi >= sg.nrgroups_e) break;
+    if (gi >= sg.nrgroups_l) break;
     const int32_t r = sg.rrow[(int64_t)gi * 32 + lane];
     const int64_t s0 = sg.rgofs[gi];
     const int32_t depth = (int32_t)((sg.rgofs[gi + 1] - s0) >> 5);
@@ -1090,10 +1109,12 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
     }
     std::vector<int64_t> rg((size_t)sp.nrgroups + 1, 0);
     sp.nrgroups_e = 0;
+    sp.nrgroups_l = 0;
     for (int64_t gi = 0; gi < sp.nrgroups; gi++) {
       const int32_t r0 = rrow[gi * 32];  // the group's longest row
       rg[gi + 1] = rg[gi] + 32 * (int64_t)(co[r0 + 1] - co[r0]);
       if (co[r0 + 1] > co[r0]) sp.nrgroups_e = gi + 1;
+      if (co[r0 + 1] - co[r0] > SEG_SHORT) sp.nrgroups_l = gi + 1;
     }
     sp.nrell = rg[sp.nrgroups];
     sp.npos = sp.nrgroups * 32 + nh;
@@ -1351,8 +1372,8 @@ static mg_status solve_setup(mg_graph *g, bool adjoint, bool weighted, const flo
       sp.p.wstart[PRB_BINS] = sp.p.wstart[6];  // hub rows are phase 1's, not work items of phase 2
       sp.sg = SegArgs{seg->ent,  seg->gofs, seg->pidx,   seg->pwts,  seg->bgrp,  seg->cta,
                       seg->bdense, (n + 31) & ~(int64_t)31, seg->S, seg->nblocks, seg->rrow, seg->rgofs,
-                      seg->ridx, seg->rwts, seg->rgrab, seg->nrgroups, seg->nrgroups_e, seg->pslot, pos_s,
-                      pos_t};
+                      seg->ridx, seg->rwts, seg->rgrab, seg->nrgroups, seg->nrgroups_e, seg->nrgroups_l,
+                      seg->pslot, pos_s, pos_t};
       a.gswz = 1;
       a.vpos = seg->ppos;
       sp.ppos = seg->ppos;

@@ -101,6 +101,7 @@ struct SegPlan {
   int32_t *rgrab = nullptr;  // group counter of phase 2 (zero between launches)
   int64_t nrgroups = 0, nrell = 0;
   int64_t nrgroups_e = 0;    // groups holding an edge (the rest, last in the order, hold rows without edges)
+  int64_t nrgroups_l = 0;    // groups deeper than SEG_SHORT (the first ones in the order)
   // Positions of the iterate during a segmented solve: g * 32 + l for phase 2's
   // group g, lane l, then nrgroups * 32 + h for hub h. Per position: its row (-1
   // for empty lanes) and the row's cached-column slot.
@@ -128,6 +129,7 @@ struct SegArgs {
   int32_t *rgrab;
   int64_t nrgroups;
   int64_t nrgroups_e;    // groups with an edge; positions from nrgroups_e * 32 on are rows without one
+  int64_t nrgroups_l;    // groups deeper than SEG_SHORT; [nrgroups_l, nrgroups_e) are short
   const int32_t *pslot;  // per position: cached-column slot
   const float *ps;       // per position: row sum s (0: dangling), filled per solve
   const float *pt;       // per position: teleport entry (nullptr: uniform), filled per solve
@@ -335,6 +337,53 @@ __device__ __forceinline__ Comp sell_walk(const int32_t *q, const float *qw, int
     }
   }
   return acc;
+}
+
+// Two short rows (depth <= SEG_SHORT each, sliced-ELL layout as in sell_walk) of
+// two groups walked together: both rows' index loads, then both rows' gathers,
+// then the sums, each row's in the order sell_walk adds them (so the results are
+// the same bits).
+constexpr int SEG_SHORT = 4;
+template <bool WEIGHTED, typename Gather>
+__device__ __forceinline__ void sell_short2(const int32_t *qa, const float *qwa, int32_t da, const int32_t *qb,
+                                            const float *qwb, int32_t db, Gather &gather, Comp &acc_a, Comp &acc_b) {
+  int32_t ca[SEG_SHORT], cb[SEG_SHORT];
+  float wa[SEG_SHORT], wb[SEG_SHORT], va[SEG_SHORT], vb[SEG_SHORT];
+#pragma unroll
+  for (int j = 0; j < SEG_SHORT; j++) {
+    ca[j] = j < da ? prb_stream(qa + 32 * j) : -1;
+    cb[j] = j < db ? prb_stream(qb + 32 * j) : -1;
+    wa[j] = (WEIGHTED && j < da) ? prb_stream(qwa + 32 * j) : 0.f;
+    wb[j] = (WEIGHTED && j < db) ? prb_stream(qwb + 32 * j) : 0.f;
+  }
+#pragma unroll
+  for (int j = 0; j < SEG_SHORT; j++) {
+    va[j] = ca[j] != -1 ? gather(ca[j]) : 0.f;
+    vb[j] = cb[j] != -1 ? gather(cb[j]) : 0.f;
+  }
+  acc_a = Comp{0.f, 0.f};
+  acc_b = Comp{0.f, 0.f};
+#pragma unroll
+  for (int j = 0; j < SEG_SHORT; j++) {
+    if (ca[j] != -1) {
+      if (WEIGHTED) {
+        const float p = wa[j] * va[j];
+        two_sum_add(acc_a, p);
+        acc_a.lo += __fmaf_rn(wa[j], va[j], -p);
+      } else {
+        two_sum_add(acc_a, va[j]);
+      }
+    }
+    if (cb[j] != -1) {
+      if (WEIGHTED) {
+        const float p = wb[j] * vb[j];
+        two_sum_add(acc_b, p);
+        acc_b.lo += __fmaf_rn(wb[j], vb[j], -p);
+      } else {
+        two_sum_add(acc_b, vb[j]);
+      }
+    }
+  }
 }
 
 // Phase 1 of a segmented iteration on one CTA: walks the CTA's groups block by
