@@ -1023,7 +1023,8 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
     for (int32_t key = 0; key < SEG_FMAX; key++) {
       const int32_t len = SEG_FMAX - key, cnt = lc[(size_t)b * SEG_FMAX + key];
       cursor[(size_t)b * SEG_FMAX + key] = (int32_t)(s0 + k);
-      for (int64_t kk = (k + 31) / 32 * 32; kk < k + cnt; kk += 32) gdepth.push_back(len);
+      // depths even: a lane's index words hold two steps (seg_pk)
+      for (int64_t kk = (k + 31) / 32 * 32; kk < k + cnt; kk += 32) gdepth.push_back((len + 1) & ~1);
       k += cnt;
     }
     grp += (k + 31) / 32;
@@ -1045,7 +1046,7 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
   MG_TRY(scratch((void **)&sp.bins.hpart, sizeof(Comp) * (size_t)std::max<int32_t>(nfrag, 1)));
   MG_TRY(dev_alloc(g, (void **)&sp.ent, sizeof(int2) * slots));
   MG_TRY(dev_alloc(g, (void **)&sp.gofs, sizeof(int64_t) * gofs.size()));
-  MG_TRY(dev_alloc(g, (void **)&sp.pidx, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nell, 1)));
+  MG_TRY(dev_alloc(g, (void **)&sp.pidx, sizeof(uint16_t) * (size_t)std::max<int64_t>(sp.nell, 2)));
   if (weighted) MG_TRY(dev_alloc(g, (void **)&sp.pwts, sizeof(float) * (size_t)std::max<int64_t>(sp.nell, 1)));
   MG_TRY(dev_alloc(g, (void **)&sp.bgrp, sizeof(int32_t) * bgrp.size()));
   MG_TRY(dev_alloc(g, (void **)&sp.bdense, (size_t)std::max<int64_t>(B, 1)));
@@ -1058,7 +1059,7 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
   MG_TRY(scratch((void **)&flen, sizeof(int32_t) * slots));
   tmp.p.push_back(flen);
   MG_CUDA_TRY(cudaMemsetAsync(sp.ent, 0xff, sizeof(int2) * slots, s));
-  MG_CUDA_TRY(cudaMemsetAsync(sp.pidx, 0xff, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nell, 1), s));
+  MG_CUDA_TRY(cudaMemsetAsync(sp.pidx, 0xff, sizeof(uint16_t) * (size_t)std::max<int64_t>(sp.nell, 2), s));
   if (weighted) MG_CUDA_TRY(cudaMemsetAsync(sp.pwts, 0, sizeof(float) * (size_t)std::max<int64_t>(sp.nell, 1), s));
   MG_CUDA_TRY(cudaMemcpyAsync(sp.gofs, gofs.data(), sizeof(int64_t) * gofs.size(), cudaMemcpyHostToDevice, s));
   MG_CUDA_TRY(cudaMemcpyAsync(sp.bgrp, bgrp.data(), sizeof(int32_t) * bgrp.size(), cudaMemcpyHostToDevice, s));
@@ -1075,7 +1076,7 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
                                                   sp.bins.hrows, sp.bins.hbase, S, (int32_t)B, lencnt, sp.sidx,
                                                   sp.swts, sp.ent, fsrc, flen);
   if (grp > 0)
-    seg_sell_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.ent, fsrc, flen, sp.gofs, grp, sp.sidx, sp.swts, sp.pidx,
+    seg_sell_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.ent, fsrc, flen, sp.gofs, grp, sp.sidx, sp.swts, S, sp.pidx,
                                                    sp.pwts);
   MG_CUDA_TRY(cudaGetLastError());
   // Phase 2's rows (in-degree below T) as sliced ELL, longest first: a counting
@@ -2383,7 +2384,8 @@ extern "C" mg_status mg_debug_seg_plan(mg_graph *g, int32_t hub_edges, int32_t b
     return MG_OK;
   };
   std::vector<int32_t> hrows(nh), hbase(nh + 1), hcount(nh), co(g->n + 1), ri(m), bgrp(sp->nblocks + 1),
-      cta(sp->grid + 1), pidx(sp->nell);
+      cta(sp->grid + 1);
+  std::vector<uint16_t> pidx(sp->nell);
   std::vector<int2> ent((size_t)ng * 32);
   std::vector<int64_t> gofs(ng + 1);
   MG_TRY(d2h(hrows.data(), sp->bins.hrows, 4 * nh));
@@ -2393,7 +2395,7 @@ extern "C" mg_status mg_debug_seg_plan(mg_graph *g, int32_t hub_edges, int32_t b
   MG_TRY(d2h(ri.data(), g->ri, 4 * m));
   MG_TRY(d2h(bgrp.data(), sp->bgrp, 4 * bgrp.size()));
   MG_TRY(d2h(cta.data(), sp->cta, 4 * cta.size()));
-  MG_TRY(d2h(pidx.data(), sp->pidx, 4 * pidx.size()));
+  MG_TRY(d2h(pidx.data(), sp->pidx, 2 * pidx.size()));
   MG_TRY(d2h(ent.data(), sp->ent, sizeof(int2) * ent.size()));
   MG_TRY(d2h(gofs.data(), sp->gofs, 8 * gofs.size()));
   MG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2413,8 +2415,8 @@ extern "C" mg_status mg_debug_seg_plan(mg_graph *g, int32_t hub_edges, int32_t b
         fhub[e.x] = e.y;
         const int64_t depth = (gofs[gi + 1] - gofs[gi]) / 32;
         for (int64_t i = 0; i < depth; i++) {
-          const int32_t c = pidx[gofs[gi] + 32 * i + l];
-          if (c >= 0) fcols[e.x].push_back(c);
+          const uint16_t off = pidx[seg_pk(gofs[gi], l, i)];
+          if (off != 0xffffu) fcols[e.x].push_back((int32_t)(b * sp->S + off));
         }
       }
   int64_t once = 0, match = 0;

@@ -87,7 +87,8 @@ struct SegPlan {
   float *swts = nullptr;     // edge weights in sidx's order (weighted graphs)
   int2 *ent = nullptr;       // {fragment id, hub} of every group lane ({-1, -1}: empty lane)
   int64_t *gofs = nullptr;   // first sliced-ELL entry of each group, ngroups + 1 entries
-  int32_t *pidx = nullptr;   // sliced-ELL column indices of the hub fragments (-1: padding)
+  uint16_t *pidx = nullptr;  // sliced-ELL column offsets of the hub fragments within their block, two
+                             // steps of a lane per 32-bit word (seg_pk; 0xFFFF: padding)
   float *pwts = nullptr;     // their edge weights (weighted graphs)
   int32_t *bgrp = nullptr;   // first group of each block, nblocks + 1 entries
   uint8_t *bdense = nullptr; // 1: the block is staged in shared memory; 0: gathered from global
@@ -116,7 +117,7 @@ struct SegPlan {
 struct SegArgs {
   const int2 *ent;
   const int64_t *gofs;
-  const int32_t *pidx;
+  const uint16_t *pidx;
   const float *pwts;
   const int32_t *bgrp, *cta;
   const uint8_t *bdense;
@@ -246,20 +247,28 @@ __global__ void __launch_bounds__(32) seg_fill_kernel(const int32_t *__restrict_
 // Sliced-ELL layout: one warp per group copies lane l's fragment (fsrc, flen) into
 // entries gofs[g] + 32 i + l, as permuted x/s positions (seg_swz). Padding entries
 // keep the -1 they were cleared to.
+// Entry of step i of lane `lane` in a group whose entries start at g0 (even): the
+// 16-bit column offsets of a lane's steps 2p and 2p + 1 share one 32-bit word, the
+// 32 lanes' words of a step pair are consecutive.
+__host__ __device__ __forceinline__ int64_t seg_pk(int64_t g0, int lane, int64_t i) {
+  return g0 + 64 * (i >> 1) + 2 * lane + (i & 1);
+}
+
 __global__ void __launch_bounds__(256) seg_sell_kernel(const int2 *__restrict__ ent, const int32_t *__restrict__ fsrc,
                                                        const int32_t *__restrict__ flen,
                                                        const int64_t *__restrict__ gofs, int64_t ngroups,
                                                        const int32_t *__restrict__ sidx, const float *__restrict__ swts,
-                                                       int32_t *__restrict__ pidx, float *__restrict__ pwts) {
+                                                       int32_t S, uint16_t *__restrict__ pidx,
+                                                       float *__restrict__ pwts) {
   const int lane = threadIdx.x & 31;
   for (int64_t gi = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < ngroups;
        gi += ((int64_t)gridDim.x * blockDim.x) >> 5) {
     const int64_t slot = gi * 32 + lane;
     if (ent[slot].x < 0) continue;
     const int32_t src = fsrc[slot], len = flen[slot];
-    const int64_t o = gofs[gi] + lane;
+    const int64_t g0 = gofs[gi], o = g0 + lane;
     for (int32_t i = 0; i < len; i++) {
-      pidx[o + 32 * (int64_t)i] = seg_swz(sidx[src + i]);
+      pidx[seg_pk(g0, lane, i)] = (uint16_t)(seg_swz(sidx[src + i]) % S);  // a fragment lies in one block
       if (pwts) pwts[o + 32 * (int64_t)i] = swts[src + i];
     }
   }
@@ -335,6 +344,58 @@ __device__ __forceinline__ Comp sell_walk(const int32_t *q, const float *qw, int
       c[j] = cn[j];
       w[j] = wn[j];
     }
+  }
+  return acc;
+}
+
+// One lane's hub fragment (phase 1): `depth` (even) steps of 16-bit block offsets,
+// two per 32-bit word at q + 32 p (seg_pk), weights (weighted graphs) one per step
+// at qw + 32 i; index words loaded one round of U steps ahead of the gathers, the
+// sum taken in step order like sell_walk's. 0xFFFF entries are padding.
+template <bool WEIGHTED, int U, typename Gather>
+__device__ __forceinline__ Comp sell_walk16(const uint32_t *q, const float *qw, int32_t depth, Gather &gather) {
+  static_assert(U % 2 == 0, "two steps per index word");
+  Comp acc{0.f, 0.f};
+  uint32_t c[U / 2];
+  float w[U];
+#pragma unroll
+  for (int p = 0; p < U / 2; p++) c[p] = 2 * p < depth ? prb_stream(q + 32 * p) : 0xffffffffu;
+#pragma unroll
+  for (int j = 0; j < U; j++) w[j] = (WEIGHTED && j < depth) ? prb_stream(qw + 32 * j) : 0.f;
+  for (int32_t i = 0; i < depth; i += U) {
+    uint32_t cn[U / 2];
+    float wn[U];
+#pragma unroll
+    for (int p = 0; p < U / 2; p++) {
+      const int32_t k = i + U + 2 * p;
+      cn[p] = k < depth ? prb_stream(q + 32 * (k >> 1)) : 0xffffffffu;
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      const int32_t k = i + U + j;
+      wn[j] = (WEIGHTED && k < depth) ? prb_stream(qw + 32 * k) : 0.f;
+    }
+    float v[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      const uint32_t off = (c[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+      v[j] = off != 0xffffu ? gather((int32_t)off) : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+      if (((c[j >> 1] >> (16 * (j & 1))) & 0xffffu) == 0xffffu) continue;
+      if (WEIGHTED) {
+        const float pr = w[j] * v[j];
+        two_sum_add(acc, pr);
+        acc.lo += __fmaf_rn(w[j], v[j], -pr);
+      } else {
+        two_sum_add(acc, v[j]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < U / 2; p++) c[p] = cn[p];
+#pragma unroll
+    for (int j = 0; j < U; j++) w[j] = wn[j];
   }
   return acc;
 }
@@ -436,9 +497,9 @@ __device__ __forceinline__ void seg_phase(const SegArgs &sg, const float *gold, 
       }
       phase ^= 1;
     }
-    const int32_t base = (int32_t)c_lo;
-    auto from_smem = [&](int32_t c) { return sbuf[c - base]; };
-    auto from_global = [&](int32_t c) { return __ldg(gold + c); };
+    const float *gblk = gold + c_lo;
+    auto from_smem = [&](int32_t off) { return sbuf[off]; };
+    auto from_global = [&](int32_t off) { return __ldg(gblk + off); };
     for (;;) {
       int32_t gi = 0;
       if (lane == 0) gi = atomicAdd(next, 1);
@@ -447,11 +508,11 @@ __device__ __forceinline__ void seg_phase(const SegArgs &sg, const float *gold, 
       const int2 e = sg.ent[(int64_t)gi * 32 + lane];
       const int64_t s0 = sg.gofs[gi];
       const int32_t steps = (int32_t)((sg.gofs[gi + 1] - s0) >> 5);
-      const int32_t *q = sg.pidx + s0 + lane;
+      const uint32_t *q = reinterpret_cast<const uint32_t *>(sg.pidx + s0) + lane;
       const float *qw = WEIGHTED ? sg.pwts + s0 + lane : nullptr;
       constexpr int U = WEIGHTED ? 4 : SEG_U;
-      const Comp acc = dense ? sell_walk<WEIGHTED, U>(q, qw, steps, from_smem)
-                             : sell_walk<WEIGHTED, U>(q, qw, steps, from_global);
+      const Comp acc = dense ? sell_walk16<WEIGHTED, U>(q, qw, steps, from_smem)
+                             : sell_walk16<WEIGHTED, U>(q, qw, steps, from_global);
       fin(e, acc);
     }
     __syncthreads();  // the segment ends for every warp at once
