@@ -64,9 +64,12 @@ constexpr uint32_t SEG_COPY = 32768;    // bytes per bulk copy of a block load
 // factor of a global gather over a shared-memory one. A block is staged in shared
 // memory when it holds at least SEG_DENSE entries; the groups of sparser blocks
 // gather straight from global memory (a block load would cost more than it saves).
+// With 16-bit indices a shared-memory step costs less next to a global gather:
+// factor 6 balanced the CTAs best (R-MAT s22: 300.5 us per iteration against
+// 305.0-305.5 with 4, 300.9-301.3 with 8; group costs 256 and 1024 were slower).
 constexpr int64_t SEG_GROUP_COST = 512;
 constexpr int64_t SEG_LOAD_COST = 65536;
-constexpr int64_t SEG_GLOBAL_FACTOR = 4;
+constexpr int64_t SEG_GLOBAL_FACTOR = 6;
 constexpr int64_t SEG_DENSE = 131072;
 #ifndef SEG_U
 #define SEG_U 8                         // ELL steps a lane loads before its first add
