@@ -99,6 +99,12 @@ __device__ void bfs_level_end(const BfsArgs &a) {
   c->mf_next = 0;
   c->blocks_done = 0;
   c->big_len = 0;
+  // the persistent kernel's per-level counters start from zero when it next runs
+  for (int k = 0; k < 3; k++) {
+    c->pq[k] = 0;
+    c->pm[k] = 0;
+    c->pb[k] = 0;
+  }
   const bool over = vload(&c->overflow) != 0;
   const bool done = nf == 0 || lvl >= c->iter_cap || over;
   int dir = vload(&c->dir);
@@ -565,14 +571,27 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
   struct Sig {
     BfsArgs a;
     int grid;
+    int32_t tail_max, tail_edges;
   } sig;
   std::memset(&sig, 0, sizeof(sig));
   sig.a = a;
   sig.grid = grid;
-  LoopBody body = [a, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
+  sig.tail_max = g->tune.bfs_tail_max;
+  sig.tail_edges = g->tune.bfs_tail_edges;
+  // Tail levels: one CTA runs the persistent kernel at the top of every iteration
+  // (its grid barrier is the CTA's own), so a run of tiny push levels (at most
+  // bfs_tail_max vertices and bfs_tail_edges out-edges) costs one launch instead of
+  // a launch sequence per level; on a larger frontier it returns at once and the
+  // per-level kernels go on from the same control block.
+  BfsArgs ta = a;
+  ta.persist_max = g->tune.bfs_tail_max;
+  ta.persist_edges = g->tune.bfs_tail_edges;
+  const bool tail = ta.persist_max > 0 && ta.persist_edges > 0 && o.direction != MG_DIR_PULL;
+  LoopBody body = [a, ta, tail, grid](cudaStream_t st, cudaGraphConditionalHandle h, int use_cond) {
     BfsArgs b = a;
     b.h = h;
     b.use_cond = use_cond;
+    if (tail) bfs_persist_kernel<<<1, BFS_NT, 0, st>>>(ta);
     bfs_push_kernel<<<grid, BFS_NT, 0, st>>>(b);
     bfs_push_big_kernel<<<grid, BFS_NT, 0, st>>>(b);
     bfs_pull_kernel<<<grid, BFS_NT, 0, st>>>(b);
@@ -593,7 +612,8 @@ extern "C" mg_status mg_bfs(mg_graph *g, const int32_t *srcs, int32_t nsrc, int3
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
     stats->kernel_ms = ms;
     stats->status_detail = hc.levels_pull;
-    stats->launches = 2 + persist_launches + (use_graph ? 4 * (int64_t)hc.body_iters : 3 * (int64_t)hc.level);
+    const int64_t per = 3 + (tail ? 1 : 0);
+    stats->launches = 2 + persist_launches + (use_graph ? (per + 1) * (int64_t)hc.body_iters : per * g->host_iters);
   }
   if (hc.status == MG_ERR_TIMEOUT) {
     mg_set_error("mg_bfs: a grid barrier of the persistent levels timed out");

@@ -128,6 +128,7 @@ mg_status run_loop(mg_graph *g, int slot, const void *sig, size_t sig_len, bool 
     return MG_OK;
   }
   for (int64_t it = 0; it < max_iters; it++) {
+    g->host_iters = it + 1;
     body(g->stream, 0, 0);
     MG_CUDA_TRY(cudaGetLastError());
     MG_CUDA_TRY(cudaMemcpyAsync(&g->ctl_host->done, &g->ctl->done, sizeof(int32_t), cudaMemcpyDeviceToHost,

@@ -106,6 +106,8 @@ inline mg_tuning tuning_defaults() {
   t.bfs_beta = 24;
   t.bfs_sparse_degree = 8;
   t.bfs_ctas_per_sm = 4;
+  t.bfs_tail_max = 2048;
+  t.bfs_tail_edges = 16384;
   return t;
 }
 
@@ -140,6 +142,7 @@ struct mg_graph {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   void *cache = nullptr;       // cached executable loop graphs (engine.cu)
   mg_tuning tune = tuning_defaults();  // traversal thresholds and launch shapes (mg_graph_set_tuning)
+  int64_t host_iters = 0;              // body calls of the last host-driven loop (run_loop)
 };
 
 // Every device allocation of the library goes through here: cudaMallocAsync on

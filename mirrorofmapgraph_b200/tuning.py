@@ -36,6 +36,8 @@ CANDIDATES: dict[str, dict[str, list[int]]] = {
         "bfs_alpha": [8, 14, 24],
         "bfs_beta": [12, 24, 48],
         "bfs_ctas_per_sm": [2, 4, 8],
+        "bfs_tail_max": [0, 512, 2048, 8192],
+        "bfs_tail_edges": [4096, 16384, 65536],
     },
     "sssp": {
         "sssp_heavy": [64, 128, 256, 512],

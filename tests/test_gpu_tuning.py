@@ -94,6 +94,8 @@ BFS_SETTINGS = [
     dict(bfs_sparse_degree=1 << 20),                                     # AUTO stays top-down
     dict(bfs_ctas_per_sm=1),
     dict(bfs_ctas_per_sm=8),
+    dict(bfs_tail_max=0),                                                # no single-CTA tail levels
+    dict(bfs_tail_max=1 << 30, bfs_tail_edges=1 << 30, bfs_persist_max=0),  # every push level in one CTA
 ]
 
 
