@@ -414,7 +414,7 @@ typedef struct mg_tuning {
                                [24; 1 .. 2^20] */
   int32_t bfs_sparse_degree;/* MG_DIR_AUTO stays top-down on graphs of mean out-degree <= this [8; 0 .. 2^20] */
   int32_t bfs_ctas_per_sm;  /* CTAs of 256 threads per SM of the BFS level kernels [4; 1 .. 8] */
-  int32_t bfs_tail_max;     /* push levels of at most this many frontier vertices ... [2048; 0 .. 2^30] */
+  int32_t bfs_tail_max;     /* push levels of at most this many frontier vertices ... [512; 0 .. 2^30] */
   int32_t bfs_tail_edges;   /* ... and out-edges run one after another in a single CTA, one launch for the
                                run of them, wherever they occur (0: never) [16384; 0 .. 2^30] */
   int32_t reserved[16];

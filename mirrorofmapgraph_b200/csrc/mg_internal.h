@@ -106,7 +106,7 @@ inline mg_tuning tuning_defaults() {
   t.bfs_beta = 24;
   t.bfs_sparse_degree = 8;
   t.bfs_ctas_per_sm = 4;
-  t.bfs_tail_max = 2048;
+  t.bfs_tail_max = 512;
   t.bfs_tail_edges = 16384;
   return t;
 }
