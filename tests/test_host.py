@@ -270,3 +270,19 @@ def test_tuning_search_and_cache(tmp_path):
     with open(p, "w") as f:
         f.write("not json")
     assert tuning.load_cache(p) == {}
+
+
+def test_tuning_default_sources_prefer_reaching_vertices():
+    """Without given sources the tuner times vertices whose BFS reaches a large part
+    of the graph (a stand-in graph: odd vertices are isolated)."""
+    from mirrorofmapgraph_b200 import tuning
+
+    class Fake:
+        n, m = 1000, 40000
+
+        def bfs(self, srcs, **kw):
+            return None, {"edges_traversed": self.m if srcs[0] % 2 == 0 else 0}
+
+    src = tuning._default_sources(Fake(), 4)
+    assert len(src) == 4 and all(s % 2 == 0 for s in src)
+    assert src == tuning._default_sources(Fake(), 4)  # deterministic
