@@ -1085,10 +1085,6 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
   {
     std::vector<int32_t> co((size_t)n + 1);
     MG_CUDA_TRY(cudaMemcpyAsync(co.data(), g->co, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-    std::vector<int32_t> hrows((size_t)std::max<int64_t>(nh, 1));
-    if (nh > 0)
-      MG_CUDA_TRY(cudaMemcpyAsync(hrows.data(), sp.bins.hrows, sizeof(int32_t) * (size_t)nh, cudaMemcpyDeviceToHost,
-                                  s));
     MG_CUDA_TRY(cudaStreamSynchronize(s));
     int32_t dmax = 0;
     for (int64_t r = 0; r < n; r++) {
@@ -1119,30 +1115,35 @@ static mg_status seg_plan_build(mg_graph *g, int32_t T, int32_t S, bool weighted
     }
     sp.nrell = rg[sp.nrgroups];
     sp.npos = sp.nrgroups * 32 + nh;
-    std::vector<int32_t> prow((size_t)std::max<int64_t>(sp.npos, 1), -1), ppos((size_t)std::max<int64_t>(n, 1), -1);
-    for (int64_t i = 0; i < sp.nrgroups * 32; i++) prow[i] = rrow[i];
-    for (int64_t h = 0; h < nh; h++) prow[sp.nrgroups * 32 + h] = hrows[h];
-    for (int64_t i = 0; i < sp.npos; i++)
-      if (prow[i] >= 0) ppos[prow[i]] = (int32_t)i;
+    // positions: phase 2's lanes (rrow), then the hubs; prow and its inverse ppos
+    // are formed on the device
+    const size_t nprow = (size_t)std::max<int64_t>(sp.npos, 1), nppos = (size_t)std::max<int64_t>(n, 1);
     MG_TRY(dev_alloc(g, (void **)&sp.rrow, sizeof(int32_t) * rrow.size()));
     MG_TRY(dev_alloc(g, (void **)&sp.rgofs, sizeof(int64_t) * rg.size()));
     MG_TRY(dev_alloc(g, (void **)&sp.ridx, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nrell, 1)));
     if (weighted) MG_TRY(dev_alloc(g, (void **)&sp.rwts, sizeof(float) * (size_t)std::max<int64_t>(sp.nrell, 1)));
     MG_TRY(dev_alloc(g, (void **)&sp.rgrab, sizeof(int32_t)));
-    MG_TRY(dev_alloc(g, (void **)&sp.ppos, sizeof(int32_t) * ppos.size()));
-    MG_TRY(dev_alloc(g, (void **)&sp.prow, sizeof(int32_t) * prow.size()));
-    MG_TRY(dev_alloc(g, (void **)&sp.pslot, sizeof(int32_t) * prow.size()));
+    MG_TRY(dev_alloc(g, (void **)&sp.ppos, sizeof(int32_t) * nppos));
+    MG_TRY(dev_alloc(g, (void **)&sp.prow, sizeof(int32_t) * nprow));
+    MG_TRY(dev_alloc(g, (void **)&sp.pslot, sizeof(int32_t) * nprow));
     MG_CUDA_TRY(cudaMemsetAsync(sp.rgrab, 0, sizeof(int32_t), s));
     MG_CUDA_TRY(cudaMemsetAsync(sp.ridx, 0xff, sizeof(int32_t) * (size_t)std::max<int64_t>(sp.nrell, 1), s));
     if (weighted) MG_CUDA_TRY(cudaMemsetAsync(sp.rwts, 0, sizeof(float) * (size_t)std::max<int64_t>(sp.nrell, 1), s));
     MG_CUDA_TRY(cudaMemcpyAsync(sp.rrow, rrow.data(), sizeof(int32_t) * rrow.size(), cudaMemcpyHostToDevice, s));
     MG_CUDA_TRY(cudaMemcpyAsync(sp.rgofs, rg.data(), sizeof(int64_t) * rg.size(), cudaMemcpyHostToDevice, s));
-    MG_CUDA_TRY(cudaMemcpyAsync(sp.ppos, ppos.data(), sizeof(int32_t) * ppos.size(), cudaMemcpyHostToDevice, s));
-    MG_CUDA_TRY(cudaMemcpyAsync(sp.prow, prow.data(), sizeof(int32_t) * prow.size(), cudaMemcpyHostToDevice, s));
+    MG_CUDA_TRY(cudaMemsetAsync(sp.ppos, 0xff, sizeof(int32_t) * nppos, s));
+    MG_CUDA_TRY(cudaMemsetAsync(sp.prow, 0xff, sizeof(int32_t) * nprow, s));
+    if (sp.nrgroups > 0)
+      MG_CUDA_TRY(cudaMemcpyAsync(sp.prow, sp.rrow, sizeof(int32_t) * (size_t)(sp.nrgroups * 32),
+                                  cudaMemcpyDeviceToDevice, s));
+    if (nh > 0)
+      MG_CUDA_TRY(cudaMemcpyAsync(sp.prow + sp.nrgroups * 32, sp.bins.hrows, sizeof(int32_t) * (size_t)nh,
+                                  cudaMemcpyDeviceToDevice, s));
     if (sp.nrgroups > 0)
       seg_rows_fill_kernel<<<g->num_sms * 8, 256, 0, s>>>(sp.rrow, sp.rgofs, sp.nrgroups, g->co, sp.sidx, sp.swts,
                                                           sp.ridx, sp.rwts);
-    if (sp.npos > 0) seg_pos_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(sp.prow, sp.npos, hc.slot, sp.pslot);
+    if (sp.npos > 0)
+      seg_pos_slot_kernel<<<g->num_sms * 4, 256, 0, s>>>(sp.prow, sp.npos, hc.slot, sp.pslot, sp.ppos);
     MG_CUDA_TRY(cudaGetLastError());
     MG_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
   }

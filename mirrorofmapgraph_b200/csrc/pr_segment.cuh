@@ -298,11 +298,15 @@ __global__ void __launch_bounds__(256) seg_rows_fill_kernel(const int32_t *__res
   }
 }
 
-// Cached-column slot of every iterate position (plan data).
+// Cached-column slot of every iterate position, and the position of every row
+// (ppos, the inverse of prow; rows without a position keep the -1 it was set to).
 __global__ void seg_pos_slot_kernel(const int32_t *__restrict__ prow, int64_t npos, const int32_t *__restrict__ slot,
-                                    int32_t *__restrict__ pslot) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npos; i += (int64_t)gridDim.x * blockDim.x)
-    pslot[i] = prow[i] >= 0 ? slot[prow[i]] : -1;
+                                    int32_t *__restrict__ pslot, int32_t *__restrict__ ppos) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npos; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t r = prow[i];
+    pslot[i] = r >= 0 ? slot[r] : -1;
+    if (r >= 0) ppos[r] = (int32_t)i;
+  }
 }
 #endif  // MG_PRB_NO_PLAN_KERNELS
 
