@@ -417,7 +417,10 @@ typedef struct mg_tuning {
   int32_t bfs_tail_max;     /* push levels of at most this many frontier vertices ... [512; 0 .. 2^30] */
   int32_t bfs_tail_edges;   /* ... and out-edges run one after another in a single CTA, one launch for the
                                run of them, wherever they occur (0: never) [16384; 0 .. 2^30] */
-  int32_t reserved[16];
+  int32_t cc_rounds;        /* CC: rounds that link every vertex to its next neighbour before the largest sampled
+                               component is picked and only the vertices outside it read their other edges
+                               [1; 0 .. 8] */
+  int32_t reserved[15];
 } mg_tuning;
 void mg_tuning_defaults(mg_tuning *t);
 mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t);

@@ -72,7 +72,7 @@ class MgTuning(C.Structure):
                 ("bfs_grid_th", C.c_int32), ("bfs_defer_warp", C.c_int32), ("bfs_persist_max", C.c_int32),
                 ("bfs_persist_edges", C.c_int32), ("bfs_alpha", C.c_int32), ("bfs_beta", C.c_int32),
                 ("bfs_sparse_degree", C.c_int32), ("bfs_ctas_per_sm", C.c_int32), ("bfs_tail_max", C.c_int32),
-                ("bfs_tail_edges", C.c_int32), ("reserved", C.c_int32 * 16)]
+                ("bfs_tail_edges", C.c_int32), ("cc_rounds", C.c_int32), ("reserved", C.c_int32 * 15)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -11,8 +11,8 @@
 // decrease, so every root is its component's minimum and the final labels equal
 // the reference's bit for bit. The edge work follows the sampling scheme of
 // Afforest (Sutton et al., IPDPS 2018):
-//   1. two rounds link every vertex to its first and second neighbour, then
-//      compress;
+//   1. mg_tuning.cc_rounds rounds (1 by default) link every vertex to its first
+//      neighbours, then compress;
 //   2. one CTA samples 1024 vertices and takes the most frequent root c (on
 //      power-law graphs, the giant component);
 //   3. only vertices outside c process their remaining edges (and, without a
@@ -31,7 +31,6 @@ namespace mg {
 
 constexpr int CC_NT = 256;
 constexpr int CC_CTA_TH = 1024;
-constexpr int CC_ROUNDS = 2;
 constexpr int CC_SAMPLES = 1024;
 
 // Root of x with path halving. Parent entries are read from L2 (ld.cg): they are
@@ -210,15 +209,19 @@ extern "C" mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_
   int64_t launches = 0;
   cc_init_kernel<<<grid, 256, 0, s>>>(parent, n);
   launches++;
+  // Neighbour-sampling rounds before the giant component is picked: R-MAT s22
+  // 0.33 / 0.41 / 0.48 ms with 1 / 2 / 3 rounds. With none, only the sampled
+  // root's own self-loops are skipped, so every count gives the same labels.
+  const int32_t rounds = g->tune.cc_rounds;
   if (n > 0 && sampling) {
     // one launch per round: every vertex's first link lands before any second
-    // (both rounds in one pass measured 0.51 against 0.41 ms on R-MAT s22)
-    for (int r = 0; r < CC_ROUNDS; r++) cc_sample_link_kernel<<<grid, 256, 0, s>>>(g->ro, g->ci, n, parent, r, r + 1);
+    // (two rounds in one pass measured 0.51 against 0.41 ms on R-MAT s22)
+    for (int r = 0; r < rounds; r++) cc_sample_link_kernel<<<grid, 256, 0, s>>>(g->ro, g->ci, n, parent, r, r + 1);
     cc_compress_kernel<<<grid, 256, 0, s>>>(parent, nullptr, n);
     cc_mode_kernel<<<1, CC_SAMPLES, 0, s>>>(parent, n, cmode);
-    cc_finish_kernel<<<g->num_sms * 4, CC_NT, 0, s>>>(g->ro, g->ci, g->co, g->ri, n, parent, cmode, CC_ROUNDS,
+    cc_finish_kernel<<<g->num_sms * 4, CC_NT, 0, s>>>(g->ro, g->ci, g->co, g->ri, n, parent, cmode, rounds,
                                                       symmetric ? 0 : 1, insp);
-    launches += CC_ROUNDS + 3;
+    launches += rounds + 3;
   } else if (n > 0) {
     cc_all_edges_kernel<<<g->num_sms * 4, CC_NT, 0, s>>>(g->ro, g->ci, n, parent, insp);
     launches++;
@@ -233,7 +236,7 @@ extern "C" mg_status mg_cc(mg_graph *g, int32_t *label, const mg_opts *opts, mg_
     std::memset(stats, 0, sizeof(*stats));
     stats->iterations = 1;
     stats->edges_traversed = g->m;
-    stats->edges_inspected = g->ctl_host->edges_inspected + (sampling ? CC_ROUNDS * n : 0);
+    stats->edges_inspected = g->ctl_host->edges_inspected + (sampling ? (int64_t)rounds * n : 0);
     // offsets and sampled neighbours, the remaining edges actually read, parent
     // init / compress passes
     stats->bytes_compulsory = 4 * (n + 1) + 4 * stats->edges_inspected + 16 * n;

@@ -99,7 +99,8 @@ extern "C" mg_status mg_graph_set_tuning(mg_graph *g, const mg_tuning *t) {
                  {"bfs_sparse_degree", t->bfs_sparse_degree, 0, 1 << 20},
                  {"bfs_ctas_per_sm", t->bfs_ctas_per_sm, 1, 8},
                  {"bfs_tail_max", t->bfs_tail_max, 0, 1 << 30},
-                 {"bfs_tail_edges", t->bfs_tail_edges, 0, 1 << 30}};
+                 {"bfs_tail_edges", t->bfs_tail_edges, 0, 1 << 30},
+                 {"cc_rounds", t->cc_rounds, 0, 8}};
   for (const Range &x : r) {
     if (x.v < x.lo || x.v > x.hi) {
       mg_set_error("mg_graph_set_tuning: %s = %d outside [%d, %d]", x.name, x.v, x.lo, x.hi);

@@ -108,6 +108,7 @@ inline mg_tuning tuning_defaults() {
   t.bfs_ctas_per_sm = 4;
   t.bfs_tail_max = 512;
   t.bfs_tail_edges = 16384;
+  t.cc_rounds = 1;
   return t;
 }
 

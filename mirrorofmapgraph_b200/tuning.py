@@ -47,6 +47,9 @@ CANDIDATES: dict[str, dict[str, list[int]]] = {
     "sssp_batch": {
         "sssp_batch_heavy": [16, 32, 64, 128],
     },
+    "cc": {
+        "cc_rounds": [0, 1, 2, 3],
+    },
 }
 
 # Fields whose legal range depends on another field: set the bound first.
@@ -133,7 +136,8 @@ def _default_sources(graph, k: int, seed: int = 7, tries: int = 64) -> list[int]
 def device_time(graph, program: str, sources: Sequence[int], reps: int = 3) -> float:
     """Median over reps of the summed device time (ms) of one run per source of
     `program` ("bfs", "sssp" single-source, "sssp_batch" one batch of all
-    sources), after one untimed run (plans, loop graphs)."""
+    sources, "cc" one run per source, which it does not use), after one untimed
+    run (plans, loop graphs)."""
     import torch
     out = torch.empty(graph.n * (len(sources) if program == "sssp_batch" else 1), dtype=torch.int32,
                       device="cuda")
@@ -141,6 +145,8 @@ def device_time(graph, program: str, sources: Sequence[int], reps: int = 3) -> f
     def once() -> float:
         if program == "sssp_batch":
             return graph.sssp_batch(np.asarray(sources, dtype=np.int32), out=out)[1]["kernel_ms"]
+        if program == "cc":
+            return sum(graph.cc(out=out)[1]["kernel_ms"] for _ in sources)
         fn = graph.bfs if program == "bfs" else graph.sssp
         return sum(fn([s], out=out)[1]["kernel_ms"] for s in sources)
 

@@ -167,3 +167,18 @@ def test_degree_stats(rmat13):
     assert g._lib.mg_graph_degree_stats(g._h, C.byref(mx), C.byref(iso)) == L.MG_OK
     deg = np.diff(h.row_offsets)
     assert mx.value == deg.max() and iso.value == int((deg == 0).sum())
+
+
+@pytest.mark.parametrize("rounds", [0, 1, 2, 8])
+def test_cc_rounds_are_exact(rounds):
+    """Every count of neighbour-sampling rounds gives the minimum-id labels: a
+    symmetric R-MAT graph (sampling over the CSR), a directed one read both ways
+    (sampling over CSR and CSC) and a graph of many small components."""
+    graphs = [(mg.gen_rmat(13, 16, 71, symmetrize=True), True), (mg.gen_rmat(12, 8, 72, symmetrize=False), False),
+              (mg.gen_er(5000, 3000, 73), False)]
+    for h, sym in graphs:
+        with mg.Graph(h.row_offsets, h.col_idx, symmetric=sym) as g:
+            g.set_tuning(cc_rounds=rounds)
+            lab, st = g.cc()
+            np.testing.assert_array_equal(lab, oracle.cc(h.row_offsets, h.col_idx))
+            assert st["edges_traversed"] == h.m

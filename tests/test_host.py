@@ -240,7 +240,7 @@ def test_binary_csr_cache_round_trip_and_rejects_garbage(tmp_path):
 def test_tuning_defaults_need_no_device():
     d = mg.Graph.default_tuning()
     assert d["sssp_heavy"] == 256 and d["sssp_heavy_small"] == 32 and d["sssp_ctas_per_sm"] == 4
-    assert d["sssp_chunk_cap"] == 0 and d["sssp_batch_heavy"] == 32
+    assert d["sssp_chunk_cap"] == 0 and d["sssp_batch_heavy"] == 32 and d["cc_rounds"] == 1
 
 
 def test_tuning_search_and_cache(tmp_path):
